@@ -1,0 +1,415 @@
+#!/usr/bin/env python
+"""Headline benchmark: Nf=2 HMC trajectories/s on a 512x512 lattice.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Workload (one "step" = one HMC trajectory): Nf=2 Wilson fermions, beta=4.0,
+m0=0.1, leapfrog ns=20, eps=0.05 (tau=1), every CG solved to |r|/|b| < 1e-12
+(the reference's stop rule with eps=1e-24), FP32-inner/FP64-reliable-update
+solver.  Synthetic data: a seeded hot start thermalised by 10 untimed pure-gauge
+trajectories.  The working set (~60 MB) fits in L2, so L2 is flushed (256 MiB
+write) between timed trajectories.
+
+Prints one JSON line (rank 0).  Under torchrun every rank runs an independent
+replica chain (no collective on the data path): value = all ranks' trajectories
+/ the slowest rank's time.
+
+--impl reference times the reference's algorithm on the host CPU cores: the C
+restatement in oracle/ (the reference itself is Julia/CUDA.jl with no CPU
+path, and Julia is not installed), on a bounded sample of the same workload.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+for _p in (REPO, os.path.join(REPO, "dav-qed2d_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "HMC traj/s Nf=2 512²: mixed+batched vs FP64 at CG res 1e-12; Dslash HBM GB/s"
+L, BETA, AM0, NS, EPS, TOL, MAXITER = 512, 4.0, 0.1, 20, 0.05, 1e-24, 200000
+SEED = 1234
+WORKLOAD = (f"Nf=2 HMC trajectory, {L}x{L}, beta={BETA}, m0={AM0}, leapfrog ns={NS} eps={EPS}, "
+            f"CG to |r|/|b|<1e-12 (eps=1e-24)")
+THERM_TRAJ = 10
+# algorithmic bytes per site (see DESIGN.md "Kernels and their rooflines")
+B_MIXED_ITER = 192.0     # FP32 fused iteration: phase A 80 B + phase B 112 B
+B_MIXED_UPDATE = 400.0   # one FP64 reliable update (4 phases)
+B_MIXED_SETUP = 112.0    # |b|^2, x=0, r32 = b/|b|, x32 = 0
+B_F64_ITER = 384.0       # FP64 fused iteration: phase A 160 B + phase B 224 B
+B_DSLASH_F64 = 96.0      # g5Dw apply, FP64: spinor in 32 + links 32 + out 32
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.index)], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def hot_start(L1, L2, seed):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    return np.exp(1j * rng.uniform(-np.pi, np.pi, (2, L2, L1)))
+
+
+# ---------------------------------------------------------------------------
+# reference arm / CPU baseline: the oracle (C restatement of the reference)
+def oracle_sample(U, seed, counter):
+    """One update_momenta! of the workload (CG solve to 1e-24 + both forces +
+    momentum kick) on the host cores; a trajectory is NS+1 of these."""
+    import numpy as np
+    from oracle import oracle as O
+    o = O.Oracle(L, L, BETA)
+    z = O.Oracle.normal(4 * L * L, seed, 16, counter)
+    X = ((z[0::2] + 1j * z[1::2]) / np.sqrt(2.0)).reshape(2, L, L)
+    F = o.g5dw(U, X, AM0)
+    mom = O.Oracle.normal(2 * L * L, seed, 1, counter).reshape(2, L, L)
+    Xs, G = o.cfield(), o.cfield()
+    it = C.c_int(0)
+    t0 = time.perf_counter()
+    st = o.L.o_update_momenta_nf2(o._pp, O._p(mom), O._p(np.ascontiguousarray(U)), O._p(Xs), O._p(F), O._p(G),
+                                  AM0, 0.5 * EPS, MAXITER, TOL, C.byref(it))
+    dt = time.perf_counter() - t0
+    if st != 0:
+        raise RuntimeError("oracle CG did not converge")
+    return dt, it.value
+
+
+def oracle_thermalised_field():
+    """The same thermalisation as the GPU arm, replayed on the oracle."""
+    from oracle import oracle as O
+    o = O.Oracle(L, L, BETA)
+    U = hot_start(L, L, SEED)
+    for t in range(THERM_TRAJ):
+        mom0 = O.Oracle.normal(2 * L * L, SEED + 1, 1, t).reshape(2, L, L)
+        st, U, acc, hi, hf = o.hmc_gauge(U, 0.1, 10, mom0, O.Oracle.uniform(SEED + 1, 3, t))
+    return U
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    U = oracle_thermalised_field()
+    times, iters = [], []
+    for k in range(args.warmup + args.steps):
+        dt, it = oracle_sample(U, SEED, 1000 + k)
+        if k >= args.warmup:
+            times.append(dt)
+            iters.append(it)
+    t_traj = (NS + 1) * statistics.mean(times)
+    value = 1.0 / t_traj
+    cores = O.num_threads()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "traj/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_traj, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "solver": "reference CG (FP64, host)"},
+        "cpu_baseline": {"value": value, "unit": "traj/s", "cores": cores, "kind": "port",
+                         "sample": f"per step one update_momenta! (CG solve to 1e-24 + forces) of the {L}x{L} "
+                                   f"workload on the thermalised field, x{NS + 1} per trajectory; "
+                                   f"mean CG iterations {statistics.mean(iters):.0f}"},
+        "e2e": {"value": value, "unit": "traj/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    import qed2d
+    from qed2d import _lib
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dev = torch.device("cuda", local)
+    Lb = _lib.lib()
+    prm = qed2d.LattParm((L, L), BETA)
+    seed = SEED + 7919 * rank
+    qed2d.seed(seed + 1)
+
+    # --- set-up: hot start + pure-gauge thermalisation (untimed)
+    U = torch.from_numpy(hot_start(L, L, SEED)).to(dev)
+    for _ in range(THERM_TRAJ):
+        qed2d.HMC_(U, 0.1, 10, [], prm, None)
+    qed2d.set_precision("mixed")
+    qed2d.seed(seed)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    acc = []
+
+    def step():
+        flush.fill_(1.0)
+        return qed2d.HMC_(U, AM0, EPS, NS, acc, MAXITER, TOL, prm, None)
+
+    for _ in range(args.warmup):
+        step()
+    clocks = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    n0 = Lb.qed2d_launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    infos = [step() for _ in range(args.steps)]
+    ev1.record()
+    torch.cuda.synchronize()
+    launches = Lb.qed2d_launch_count() - n0
+    clk = clocks.stop()
+    elapsed = ev0.elapsed_time(ev1) / 1e3
+    if dist:
+        t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    value = world * args.steps / elapsed
+    iters = [i.cg_iterations for i in infos]
+
+    # --- e2e: the same step through the C ABI with host buffers (H2D of the
+    # links from pinned memory, the trajectory, D2H of links + result)
+    h = qed2d.context(L, L, BETA)
+    U_host = U.cpu().pin_memory()
+    res = _lib.HmcResult()
+    e2e_steps = max(1, args.steps)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for k in range(e2e_steps):
+        U.copy_(U_host, non_blocking=True)
+        st = Lb.qed2d_hmc_nf2(h, C.c_void_p(U.data_ptr()), AM0, EPS, NS, _lib.LEAPFROG, MAXITER, TOL, 0,
+                              seed, 50000 + k, C.byref(res))
+        _lib.check(st, "hmc_nf2")
+        U_host.copy_(U, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_t = e0.elapsed_time(e1) / 1e3
+    if dist:
+        t = torch.tensor([e2e_t], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_t = float(t.item())
+    e2e = {"value": world * e2e_steps / e2e_t, "unit": "traj/s",
+           "h2d_bytes_per_step": U.numel() * 16, "d2h_bytes_per_step": U.numel() * 16 + C.sizeof(res)}
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+
+    # --- roofline of the dominant kernel: one mixed CG solve (a single
+    # persistent launch) at the workload's field, timed with CUDA events
+    peak, peak_kind = load_peaks()
+    X = qed2d.cfield(L, L)
+    X.copy_(torch.randn(2, L, L, dtype=torch.complex128, device=dev) / np.sqrt(2.0))
+    F = qed2d.cfield(L, L)
+    qed2d.gamm5Dw(F, U, X, AM0, prm)
+    Xs = qed2d.cfield(L, L)
+    kern = []
+    for _ in range(4):
+        flush.fill_(1.0)
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record()
+        it = qed2d.CG(Xs, U, F, AM0, MAXITER, TOL, qed2d.gamm5Dw_sqr_msq, prm, None)
+        a1.record()
+        torch.cuda.synchronize()
+        it, _, upd = qed2d.last_solve(prm)
+        kern.append((a0.elapsed_time(a1) / 1e3, it, upd))
+    t_k, it_k, upd_k = min(kern[1:])
+    V = L * L
+    bytes_k = V * (B_MIXED_SETUP + it_k * B_MIXED_ITER + upd_k * B_MIXED_UPDATE)
+    achieved = bytes_k / t_k / 1e9
+    traffic = None
+    prof = os.path.join(REPO, "profiles", "cg_mixed_512_traffic.json")
+    if os.path.exists(prof):
+        try:
+            pj = json.load(open(prof))
+            traffic = pj["dram_bytes_per_iteration"] * it_k
+        except Exception:
+            traffic = None
+    roofline = {"kernel": "k_cg_mixed", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                "note": f"one launch = one solve: {it_k} FP32 iterations x {B_MIXED_ITER:.0f} B/site + "
+                        f"{upd_k} FP64 reliable updates x {B_MIXED_UPDATE:.0f} B/site; working set L2-resident "
+                        f"at {L}^2 (effective bandwidth)"}
+
+    # --- the plain FP64 GPU path (reference-structured) and the fused FP64 path,
+    # same trajectory (same seed and counter) as the first timed step
+    base = {}
+    for prec in (() if args.skip_baselines else ("plain", "f64")):
+        qed2d.set_precision(prec)
+        Ub = U.clone()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        info = qed2d.HMC_(Ub, AM0, EPS, NS, [], MAXITER, TOL, prm, None, counter=infos[0].counter)
+        torch.cuda.synchronize()
+        base[prec] = (time.perf_counter() - t0, info.cg_iterations)
+    qed2d.set_precision("mixed")
+
+    # --- Dslash / CG-iteration HBM bandwidth at 8192^2 (working set >> L2)
+    dslash = None
+    if not args.skip_sweep:
+        Lbig = 8192
+        pb = qed2d.LattParm((Lbig, Lbig), BETA)
+        Ub = torch.polar(torch.ones(2, Lbig, Lbig, dtype=torch.float64, device=dev),
+                         (torch.rand(2, Lbig, Lbig, dtype=torch.float64, device=dev) * 2 - 1) * np.pi)
+        si = torch.randn(2, Lbig, Lbig, dtype=torch.complex128, device=dev)
+        so = torch.empty_like(si)
+        for _ in range(3):
+            qed2d.gamm5Dw(so, Ub, si, AM0, pb)
+        n_ap = 20
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record()
+        for _ in range(n_ap):
+            qed2d.gamm5Dw(so, Ub, si, AM0, pb)
+        a1.record()
+        torch.cuda.synchronize()
+        t_ap = a0.elapsed_time(a1) / 1e3 / n_ap
+        Vb = Lbig * Lbig
+        f64_gbs = B_DSLASH_F64 * Vb / t_ap / 1e9
+        # FP32 fused CG iterations (mixed solver capped at 60 iterations)
+        xs = torch.zeros_like(si)
+        cg_runs = []
+        for _ in range(2):
+            a0.record()
+            try:
+                qed2d.CG(xs, Ub, si, AM0, 60, TOL, qed2d.gamm5Dw_sqr_msq, pb, None)
+            except qed2d.Qed2dError:
+                pass
+            a1.record()
+            torch.cuda.synchronize()
+            it, _, upd = qed2d.last_solve(pb)
+            cg_runs.append((a0.elapsed_time(a1) / 1e3, it, upd))
+        t_cg, it_cg, upd_cg = cg_runs[-1]
+        cg_gbs = Vb * (B_MIXED_SETUP + it_cg * B_MIXED_ITER + upd_cg * B_MIXED_UPDATE) / t_cg / 1e9
+        dslash = {"lattice": f"{Lbig}x{Lbig}", "g5dw_f64_GBs": f64_gbs, "g5dw_f64_frac": f64_gbs / peak,
+                  "g5dw_f64_us": t_ap * 1e6, "cg_mixed_GBs": cg_gbs, "cg_mixed_frac": cg_gbs / peak,
+                  "cg_mixed_iters": it_cg, "cg_mixed_updates": upd_cg, "peak_GBs": peak, "peak_kind": peak_kind}
+        del Ub, si, so, xs
+        torch.cuda.empty_cache()
+
+    # --- CPU baseline: the oracle on the host cores, bounded sample
+    cpu = None
+    if not args.skip_cpu:
+        from oracle import oracle as O
+        Uh = U.cpu().numpy()
+        dt, it = oracle_sample(Uh, seed, 999)
+        cpu = {"value": 1.0 / ((NS + 1) * dt), "unit": "traj/s", "cores": O.num_threads(), "kind": "port",
+               "sample": f"one update_momenta! (CG to 1e-24, {it} iterations, + forces) of the {L}x{L} workload "
+                         f"on the benchmark's field, x{NS + 1} per trajectory"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "traj/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": f"synthetic: seeded hot start thermalised by {THERM_TRAJ} pure-gauge trajectories",
+        "config": {"workload": WORKLOAD, "L1": L, "L2": L, "beta": BETA, "m0": AM0, "ns": NS, "eps": EPS,
+                   "cg_tol_sq": TOL, "solver": "mixed FP32 inner / FP64 reliable updates, FP64 stop rule",
+                   "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"},
+        "e2e": e2e,
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "gpu_launches": int(launches),
+        "trajectories": {"cg_iterations_mean": statistics.mean(iters), "accepted": sum(acc[-args.steps:]),
+                         "dH": [round(i.dH, 6) for i in infos]},
+        "baselines": None if not base else {
+            "plain_f64_gpu_traj_s": 1.0 / base["plain"][0], "plain_f64_cg_iterations": base["plain"][1],
+            "f64_fused_gpu_traj_s": 1.0 / base["f64"][0], "f64_fused_cg_iterations": base["f64"][1],
+            "mixed_vs_plain": value / world / (1.0 / base["plain"][0]),
+            "mixed_vs_f64_fused": value / world / (1.0 / base["f64"][0])},
+        "dslash_hbm": dslash,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--skip-sweep", action="store_true", help="skip the 8192^2 Dslash bandwidth sweep")
+    ap.add_argument("--skip-cpu", action="store_true", help="skip the oracle CPU baseline")
+    ap.add_argument("--skip-baselines", action="store_true",
+                    help="skip the plain-FP64 and fused-FP64 GPU trajectories")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,734 @@
+// cg.cu -- conjugate-gradient solvers of libqed2d on the Hermitian positive
+// operator A + mu^2, A = (g5 Dw)^2 (gamm5Dw_sqr_msq / gamm5Dw_sqr_musq of
+// src/QED2dDirac.jl:69-95).
+//
+// QED2D_PREC_F64 and QED2D_PREC_MIXED run a whole solve as ONE persistent
+// cooperative launch: every block owns a fixed set of 32x8 tiles, the two
+// reductions of an iteration go through per-block partials summed in a fixed
+// order by every block (deterministic, no host round trip), and phases are
+// separated by a bounded grid barrier.  Per iteration:
+//   phase A:  p = r + beta p_old (evaluated on load, at the 5 stencil points),
+//             t = g5Dw p, store p and t,  partial <p,Ap> = |t|^2 + mu^2 |p|^2
+//   phase B:  Ap = g5Dw t + mu^2 p, x += alpha p, r -= alpha Ap, partial |r|^2
+// (g5Dw is Hermitian, so <p, (g5Dw)^2 p> = |g5Dw p|^2.)  The stop rule is the
+// reference's: |r|^2 < eps |b|^2 (src/QED2dSolver.jl:13-29).
+//
+// QED2D_PREC_MIXED runs phases A/B in FP32 on packed float4 fields with FP64
+// partial sums, and replaces the residual by the FP64 true residual
+// b - (A + mu^2) x (reliable update) whenever the FP32 residual has dropped by
+// delta^2 since the last update, or looks converged; it stops only when the FP64
+// true residual meets the reference's tolerance.  FP32 fields are kept at unit
+// norm (rescaled at every update), so tiny right-hand sides cannot underflow.
+//
+// QED2D_PREC_PLAIN mirrors the reference's own structure (src/QED2dSolver.jl):
+// unfused kernels and two device-to-host reads per iteration.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "stencil.cuh"
+
+namespace qed2d {
+
+constexpr int kMaxShifts = QED2D_MAXPOLES;
+
+struct CGP {
+    Lat g;
+    const double2* U;
+    const float4* U32;
+    const double2* b;
+    double2* x;
+    double2* r;      // FP64 residual (planes)
+    double2* p0;     // FP64 search directions (double buffer)
+    double2* p1;
+    double2* t;      // FP64 g5Dw p  (mixed: g5Dw x at reliable updates)
+    float4* r32;
+    float4* q0;      // FP32 search directions (double buffer)
+    float4* q1;
+    float4* t32;
+    float4* x32;
+    double2* g5x;    // optional output g5Dw x (F64 path)
+    double m2;       // 2 + m0
+    double mu2;
+    double eps;
+    double delta2;   // reliable-update threshold delta^2 (mixed)
+    int maxiter;
+    int guess;
+    DevCtl* ctl;
+    double* part;
+};
+
+__device__ __forceinline__ void write_partials(double* part, const double* v, int nv) {
+    if (threadIdx.x == 0)
+        for (int k = 0; k < nv; k++) part[(size_t)k * kMaxPartBlocks + blockIdx.x] = v[k];
+}
+
+template <int NV>
+__device__ __forceinline__ bool reduce_sync(GridSync& gs, double (&v)[NV], double* part, double* smem) {
+    block_sum<NV>(v, smem);
+    write_partials(part, v, NV);
+    if (!gs.sync()) return false;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            double s = 0.0;
+            for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) s += __ldcg(part + (size_t)k * kMaxPartBlocks + i);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (threadIdx.x == 0) smem[k] = s;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; k++) v[k] = smem[k];
+    __syncthreads();
+    return true;
+}
+
+__device__ __forceinline__ void finish_solve(const CGP& P, int iters, bool conv, double rr, double bb,
+                                             int updates = 0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        DevCtl* c = P.ctl;
+        const int err = ld_volatile_int(&c->err);
+        c->last_iters = iters;
+        c->last_updates = updates;
+        c->last_conv = conv && !err;
+        c->last_relres = bb > 0.0 ? rr / bb : 0.0;
+        c->iters_total += iters;
+        if (c->status == 0) {
+            if (err) c->status = QED2D_ERR_TIMEOUT;
+            else if (!conv) c->status = QED2D_ERR_NOT_CONVERGED;
+        }
+    }
+}
+
+#define FOR_TILES(q)                                                                     \
+    for (long long tile_ = blockIdx.x; tile_ < ntiles; tile_ += gridDim.x)              \
+        if (const Site q = site_of_tile(P.g, tile_, threadIdx.x); q.ok)
+
+// ---------------------------------------------------------------------------
+// FP64 persistent CG
+__global__ void __launch_bounds__(TILE) k_cg_f64(const CGP P) {
+    __shared__ double smem[32 * 2];
+    GridSync gs{&P.ctl->bar, &P.ctl->err, 0};
+    const long long ntiles = num_tiles(P.g), V = P.g.V;
+    const LkD L{P.U, V};
+    const double m2 = P.m2, mu2 = P.mu2;
+    int k = 0;
+    bool conv = false;
+    double rr = 0.0, bb = 0.0;
+
+    // setup: |b|^2, and x = 0 / r = b, or t = g5Dw x for a warm start
+    {
+        double v[1] = {0.0};
+        FOR_TILES(q) {
+            const Pair<double> bv{__ldg(P.b + q.x), __ldg(P.b + q.x + V)};
+            v[0] += norm2(bv.a) + norm2(bv.b);
+            if (!P.guess) {
+                st_d(P.x, V, q.x, Pair<double>{make_double2(0, 0), make_double2(0, 0)});
+                st_d(P.r, V, q.x, bv);
+            } else {
+                st_d(P.t, V, q.x, g5dw_at<double>(SpD{P.x, V}, L, q, m2));
+            }
+        }
+        if (!reduce_sync<1>(gs, v, P.part, smem)) goto done;
+        bb = v[0];
+    }
+    if (bb == 0.0) {   // zero source: zero solution
+        if (P.guess) FOR_TILES(q) st_d(P.x, V, q.x, Pair<double>{make_double2(0, 0), make_double2(0, 0)});
+        conv = true;
+        if (!gs.sync()) goto done;
+        goto epilogue;
+    }
+    {
+        const double tol = P.eps * bb;
+        if (P.guess) {
+            double v[1] = {0.0};
+            FOR_TILES(q) {
+                const Pair<double> xc = SpD{P.x, V}.ld(q.x);
+                const Pair<double> a = g5dw_at<double>(SpD{P.t, V}, L, q, m2);
+                Pair<double> r;
+                r.a = __ldg(P.b + q.x) - (a.a + mu2 * xc.a);
+                r.b = __ldg(P.b + q.x + V) - (a.b + mu2 * xc.b);
+                st_d(P.r, V, q.x, r);
+                v[0] += norm2(r.a) + norm2(r.b);
+            }
+            if (!reduce_sync<1>(gs, v, P.part, smem)) goto done;
+            rr = v[0];
+            if (rr < tol) { conv = true; goto epilogue; }
+        } else {
+            rr = bb;
+        }
+        double beta = 0.0;
+        for (k = 1; k <= P.maxiter; k++) {
+            double2* pn = (k & 1) ? P.p0 : P.p1;
+            const double2* po = (k & 1) ? P.p1 : P.p0;
+            const SpAxpy<double, SpD> Q{SpD{P.r, V}, SpD{po, V}, beta, k > 1};
+            double v[1] = {0.0};
+            FOR_TILES(q) {
+                const Pair<double> c = Q.ld(q.x);
+                const Pair<double> tt = g5dw_at_c<double>(Q, c, L, q, m2);
+                st_d(pn, V, q.x, c);
+                st_d(P.t, V, q.x, tt);
+                v[0] += norm2(tt.a) + norm2(tt.b) + mu2 * (norm2(c.a) + norm2(c.b));
+            }
+            if (!reduce_sync<1>(gs, v, P.part, smem)) goto done;
+            const double alpha = rr / v[0];
+            v[0] = 0.0;
+            FOR_TILES(q) {
+                const Pair<double> pc = SpD{pn, V}.ld(q.x);
+                const Pair<double> a = g5dw_at<double>(SpD{P.t, V}, L, q, m2);
+                Pair<double> xv = SpD{P.x, V}.ld(q.x), r = SpD{P.r, V}.ld(q.x);
+                xv.a = xv.a + alpha * pc.a;
+                xv.b = xv.b + alpha * pc.b;
+                r.a = r.a - alpha * (a.a + mu2 * pc.a);
+                r.b = r.b - alpha * (a.b + mu2 * pc.b);
+                st_d(P.x, V, q.x, xv);
+                st_d(P.r, V, q.x, r);
+                v[0] += norm2(r.a) + norm2(r.b);
+            }
+            if (!reduce_sync<1>(gs, v, P.part, smem)) goto done;
+            const double rn = v[0];
+            if (rn < tol) { rr = rn; conv = true; break; }
+            beta = rn / rr;
+            rr = rn;
+        }
+        if (!conv) k = P.maxiter;
+    }
+epilogue:
+    if (P.g5x) FOR_TILES(q) st_d(P.g5x, V, q.x, g5dw_at<double>(SpD{P.x, V}, L, q, m2));
+done:
+    finish_solve(P, k, conv, rr, bb);
+}
+
+// ---------------------------------------------------------------------------
+// mixed FP32/FP64 reliable-update CG
+__global__ void __launch_bounds__(TILE) k_cg_mixed(const CGP P) {
+    __shared__ double smem[32 * 2];
+    GridSync gs{&P.ctl->bar, &P.ctl->err, 0};
+    const long long ntiles = num_tiles(P.g), V = P.g.V;
+    const LkD L{P.U, V};
+    const LkF Lf{P.U32};
+    const double m2 = P.m2, mu2 = P.mu2;
+    const float m2f = (float)m2, mu2f = (float)mu2;
+    double2* t64 = P.g5x ? P.g5x : P.t;
+    int k = 0, nupd = 0;
+    bool conv = false;
+    double rr64 = 0.0, bb = 0.0;
+
+    {
+        double v[1] = {0.0};
+        FOR_TILES(q) {
+            const Pair<double> bv{__ldg(P.b + q.x), __ldg(P.b + q.x + V)};
+            v[0] += norm2(bv.a) + norm2(bv.b);
+            if (!P.guess) st_d(P.x, V, q.x, Pair<double>{make_double2(0, 0), make_double2(0, 0)});
+            else st_d(t64, V, q.x, g5dw_at<double>(SpD{P.x, V}, L, q, m2));
+        }
+        if (!reduce_sync<1>(gs, v, P.part, smem)) goto done;
+        bb = v[0];
+    }
+    if (bb == 0.0) {
+        FOR_TILES(q) {
+            st_d(P.x, V, q.x, Pair<double>{make_double2(0, 0), make_double2(0, 0)});
+            if (P.g5x) st_d(P.g5x, V, q.x, Pair<double>{make_double2(0, 0), make_double2(0, 0)});
+        }
+        conv = true;
+        goto done;
+    }
+    {
+        const double tol = P.eps * bb;
+        if (P.guess) {
+            double v[1] = {0.0};
+            FOR_TILES(q) {
+                const Pair<double> xc = SpD{P.x, V}.ld(q.x);
+                const Pair<double> a = g5dw_at<double>(SpD{t64, V}, L, q, m2);
+                Pair<double> r;
+                r.a = __ldg(P.b + q.x) - (a.a + mu2 * xc.a);
+                r.b = __ldg(P.b + q.x + V) - (a.b + mu2 * xc.b);
+                st_d(P.r, V, q.x, r);
+                v[0] += norm2(r.a) + norm2(r.b);
+            }
+            if (!reduce_sync<1>(gs, v, P.part, smem)) goto done;
+            rr64 = v[0];
+            if (rr64 < tol) { conv = true; goto done; }
+        } else {
+            rr64 = bb;
+        }
+        const double2* rsrc = P.guess ? P.r : P.b;
+        double s = 1.0 / sqrt(rr64);
+        double rr;   // |r32|^2 at the start of the current iteration
+        {
+            double v[1] = {0.0};
+            FOR_TILES(q) {
+                const double2 a = rsrc[q.x], b2 = rsrc[q.x + V];
+                const Pair<float> r32{to_f(s * a), to_f(s * b2)};
+                st_f(P.r32, q.x, r32);
+                st_f(P.x32, q.x, Pair<float>{make_float2(0, 0), make_float2(0, 0)});
+                v[0] += (double)norm2(r32.a) + (double)norm2(r32.b);
+            }
+            if (!reduce_sync<1>(gs, v, P.part, smem)) goto done;
+            rr = v[0];
+        }
+        double maxrr = rr, beta = 0.0;
+        bool first = true;
+        int cur = 0;
+        for (k = 1; k <= P.maxiter; k++) {
+            float4* qn = cur ? P.q1 : P.q0;
+            const float4* qo = cur ? P.q0 : P.q1;
+            const SpAxpy<float, SpF> Q{SpF{P.r32}, SpF{qo}, (float)beta, !first};
+            double v[1] = {0.0};
+            FOR_TILES(q) {
+                const Pair<float> c = Q.ld(q.x);
+                const Pair<float> tt = g5dw_at_c<float>(Q, c, Lf, q, m2f);
+                st_f(qn, q.x, c);
+                st_f(P.t32, q.x, tt);
+                v[0] += (double)(norm2(tt.a) + norm2(tt.b)) + mu2 * (double)(norm2(c.a) + norm2(c.b));
+            }
+            if (!reduce_sync<1>(gs, v, P.part, smem)) goto done;
+            const float alpha = (float)(rr / v[0]);
+            v[0] = 0.0;
+            FOR_TILES(q) {
+                const Pair<float> pc = SpF{qn}.ld(q.x);
+                const Pair<float> a = g5dw_at<float>(SpF{P.t32}, Lf, q, m2f);
+                Pair<float> xv = SpF{P.x32}.ld(q.x), r = SpF{P.r32}.ld(q.x);
+                xv.a = xv.a + alpha * pc.a;
+                xv.b = xv.b + alpha * pc.b;
+                r.a = r.a - alpha * (a.a + mu2f * pc.a);
+                r.b = r.b - alpha * (a.b + mu2f * pc.b);
+                st_f(P.x32, q.x, xv);
+                st_f(P.r32, q.x, r);
+                v[0] += (double)(norm2(r.a) + norm2(r.b));
+            }
+            if (!reduce_sync<1>(gs, v, P.part, smem)) goto done;
+            const double rn = v[0];
+            maxrr = fmax(maxrr, rn);
+            const bool cand = rn < tol * s * s;
+            if (rn < P.delta2 * maxrr || cand || k == P.maxiter) {
+                // reliable update: x += x32 / s, then the FP64 true residual
+                nupd++;
+                const double inv_s = 1.0 / s;
+                FOR_TILES(q) {
+                    const Pair<float> d = SpF{P.x32}.ld(q.x);
+                    Pair<double> xv = SpD{P.x, V}.ld(q.x);
+                    xv.a = xv.a + inv_s * to_d(d.a);
+                    xv.b = xv.b + inv_s * to_d(d.b);
+                    st_d(P.x, V, q.x, xv);
+                    st_f(P.x32, q.x, Pair<float>{make_float2(0, 0), make_float2(0, 0)});
+                }
+                if (!gs.sync()) goto done;
+                FOR_TILES(q) st_d(t64, V, q.x, g5dw_at<double>(SpD{P.x, V}, L, q, m2));
+                if (!gs.sync()) goto done;
+                double w[1] = {0.0};
+                FOR_TILES(q) {
+                    const Pair<double> xc = SpD{P.x, V}.ld(q.x);
+                    const Pair<double> a = g5dw_at<double>(SpD{t64, V}, L, q, m2);
+                    Pair<double> r;
+                    r.a = __ldg(P.b + q.x) - (a.a + mu2 * xc.a);
+                    r.b = __ldg(P.b + q.x + V) - (a.b + mu2 * xc.b);
+                    st_d(P.r, V, q.x, r);
+                    w[0] += norm2(r.a) + norm2(r.b);
+                }
+                if (!reduce_sync<1>(gs, w, P.part, smem)) goto done;
+                const double rrt = w[0];
+                rr64 = rrt;
+                if (rrt < tol) { conv = true; break; }
+                if (k == P.maxiter) break;
+                const double s_new = 1.0 / sqrt(rrt);
+                w[0] = 0.0;
+                FOR_TILES(q) {
+                    const Pair<float> r32{to_f(s_new * P.r[q.x]), to_f(s_new * P.r[q.x + V])};
+                    st_f(P.r32, q.x, r32);
+                    w[0] += (double)(norm2(r32.a) + norm2(r32.b));
+                }
+                if (!reduce_sync<1>(gs, w, P.part, smem)) goto done;
+                beta = (rrt * s * s / rr) * (s_new / s);
+                s = s_new;
+                rr = w[0];
+                maxrr = rr;
+            } else {
+                beta = rn / rr;
+                rr = rn;
+                rr64 = rn / (s * s);
+            }
+            first = false;
+            cur ^= 1;
+        }
+        if (!conv) k = P.maxiter;
+    }
+done:
+    finish_solve(P, k, conv, rr64, bb, nupd);
+}
+
+// ---------------------------------------------------------------------------
+// FP64 multi-shift CG (one Krylov space for all shifts).  The base system is
+// the smallest shift; shift i uses the collinear-residual recurrences
+//   z_{k+1} = z_k z_{k-1} a_{k-1} / (a_k b_{k-1} (z_{k-1} - z_k) + z_{k-1} a_{k-1} (1 + d_i a_k))
+//   a^i_k = a_k z_{k+1}/z_k,  b^i_k = b_k (z_{k+1}/z_k)^2,
+//   x_i += a^i_k p_i,  p_i <- z_{k+1} r_{k+1} + b^i_k p_i
+// (B. Jegerlehner, "Krylov space solvers for shifted linear systems",
+// hep-lat/9612014), d_i = mu_i^2 - mu_base^2.  Shift i is frozen once
+// |z|^2 |r|^2 < eps |b|^2; the x_i update of step k is applied in phase A of
+// step k+1, before p_i is overwritten.
+struct MSP {
+    Lat g;
+    const double2* U;
+    const double2* b;
+    double2* r;
+    double2* p0;
+    double2* p1;
+    double2* t;
+    double2* x[kMaxShifts];
+    double2* ps[kMaxShifts];
+    double d[kMaxShifts];
+    int n;
+    int base;
+    double m2;
+    double mu2b;
+    double eps;
+    int maxiter;
+    DevCtl* ctl;
+    double* part;
+};
+
+__global__ void __launch_bounds__(TILE) k_cg_multishift(const MSP P) {
+    __shared__ double smem[32 * 2];
+    __shared__ double z[kMaxShifts], zp[kMaxShifts], ai[kMaxShifts], bi[kMaxShifts];
+    __shared__ int upd[kMaxShifts], act[kMaxShifts];
+    GridSync gs{&P.ctl->bar, &P.ctl->err, 0};
+    const long long ntiles = num_tiles(P.g), V = P.g.V;
+    const LkD L{P.U, V};
+    const double m2 = P.m2, mu2 = P.mu2b;
+    int k = 0;
+    bool conv = false;
+    double rr = 0.0, bb = 0.0;
+    if (threadIdx.x < kMaxShifts) {
+        z[threadIdx.x] = 1.0; zp[threadIdx.x] = 1.0; ai[threadIdx.x] = 0.0; bi[threadIdx.x] = 0.0;
+        upd[threadIdx.x] = 0; act[threadIdx.x] = threadIdx.x < P.n;
+    }
+    {
+        double v[1] = {0.0};
+        FOR_TILES(q) {
+            const Pair<double> bv{__ldg(P.b + q.x), __ldg(P.b + q.x + V)};
+            v[0] += norm2(bv.a) + norm2(bv.b);
+            st_d(P.r, V, q.x, bv);
+            for (int i = 0; i < P.n; i++) st_d(P.x[i], V, q.x, Pair<double>{make_double2(0, 0), make_double2(0, 0)});
+        }
+        if (!reduce_sync<1>(gs, v, P.part, smem)) goto done;
+        bb = v[0];
+    }
+    if (bb == 0.0) { conv = true; goto done; }
+    {
+        const double tol = P.eps * bb;
+        rr = bb;
+        double beta = 0.0, alpha_prev = 1.0;
+        for (k = 1; k <= P.maxiter; k++) {
+            double2* pn = (k & 1) ? P.p0 : P.p1;
+            const double2* po = (k & 1) ? P.p1 : P.p0;
+            const SpAxpy<double, SpD> Q{SpD{P.r, V}, SpD{po, V}, beta, k > 1};
+            double v[1] = {0.0};
+            FOR_TILES(q) {
+                const Pair<double> c = Q.ld(q.x);
+                const Pair<double> tt = g5dw_at_c<double>(Q, c, L, q, m2);
+                st_d(pn, V, q.x, c);
+                st_d(P.t, V, q.x, tt);
+                v[0] += norm2(tt.a) + norm2(tt.b) + mu2 * (norm2(c.a) + norm2(c.b));
+                const Pair<double> rc = SpD{P.r, V}.ld(q.x);
+                for (int i = 0; i < P.n; i++) {
+                    if (i == P.base) continue;
+                    if (upd[i]) {   // x_i += a^i_{k-1} p_i^{k-1}
+                        const Pair<double> pi = SpD{P.ps[i], V}.ld(q.x);
+                        Pair<double> xi = SpD{P.x[i], V}.ld(q.x);
+                        xi.a = xi.a + ai[i] * pi.a;
+                        xi.b = xi.b + ai[i] * pi.b;
+                        st_d(P.x[i], V, q.x, xi);
+                        if (act[i]) {
+                            Pair<double> pnew;
+                            pnew.a = z[i] * rc.a + bi[i] * pi.a;
+                            pnew.b = z[i] * rc.b + bi[i] * pi.b;
+                            st_d(P.ps[i], V, q.x, pnew);
+                        }
+                    } else if (k == 1) {
+                        st_d(P.ps[i], V, q.x, rc);
+                    }
+                }
+            }
+            if (!reduce_sync<1>(gs, v, P.part, smem)) goto done;
+            const double alpha = rr / v[0];
+            v[0] = 0.0;
+            FOR_TILES(q) {
+                const Pair<double> pc = SpD{pn, V}.ld(q.x);
+                const Pair<double> a = g5dw_at<double>(SpD{P.t, V}, L, q, m2);
+                Pair<double> xb = SpD{P.x[P.base], V}.ld(q.x), r = SpD{P.r, V}.ld(q.x);
+                xb.a = xb.a + alpha * pc.a;
+                xb.b = xb.b + alpha * pc.b;
+                r.a = r.a - alpha * (a.a + mu2 * pc.a);
+                r.b = r.b - alpha * (a.b + mu2 * pc.b);
+                st_d(P.x[P.base], V, q.x, xb);
+                st_d(P.r, V, q.x, r);
+                v[0] += norm2(r.a) + norm2(r.b);
+            }
+            if (!reduce_sync<1>(gs, v, P.part, smem)) goto done;
+            const double rn = v[0];
+            const double beta_new = rn / rr;
+            // shift scalars (identical in every block)
+            if (threadIdx.x < P.n && threadIdx.x != P.base) {
+                const int i = threadIdx.x;
+                if (act[i]) {
+                    const double zk = z[i], zkm = zp[i];
+                    const double znew = zk * zkm * alpha_prev /
+                                        (alpha * beta * (zkm - zk) + zkm * alpha_prev * (1.0 + P.d[i] * alpha));
+                    ai[i] = alpha * znew / zk;
+                    bi[i] = beta_new * (znew / zk) * (znew / zk);
+                    zp[i] = zk;
+                    z[i] = znew;
+                    upd[i] = 1;
+                    if (znew * znew * rn < tol) act[i] = 0;
+                } else {
+                    upd[i] = 0;
+                }
+            }
+            __syncthreads();
+            alpha_prev = alpha;
+            beta = beta_new;
+            rr = rn;
+            if (rn < tol) { conv = true; break; }
+        }
+        if (!conv) k = P.maxiter;
+        // final x_i updates of the last step
+        if (!gs.sync()) goto done;
+        FOR_TILES(q) {
+            for (int i = 0; i < P.n; i++) {
+                if (i == P.base || !upd[i]) continue;
+                const Pair<double> pi = SpD{P.ps[i], V}.ld(q.x);
+                Pair<double> xi = SpD{P.x[i], V}.ld(q.x);
+                xi.a = xi.a + ai[i] * pi.a;
+                xi.b = xi.b + ai[i] * pi.b;
+                st_d(P.x[i], V, q.x, xi);
+            }
+        }
+    }
+done:
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        DevCtl* c = P.ctl;
+        const int err = ld_volatile_int(&c->err);
+        c->last_iters = k;
+        c->last_updates = 0;
+        c->last_conv = conv && !err;
+        c->last_relres = bb > 0.0 ? rr / bb : 0.0;
+        c->iters_total += k;
+        if (c->status == 0) {
+            if (err) c->status = QED2D_ERR_TIMEOUT;
+            else if (!conv) c->status = QED2D_ERR_NOT_CONVERGED;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+template <class K>
+static int coop_grid(Ctx& c, K kernel, int* grid) {
+    int per_sm = 0;
+    QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, TILE, 0));
+    if (per_sm < 1) return QED2D_ERR_UNSUPPORTED;
+    long long g = (long long)per_sm * c.num_sms;
+    const long long nt = num_tiles(c.g);
+    if (g > nt) g = nt;
+    if (g > kMaxPartBlocks) g = kMaxPartBlocks;
+    *grid = (int)g;
+    return QED2D_OK;
+}
+
+static int reset_barrier(Ctx& c) {
+    QCHECK(cudaMemsetAsync(&c.ctl->bar, 0, sizeof(unsigned long long) + sizeof(int), c.stream));
+    return QED2D_OK;
+}
+
+template <class K, class Par>
+static int launch_coop(Ctx& c, K kernel, const Par& P) {
+    int grid = 0;
+    QTRY(coop_grid(c, kernel, &grid));
+    QTRY(reset_barrier(c));
+    void* args[] = {(void*)&P};
+    QCHECK(cudaLaunchCooperativeKernel((const void*)kernel, dim3(grid), dim3(TILE), args, 0, c.stream));
+    count_launch();
+    return QED2D_OK;
+}
+
+static int solve_plain(Ctx& c, const SolveArgs& a);
+
+int cg_solve(Ctx& c, const SolveArgs& a, int precision) {
+    if (precision == QED2D_PREC_PLAIN) return solve_plain(c, a);
+    CGP P{};
+    P.g = c.g;
+    P.U = a.U;
+    P.b = a.b;
+    P.x = a.x;
+    P.r = c.spinor("cg_r");
+    P.t = c.spinor("cg_t");
+    P.g5x = a.g5x;
+    P.m2 = 2.0 + a.am0;
+    P.mu2 = a.mu2;
+    P.eps = a.eps;
+    P.maxiter = a.maxiter;
+    P.guess = a.guess ? 1 : 0;
+    P.ctl = c.ctl;
+    P.part = c.part;
+    P.delta2 = 0.05 * 0.05;
+    if (precision == QED2D_PREC_F64) {
+        P.p0 = c.spinor("cg_p0");
+        P.p1 = c.spinor("cg_p1");
+        return launch_coop(c, k_cg_f64, P);
+    }
+    P.r32 = c.spinor32("cg_r32");
+    P.q0 = c.spinor32("cg_q0");
+    P.q1 = c.spinor32("cg_q1");
+    P.t32 = c.spinor32("cg_t32");
+    P.x32 = c.spinor32("cg_x32");
+    if (a.U32) {
+        P.U32 = a.U32;
+    } else {
+        float4* u32 = c.spinor32("cg_u32");
+        QTRY(launch_pack_links(c, u32, a.U));
+        P.U32 = u32;
+    }
+    return launch_coop(c, k_cg_mixed, P);
+}
+
+int multishift_solve(Ctx& c, const double2* U, const double2* b, double2* const* x, const double* mu2, int n,
+                     double am0, int maxiter, double eps) {
+    if (n < 1 || n > kMaxShifts) return QED2D_ERR_BAD_ARG;
+    MSP P{};
+    P.g = c.g;
+    P.U = U;
+    P.b = b;
+    P.r = c.spinor("ms_r");
+    P.p0 = c.spinor("ms_p0");
+    P.p1 = c.spinor("ms_p1");
+    P.t = c.spinor("ms_t");
+    int base = 0;
+    for (int i = 1; i < n; i++)
+        if (mu2[i] < mu2[base]) base = i;
+    for (int i = 0; i < n; i++) {
+        P.x[i] = x[i];
+        P.ps[i] = i == base ? nullptr : c.spinor("ms_p_" + std::to_string(i));
+        P.d[i] = mu2[i] - mu2[base];
+    }
+    P.n = n;
+    P.base = base;
+    P.m2 = 2.0 + am0;
+    P.mu2b = mu2[base];
+    P.eps = eps;
+    P.maxiter = maxiter;
+    P.ctl = c.ctl;
+    P.part = c.part;
+    return launch_coop(c, k_cg_multishift, P);
+}
+
+// ---------------------------------------------------------------------------
+// QED2D_PREC_PLAIN: the reference's CG loop structure (src/QED2dSolver.jl:49-105)
+// on the GPU -- operator as two gamm5Dw launches, BLAS-1 launches, and the host
+// reading <p,Ap> and |r|^2 back every iteration.
+static int read_scal(Ctx& c, int slot, int n, double* out) {
+    QCHECK(cudaMemcpyAsync(out, &c.ctl->scal[slot], sizeof(double) * n, cudaMemcpyDeviceToHost, c.stream));
+    QCHECK(cudaStreamSynchronize(c.stream));
+    return QED2D_OK;
+}
+
+static int plain_op(Ctx& c, double2* Ap, double2* tmp, const double2* U, const double2* p, double am0, double mu2) {
+    QTRY(launch_g5dw(c, tmp, U, p, am0, nullptr, make_double2(0, 0), false));
+    return launch_g5dw(c, Ap, U, tmp, am0, mu2 != 0.0 ? p : nullptr, make_double2(mu2, 0), false);
+}
+
+static int solve_plain(Ctx& c, const SolveArgs& a) {
+    const long long n = 2 * c.g.V;
+    double2* r = c.spinor("pl_r");
+    double2* p = c.spinor("pl_p");
+    double2* Ap = c.spinor("pl_Ap");
+    double2* tmp = c.spinor("pl_tmp");
+    const double2 one = make_double2(1, 0), zero = make_double2(0, 0);
+    double h[2];
+    QTRY(launch_reduce_vec(c, 0, a.b, nullptr, n, 0));
+    QTRY(read_scal(c, 0, 1, h));
+    const double bb = h[0], tol = a.eps * bb;
+    int iters = 0;
+    bool conv = false;
+    double err = 0.0, norm, final_rr = 0.0;
+    if (bb == 0.0) {
+        QTRY(launch_zero(c, a.x, sizeof(double2) * n));
+        conv = true;
+        norm = 0.0;
+    } else if (!a.guess) {
+        QTRY(launch_zero(c, a.x, sizeof(double2) * n));
+        QTRY(launch_copy(c, r, a.b, sizeof(double2) * n));
+        QTRY(launch_copy(c, p, a.b, sizeof(double2) * n));
+        norm = bb;
+    } else {
+        QTRY(plain_op(c, Ap, tmp, a.U, a.x, a.am0, a.mu2));
+        QTRY(launch_zaxpby(c, r, one, a.b, make_double2(-1, 0), Ap, n));
+        QTRY(launch_copy(c, p, r, sizeof(double2) * n));
+        QTRY(launch_reduce_vec(c, 0, r, nullptr, n, 0));
+        QTRY(read_scal(c, 0, 1, h));
+        norm = h[0];
+        final_rr = norm;
+        if (norm < tol) conv = true;
+    }
+    if (!conv) {
+        for (int i = 1; i <= a.maxiter; i++) {
+            QTRY(plain_op(c, Ap, tmp, a.U, p, a.am0, a.mu2));
+            QTRY(launch_reduce_vec(c, 1, p, Ap, n, 0));
+            QTRY(read_scal(c, 0, 2, h));
+            // alpha = norm / prod (complex), Smith's division
+            double2 alpha;
+            {
+                const double br = h[0], bi = h[1];
+                if (fabs(br) >= fabs(bi)) {
+                    const double t = bi / br, den = br + bi * t;
+                    alpha = make_double2(norm / den, (-norm * t) / den);
+                } else {
+                    const double t = br / bi, den = bi + br * t;
+                    alpha = make_double2((norm * t) / den, -norm / den);
+                }
+            }
+            QTRY(launch_zaxpby(c, a.x, one, a.x, alpha, p, n));
+            QTRY(launch_zaxpby(c, r, one, r, make_double2(-alpha.x, -alpha.y), Ap, n));
+            QTRY(launch_reduce_vec(c, 0, r, nullptr, n, 0));
+            QTRY(read_scal(c, 0, 1, h));
+            err = h[0];
+            final_rr = err;
+            if (err < tol) { iters = i; conv = true; break; }
+            const double beta = err / norm;
+            QTRY(launch_zaxpby(c, p, one, r, make_double2(beta, 0), p, n));
+            norm = err;
+        }
+        if (!conv) iters = a.maxiter;
+    }
+    if (a.g5x) QTRY(launch_g5dw(c, a.g5x, a.U, a.x, a.am0, nullptr, make_double2(0, 0), false));
+    // record in the control block like the persistent solvers do
+    QTRY(read_ctl(c, false));
+    c.ctl_host->last_iters = iters;
+    c.ctl_host->last_updates = 0;
+    c.ctl_host->last_conv = conv;
+    c.ctl_host->last_relres = bb > 0 ? final_rr / bb : 0.0;
+    c.ctl_host->iters_total += iters;
+    if (c.ctl_host->status == 0 && !conv) c.ctl_host->status = QED2D_ERR_NOT_CONVERGED;
+    QCHECK(cudaMemcpyAsync(c.ctl, c.ctl_host, sizeof(DevCtl), cudaMemcpyHostToDevice, c.stream));
+    QCHECK(cudaStreamSynchronize(c.stream));
+    return QED2D_OK;
+}
+
+int read_ctl(Ctx& c, bool reset_sequence) {
+    QCHECK(cudaMemcpyAsync(c.ctl_host, c.ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, c.stream));
+    QCHECK(cudaStreamSynchronize(c.stream));
+    const int st = c.ctl_host->status;
+    c.last_iters = c.ctl_host->last_iters;
+    c.last_updates = c.ctl_host->last_updates;
+    c.last_relres = c.ctl_host->last_relres;
+    if (reset_sequence) {
+        QCHECK(cudaMemsetAsync(&c.ctl->status, 0, sizeof(int), c.stream));
+        QCHECK(cudaMemsetAsync(&c.ctl->iters_total, 0, sizeof(long long), c.stream));
+    }
+    return st;
+}
+
+}  // namespace qed2d

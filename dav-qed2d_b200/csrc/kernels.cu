@@ -1,0 +1,386 @@
+// kernels.cu -- standalone (one tile per block) kernels of libqed2d and their
+// launchers: the reference's device kernels (gamm5Dw, gamm5, tr_dQwdU,
+// plaquette!, qtop!, krnl_force!, updt_fld!, unfold, plwv), the fused momentum
+// kick, random fields, BLAS-1 and deterministic single-launch reductions.
+#include <atomic>
+
+#include "stencil.cuh"
+
+namespace qed2d {
+
+static std::atomic<int64_t> g_launches{0};
+void count_launch(int n) { g_launches += n; }
+int64_t launches() { return g_launches.load(); }
+
+static inline unsigned tiles_grid(const Lat& g) { return (unsigned)num_tiles(g); }
+
+// ---------------------------------------------------------------------------
+// gamm5Dw (src/QED2dDirac.jl:2-33); optionally  so += addc * addv  with complex
+// addc (the mu^2 si term of gamm5Dw_sqr_musq, :92, and the +-i mu terms of
+// generate_pseudofermion!, src/QED2dRHMC.jl:308,317) and optionally so2 *= -1
+// (Dw = g5 (g5 Dw), :157-169)
+__global__ void __launch_bounds__(TILE) k_g5dw(double2* __restrict__ so, const double2* __restrict__ U,
+                                               const double2* __restrict__ si, double m2, Lat g,
+                                               const double2* __restrict__ addv, double2 addc, int g5_out) {
+    const Site q = site_of_tile(g, blockIdx.x, threadIdx.x);
+    if (!q.ok) return;
+    Pair<double> o = g5dw_at<double>(SpDro{si, g.V}, LkD{U, g.V}, q, m2);
+    if (addv) {
+        o.a = o.a + cmul(addc, __ldg(addv + q.x));
+        o.b = o.b + cmul(addc, __ldg(addv + q.x + g.V));
+    }
+    if (g5_out) o.b = -o.b;
+    st_d(so, g.V, q.x, o);
+}
+
+// gamm5 (src/QED2dDirac.jl:130-146)
+__global__ void k_g5(double2* __restrict__ so, const double2* __restrict__ si, long long V) {
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (x >= V) return;
+    so[x] = si[x];
+    so[x + V] = -si[x + V];
+}
+
+// tr_dQwdU (src/QED2dDirac.jl:172-199); frc = [accumulate ? frc : 0] + rho * force
+__global__ void __launch_bounds__(TILE) k_force(double* __restrict__ frc, const double2* __restrict__ U,
+                                                const double2* __restrict__ X, const double2* __restrict__ G,
+                                                Lat g, double rho, int accumulate) {
+    const Site q = site_of_tile(g, blockIdx.x, threadIdx.x);
+    if (!q.ok) return;
+    double f1, f2;
+    fermion_force_at(U, X, G, g.V, q, f1, f2);
+    if (accumulate) {
+        frc[q.x] += rho * f1;
+        frc[q.x + g.V] += rho * f2;
+    } else {
+        frc[q.x] = rho * f1;
+        frc[q.x + g.V] = rho * f2;
+    }
+}
+
+// plaquette! (mode 0, Re P) and qtop! (mode 1, arg P) -- src/QED2dAction.jl:2-32
+__global__ void __launch_bounds__(TILE) k_plaq_field(double* __restrict__ plx, const double2* __restrict__ U, Lat g,
+                                                     int mode) {
+    const Site q = site_of_tile(g, blockIdx.x, threadIdx.x);
+    if (!q.ok) return;
+    const double2 p = plaquette_of(__ldg(U + q.x), __ldg(U + g.V + q.xp1), __ldg(U + q.xp2), __ldg(U + g.V + q.x));
+    plx[q.x] = mode == 0 ? p.x : atan2(p.y, p.x);
+}
+
+// krnl_force! -- src/QED2dAction.jl:34-53: every element of frc1 and frc2 written once
+__global__ void __launch_bounds__(TILE) k_krnl_force(double* __restrict__ frc1, double* __restrict__ frc2,
+                                                     const double2* __restrict__ U, Lat g, double beta) {
+    const Site q = site_of_tile(g, blockIdx.x, threadIdx.x);
+    if (!q.ok) return;
+    const double2 p = plaquette_of(__ldg(U + q.x), __ldg(U + g.V + q.xp1), __ldg(U + q.xp2), __ldg(U + g.V + q.x));
+    const double v = beta * p.y;
+    frc1[q.x] = -v;
+    frc1[q.x + g.V] = v;
+    frc2[q.xp1 + g.V] = -v;
+    frc2[q.xp2] = v;
+}
+
+// updt_fld! -- src/QED2dAction.jl:55-65; also refreshes the packed FP32 copy
+__global__ void k_updt_fld(double2* __restrict__ U, const double* __restrict__ mom, double eps, long long V,
+                           float4* __restrict__ U32) {
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (x >= V) return;
+    double s1, c1, s2, c2;
+    sincos(eps * mom[x], &s1, &c1);
+    sincos(eps * mom[x + V], &s2, &c2);
+    const double2 u1 = cmul(make_double2(c1, s1), U[x]);
+    const double2 u2 = cmul(make_double2(c2, s2), U[x + V]);
+    U[x] = u1;
+    U[x + V] = u2;
+    if (U32) U32[x] = make_float4((float)u1.x, (float)u1.y, (float)u2.x, (float)u2.y);
+}
+
+__global__ void k_pack_links(float4* __restrict__ U32, const double2* __restrict__ U, long long V) {
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (x >= V) return;
+    const double2 u1 = U[x], u2 = U[x + V];
+    U32[x] = make_float4((float)u1.x, (float)u1.y, (float)u2.x, (float)u2.y);
+}
+
+// krnl_unfold! / krnl_reflect! -- src/QED2dFields.jl:12-25,37-50
+__global__ void k_unfold(double2* __restrict__ Uout, const double2* __restrict__ Uin, Lat g, int reflect) {
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (x >= 2 * g.V) return;
+    const int mu = x >= g.V;
+    const long long s = x - mu * g.V;
+    const int i2 = (int)(s / g.L1), i1 = (int)(s - (long long)i2 * g.L1);
+    const long long L1n = 2LL * g.L1, Vout = 4 * g.V;
+    const double2 u = Uin[x];
+    const double2 uc = reflect ? conj(u) : u;
+    double2* o = Uout + mu * Vout;
+    o[i1 + L1n * i2] = u;
+    o[i1 + g.L1 + L1n * i2] = uc;
+    o[i1 + L1n * (i2 + g.L2)] = uc;
+    o[i1 + g.L1 + L1n * (i2 + g.L2)] = u;
+}
+
+// plwv -- src/QED2dUtils.jl:2-11; pref = i sqrt(-sin^2 k1 - sin^2 k2) / (sin k1 + i sin k2)
+__global__ void k_plwv(double2* __restrict__ so, Lat g, double k1, double k2, double2 pref) {
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (x >= g.V) return;
+    const int i2 = (int)(x / g.L1), i1 = (int)(x - (long long)i2 * g.L1);
+    double s, c;
+    sincos(k1 * i1 + k2 * i2, &s, &c);
+    const double2 e = make_double2(c, s);
+    so[x] = cmul(pref, e);
+    so[x + g.V] = e;
+}
+
+// n N(0,1) numbers of (seed, stream, counter), times scale
+__global__ void k_random_normal(double* __restrict__ out, long long n, uint64_t seed, uint32_t stream,
+                                uint32_t counter, double scale) {
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (2 * j >= n) return;
+    double z0, z1;
+    normal_pair(seed, stream, counter, (uint64_t)j, z0, z1);
+    out[2 * j] = scale * z0;
+    if (2 * j + 1 < n) out[2 * j + 1] = scale * z1;
+}
+
+// mom += eps * (frc1 + frc2 [+ fermion force]) -- the kick of OMF4!/update_momenta!
+// (src/QED2dHMC.jl:256,478,554) with krnl_force!'s two scattered buffers gathered
+// per link, so no force arrays are stored.
+__global__ void __launch_bounds__(TILE) k_mom_kick(double* __restrict__ mom, const double2* __restrict__ U, Lat g,
+                                                   double beta, double eps, const double2* __restrict__ X,
+                                                   const double2* __restrict__ G, const double* __restrict__ frc) {
+    const Site q = site_of_tile(g, blockIdx.x, threadIdx.x);
+    if (!q.ok) return;
+    double F1, F2;
+    gauge_force_at(U, g, q, beta, F1, F2);
+    if (X) {
+        double f1, f2;
+        fermion_force_at(U, X, G, g.V, q, f1, f2);
+        F1 = F1 + f1;
+        F2 = F2 + f2;
+    }
+    if (frc) {
+        F1 = F1 + frc[q.x];
+        F2 = F2 + frc[q.x + g.V];
+    }
+    mom[q.x] = mom[q.x] + eps * F1;
+    mom[q.x + g.V] = mom[q.x + g.V] + eps * F2;
+}
+
+// y = a x + b z (complex scalars; z may alias y)
+__global__ void k_zaxpby(double2* y, double2 a, const double2* x, double2 b, const double2* z,
+                         long long n) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double2 v = cmul(a, x[i]);
+    if (z) v = v + cmul(b, z[i]);
+    y[i] = v;
+}
+
+// ---------------------------------------------------------------------------
+// single-launch deterministic reductions: per-block tree sums to part[], the
+// last block to finish sums part[] in a fixed order into ctl->scal[slot..]
+constexpr int RB = 256;
+
+template <int NV>
+__device__ __forceinline__ void finish_reduce(double (&v)[NV], double* part, DevCtl* ctl, int slot) {
+    __shared__ double smem[32 * NV];
+    __shared__ bool last;
+    block_sum<NV>(v, smem);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) part[(size_t)k * kMaxPartBlocks + blockIdx.x] = v[k];
+        __threadfence();
+        last = atomicAdd(&ctl->ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    if (threadIdx.x < 32) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            double s = 0.0;
+            for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) s += __ldcg(part + (size_t)k * kMaxPartBlocks + i);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (threadIdx.x == 0) ctl->scal[slot + k] = s;
+        }
+        if (threadIdx.x == 0) ctl->ticket = 0;
+    }
+}
+
+__global__ void __launch_bounds__(RB) k_reduce_vec(int kind, const double2* __restrict__ x,
+                                                   const double2* __restrict__ y, long long n, double* part,
+                                                   DevCtl* ctl, int slot) {
+    double v[2] = {0.0, 0.0};
+    for (long long i = blockIdx.x * (long long)RB + threadIdx.x; i < n; i += (long long)gridDim.x * RB) {
+        const double2 a = x[i];
+        if (kind == 0) {
+            v[0] += norm2(a);
+        } else {
+            const double2 d = cjmul(a, y[i]);
+            v[0] += d.x;
+            v[1] += d.y;
+        }
+    }
+    finish_reduce<2>(v, part, ctl, slot);
+}
+
+// (sum Re P, sum arg P, sum mom^2) -- Action/Plaquette/Qtop/Hamiltonian (src/QED2dHMC.jl:198-237)
+__global__ void __launch_bounds__(RB) k_reduce_gauge(const double2* __restrict__ U, const double* __restrict__ mom,
+                                                     Lat g, double* part, DevCtl* ctl, int slot) {
+    double v[3] = {0.0, 0.0, 0.0};
+    for (long long x = blockIdx.x * (long long)RB + threadIdx.x; x < g.V; x += (long long)gridDim.x * RB) {
+        const int i2 = (int)(x / g.L1), i1 = (int)(x - (long long)i2 * g.L1);
+        const long long xp1 = (i1 + 1 == g.L1) ? x - (g.L1 - 1) : x + 1;
+        const long long xp2 = (i2 + 1 == g.L2) ? (long long)i1 : x + g.L1;
+        const double2 p = plaquette_of(__ldg(U + x), __ldg(U + g.V + xp1), __ldg(U + xp2), __ldg(U + g.V + x));
+        v[0] += p.x;
+        v[1] += atan2(p.y, p.x);
+        if (mom) v[2] += mom[x] * mom[x] + mom[x + g.V] * mom[x + g.V];
+    }
+    finish_reduce<3>(v, part, ctl, slot);
+}
+
+__global__ void k_copy_scalar(DevCtl* ctl, int dst, int src) { ctl->scal[dst] = ctl->scal[src]; }
+
+// y = x / ctl->scal[slot] (the power method's normalisation, kept on the device)
+__global__ void k_scale_inv(double2* y, const double2* x, long long n, const DevCtl* __restrict__ ctl, int slot) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double d = ctl->scal[slot];
+    y[i] = make_double2(x[i].x / d, x[i].y / d);
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+static int post_launch(const char* name) {
+    count_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_status(e, name);
+    return QED2D_OK;
+}
+
+static unsigned blocks_for(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+static unsigned reduce_grid(long long n) {
+    long long b = (n + RB - 1) / RB;
+    if (b > 4 * 148) b = 4 * 148;
+    if (b < 1) b = 1;
+    return (unsigned)b;
+}
+
+int launch_g5dw(Ctx& c, double2* so, const double2* U, const double2* si, double am0, const double2* addv,
+                double2 addc, bool g5_out) {
+    k_g5dw<<<tiles_grid(c.g), TILE, 0, c.stream>>>(so, U, si, 2.0 + am0, c.g, addv, addc, g5_out ? 1 : 0);
+    return post_launch("k_g5dw");
+}
+
+int launch_g5(Ctx& c, double2* so, const double2* si) {
+    k_g5<<<blocks_for(c.g.V, 256), 256, 0, c.stream>>>(so, si, c.g.V);
+    return post_launch("k_g5");
+}
+
+int launch_tr_dqwdu(Ctx& c, double* frc, const double2* U, const double2* X, const double2* G) {
+    k_force<<<tiles_grid(c.g), TILE, 0, c.stream>>>(frc, U, X, G, c.g, 1.0, 0);
+    return post_launch("k_force");
+}
+
+int launch_force_accum(Ctx& c, double* frc, const double2* U, const double2* X, const double2* G, double rho,
+                       bool accumulate) {
+    k_force<<<tiles_grid(c.g), TILE, 0, c.stream>>>(frc, U, X, G, c.g, rho, accumulate ? 1 : 0);
+    return post_launch("k_force");
+}
+
+int launch_plaq_field(Ctx& c, double* plx, const double2* U, int mode) {
+    k_plaq_field<<<tiles_grid(c.g), TILE, 0, c.stream>>>(plx, U, c.g, mode);
+    return post_launch("k_plaq_field");
+}
+
+int launch_krnl_force(Ctx& c, double* frc1, double* frc2, const double2* U) {
+    k_krnl_force<<<tiles_grid(c.g), TILE, 0, c.stream>>>(frc1, frc2, U, c.g, c.beta);
+    return post_launch("k_krnl_force");
+}
+
+int launch_updt_fld(Ctx& c, double2* U, const double* mom, double eps, float4* U32) {
+    k_updt_fld<<<blocks_for(c.g.V, 256), 256, 0, c.stream>>>(U, mom, eps, c.g.V, U32);
+    return post_launch("k_updt_fld");
+}
+
+int launch_pack_links(Ctx& c, float4* U32, const double2* U) {
+    k_pack_links<<<blocks_for(c.g.V, 256), 256, 0, c.stream>>>(U32, U, c.g.V);
+    return post_launch("k_pack_links");
+}
+
+int launch_unfold(Ctx& c, double2* Uout, const double2* Uin, int reflect) {
+    k_unfold<<<blocks_for(2 * c.g.V, 256), 256, 0, c.stream>>>(Uout, Uin, c.g, reflect);
+    return post_launch("k_unfold");
+}
+
+int launch_plwv(Ctx& c, double2* so, double k1, double k2) {
+    // pref = i * sqrt(complex(-s1^2 - s2^2)) / (s1 + i s2); sqrt of a non-positive
+    // real is i*sqrt(|.|), so pref = -sqrt(s1^2 + s2^2) / (s1 + i s2)
+    const double s1 = sin(k1), s2 = sin(k2);
+    const double r = sqrt(s1 * s1 + s2 * s2);
+    double2 pref;
+    // -r / (s1 + i s2) by Smith's scaled division
+    if (fabs(s1) >= fabs(s2)) {
+        const double t = s2 / s1, den = s1 + s2 * t;
+        pref = make_double2(-r / den, (r * t) / den);
+    } else {
+        const double t = s1 / s2, den = s2 + s1 * t;
+        pref = make_double2((-r * t) / den, r / den);
+    }
+    k_plwv<<<blocks_for(c.g.V, 256), 256, 0, c.stream>>>(so, c.g, k1, k2, pref);
+    return post_launch("k_plwv");
+}
+
+int launch_random_normal(Ctx& c, double* out, int64_t n, uint64_t seed, uint32_t stream, uint32_t counter,
+                         double scale) {
+    if (n <= 0) return QED2D_OK;
+    k_random_normal<<<blocks_for((n + 1) / 2, 256), 256, 0, c.stream>>>(out, n, seed, stream, counter, scale);
+    return post_launch("k_random_normal");
+}
+
+int launch_mom_kick(Ctx& c, double* mom, const double2* U, double eps, const double2* X, const double2* G,
+                    const double* frc) {
+    k_mom_kick<<<tiles_grid(c.g), TILE, 0, c.stream>>>(mom, U, c.g, c.beta, eps, X, G, frc);
+    return post_launch("k_mom_kick");
+}
+
+int launch_zaxpby(Ctx& c, double2* y, double2 a, const double2* x, double2 b, const double2* z, long long n) {
+    k_zaxpby<<<blocks_for(n, 256), 256, 0, c.stream>>>(y, a, x, b, z, n);
+    return post_launch("k_zaxpby");
+}
+
+int launch_copy(Ctx& c, void* dst, const void* src, size_t bytes) {
+    if (dst == src || bytes == 0) return QED2D_OK;
+    QCHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, c.stream));
+    return QED2D_OK;
+}
+
+int launch_zero(Ctx& c, void* dst, size_t bytes) {
+    QCHECK(cudaMemsetAsync(dst, 0, bytes, c.stream));
+    return QED2D_OK;
+}
+
+int launch_reduce_vec(Ctx& c, int kind, const double2* x, const double2* y, long long n, int slot) {
+    k_reduce_vec<<<reduce_grid(n), RB, 0, c.stream>>>(kind, x, y, n, c.part, c.ctl, slot);
+    return post_launch("k_reduce_vec");
+}
+
+int launch_reduce_gauge(Ctx& c, const double2* U, const double* mom, int slot) {
+    k_reduce_gauge<<<reduce_grid(c.g.V), RB, 0, c.stream>>>(U, mom, c.g, c.part, c.ctl, slot);
+    return post_launch("k_reduce_gauge");
+}
+
+int launch_scale_inv(Ctx& c, double2* y, const double2* x, long long n, int slot) {
+    k_scale_inv<<<blocks_for(n, 256), 256, 0, c.stream>>>(y, x, n, c.ctl, slot);
+    return post_launch("k_scale_inv");
+}
+
+int launch_copy_scalar(Ctx& c, int dst_slot, int src_slot) {
+    k_copy_scalar<<<1, 1, 0, c.stream>>>(c.ctl, dst_slot, src_slot);
+    return post_launch("k_copy_scalar");
+}
+
+}  // namespace qed2d

@@ -1,0 +1,159 @@
+// stencil.cuh -- lattice geometry, field accessors and the stencil/force
+// evaluators used by both the standalone kernels and the persistent solvers.
+//
+// Sites are visited in tiles of TX x TY = 32 x 8 (i1 fastest): a warp covers 32
+// consecutive i1 of one row, so every plane load of a warp is one contiguous
+// 512-byte segment, and the rows i2 +- 1 of a tile are read by the same block.
+#pragma once
+
+#include "device.cuh"
+#include "internal.h"
+
+namespace qed2d {
+
+constexpr int TX = 32;
+constexpr int TY = 8;
+constexpr int TILE = TX * TY;
+
+struct Site {
+    int i1, i2;
+    long long x, xp1, xm1, xp2, xm2;
+    bool ok;
+};
+
+// neighbours with periodic wrap (src/QED2dDirac.jl:7-11)
+__device__ __forceinline__ Site site_of_tile(const Lat& g, long long tile, int t) {
+    const int nt1 = (g.L1 + TX - 1) / TX;
+    const long long t2 = tile / nt1;
+    const int t1 = (int)(tile - t2 * nt1);
+    Site s;
+    s.i1 = t1 * TX + (t & (TX - 1));
+    s.i2 = (int)t2 * TY + (t >> 5);
+    s.ok = s.i1 < g.L1 && s.i2 < g.L2;
+    s.x = s.i1 + (long long)g.L1 * s.i2;
+    s.xp1 = (s.i1 + 1 == g.L1) ? s.x - (g.L1 - 1) : s.x + 1;
+    s.xm1 = (s.i1 == 0) ? s.x + (g.L1 - 1) : s.x - 1;
+    s.xp2 = (s.i2 + 1 == g.L2) ? (long long)s.i1 : s.x + g.L1;
+    s.xm2 = (s.i2 == 0) ? s.x + (g.V - g.L1) : s.x - g.L1;
+    return s;
+}
+
+__host__ __device__ __forceinline__ long long num_tiles(const Lat& g) {
+    return (long long)((g.L1 + TX - 1) / TX) * ((g.L2 + TY - 1) / TY);
+}
+
+// ---------------------------------------------------------------------------
+// spinor accessors
+struct SpD {   // FP64 planes (reference layout): spin k of site x at p[x + k V]
+    const double2* p;
+    long long V;
+    __device__ __forceinline__ Pair<double> ld(long long x) const { return {p[x], p[x + V]}; }
+};
+struct SpDro {   // read-only for the kernel's lifetime: non-coherent path
+    const double2* p;
+    long long V;
+    __device__ __forceinline__ Pair<double> ld(long long x) const { return {__ldg(p + x), __ldg(p + x + V)}; }
+};
+__device__ __forceinline__ void st_d(double2* p, long long V, long long x, const Pair<double>& v) {
+    p[x] = v.a;
+    p[x + V] = v.b;
+}
+struct SpF {   // FP32 packed: (s1, s2) of site x in one float4
+    const float4* p;
+    __device__ __forceinline__ Pair<float> ld(long long x) const {
+        const float4 q = p[x];
+        return {make_float2(q.x, q.y), make_float2(q.z, q.w)};
+    }
+};
+__device__ __forceinline__ void st_f(float4* p, long long x, const Pair<float>& v) {
+    p[x] = make_float4(v.a.x, v.a.y, v.b.x, v.b.y);
+}
+// q = r + beta p, evaluated on load (p skipped when beta == 0)
+template <typename R, class A>
+struct SpAxpy {
+    A r, p;
+    R beta;
+    bool use_p;
+    __device__ __forceinline__ Pair<R> ld(long long x) const {
+        Pair<R> v = r.ld(x);
+        if (use_p) {
+            const Pair<R> w = p.ld(x);
+            v.a = v.a + beta * w.a;
+            v.b = v.b + beta * w.b;
+        }
+        return v;
+    }
+};
+
+// link accessors
+struct LkD {
+    const double2* U;
+    long long V;
+    __device__ __forceinline__ double2 u1(long long x) const { return __ldg(U + x); }
+    __device__ __forceinline__ double2 u2(long long x) const { return __ldg(U + V + x); }
+};
+struct LkF {
+    const float4* U;
+    __device__ __forceinline__ float2 u1(long long x) const {
+        const float4 q = __ldg(U + x);
+        return make_float2(q.x, q.y);
+    }
+    __device__ __forceinline__ float2 u2(long long x) const {
+        const float4 q = __ldg(U + x);
+        return make_float2(q.z, q.w);
+    }
+};
+
+// gamma5 Dw applied at one site
+template <typename R, class S, class L>
+__device__ __forceinline__ Pair<R> g5dw_at(const S& s, const L& U, const Site& q, R m2) {
+    const Pair<R> c = s.ld(q.x), p1 = s.ld(q.xp1), m1 = s.ld(q.xm1), p2 = s.ld(q.xp2), mm2 = s.ld(q.xm2);
+    Pair<R> o;
+    g5dw_site<R>(c.a, c.b, p1.a, p1.b, m1.a, m1.b, p2.a, p2.b, mm2.a, mm2.b, U.u1(q.x), U.u2(q.x), U.u1(q.xm1),
+                 U.u2(q.xm2), m2, o.a, o.b);
+    return o;
+}
+
+// gamma5 Dw at one site with the centre value already known (saves a load)
+template <typename R, class S, class L>
+__device__ __forceinline__ Pair<R> g5dw_at_c(const S& s, const Pair<R>& c, const L& U, const Site& q, R m2) {
+    const Pair<R> p1 = s.ld(q.xp1), m1 = s.ld(q.xm1), p2 = s.ld(q.xp2), mm2 = s.ld(q.xm2);
+    Pair<R> o;
+    g5dw_site<R>(c.a, c.b, p1.a, p1.b, m1.a, m1.b, p2.a, p2.b, mm2.a, mm2.b, U.u1(q.x), U.u2(q.x), U.u1(q.xm1),
+                 U.u2(q.xm2), m2, o.a, o.b);
+    return o;
+}
+
+// v(y) = Im P(y) for the gauge force (src/QED2dAction.jl:42-45, without beta)
+__device__ __forceinline__ double im_plaq(const double2* U, const Lat& g, int i1, int i2) {
+    const long long V = g.V;
+    const int iu1 = (i1 + 1 == g.L1) ? 0 : i1 + 1;
+    const int iu2 = (i2 + 1 == g.L2) ? 0 : i2 + 1;
+    const long long x = i1 + (long long)g.L1 * i2;
+    const double2 p = plaquette_of(__ldg(U + x), __ldg(U + V + iu1 + (long long)g.L1 * i2),
+                                   __ldg(U + i1 + (long long)g.L1 * iu2), __ldg(U + V + x));
+    return p.y;
+}
+
+// total gauge force on the two links of site y: frc1+frc2 of krnl_force!
+//   F1(y) = -v(y) + v(y-2),  F2(y) = v(y) - v(y-1)
+__device__ __forceinline__ void gauge_force_at(const double2* U, const Lat& g, const Site& q, double beta,
+                                               double& F1, double& F2) {
+    const int im1 = (q.i1 == 0) ? g.L1 - 1 : q.i1 - 1;
+    const int im2 = (q.i2 == 0) ? g.L2 - 1 : q.i2 - 1;
+    const double v = beta * im_plaq(U, g, q.i1, q.i2);
+    const double vm2 = beta * im_plaq(U, g, q.i1, im2);
+    const double vm1 = beta * im_plaq(U, g, im1, q.i2);
+    F1 = -v + vm2;
+    F2 = v - vm1;
+}
+
+// fermion force at one site from (X, G) planes
+__device__ __forceinline__ void fermion_force_at(const double2* U, const double2* X, const double2* G,
+                                                 long long V, const Site& q, double& f1, double& f2) {
+    force_site<double>(__ldg(U + q.x), __ldg(U + V + q.x), X[q.x], X[q.x + V], G[q.x], G[q.x + V], X[q.xp1],
+                       X[q.xp1 + V], G[q.xp1], G[q.xp1 + V], X[q.xp2], X[q.xp2 + V], G[q.xp2], G[q.xp2 + V], f1,
+                       f2);
+}
+
+}  // namespace qed2d

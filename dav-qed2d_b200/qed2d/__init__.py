@@ -1,0 +1,553 @@
+"""qed2d -- Python host API of libqed2d, mirroring the reference's Julia module
+``QED2d`` (src/QED2d.jl:27-54) name for name.
+
+Conventions
+* Fields are CUDA ``torch`` tensors in the reference's memory layout: a Julia
+  ``CuArray{ComplexF64}(L1, L2, 2)`` is a contiguous ``complex128`` tensor of
+  shape ``(2, L2, L1)``; ``Float64(L1, L2, 2)`` is ``float64`` ``(2, L2, L1)`` and
+  a per-site ``Float64(L1, L2)`` is ``(L2, L1)``.
+* Julia's mutating ``f!`` is Python's ``f_`` (``HMC!`` -> ``HMC_``,
+  ``plaquette!`` -> ``plaquette_``).  Kernels the reference launches with
+  ``CUDA.@cuda threads= blocks= f(args)`` are plain calls ``f(args)`` here;
+  ``KernelParm`` is accepted everywhere and ignored (launch geometry is chosen
+  by the library).
+* Errors: CG non-convergence raises ``Qed2dError`` (the reference calls
+  ``error``, src/QED2dSolver.jl:39-43, 98-102).
+* Random numbers: the reference draws from CURAND's and Julia's global
+  generators.  Here every draw comes from Philox4x32-10 keyed by the module's
+  seed (``seed(s)``, the role of ``Random.seed!``) and a counter that advances
+  once per HMC step / power method / reweighting call.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+from typing import List, Sequence
+
+import torch
+
+from . import _lib
+from ._lib import Qed2dError, check, lib
+
+__all__ = [
+    "LattParm", "KernelParm", "RHMCParm", "Integrators", "Leapfrog", "OMF4",
+    "plaquette_", "qtop_", "updt_fld_", "krnl_force_",
+    "HMC_", "Hamiltonian", "Action", "Plaquette", "Qtop", "OMF4_", "leapfrog_", "update_momenta_",
+    "unfold_fld_", "unfold_reflect_",
+    "gamm5Dw", "gamm5Dw_sqr", "gamm5Dw_sqr_msq", "tr_dQwdU", "gamm5Dw_sqr_musq", "gamm5Dw_sqr_sqr_musq",
+    "gamm5Dw_sqr_sqr", "gamm5", "Dw", "CG", "save_gauge", "load_gauge", "get_rhmc_params", "power_method",
+    "reweighting_factor", "R", "MultiCG", "generate_pseudofermion_", "plwv", "LuscherZ",
+    "seed", "set_precision", "Qed2dError", "cfield", "rfield", "context",
+]
+
+
+# ---------------------------------------------------------------------------
+# parameter types (src/QED2d.jl:5-26, src/integrators/integrators.jl:1-3)
+@dataclass(frozen=True)
+class LattParm:
+    iL: tuple
+    beta: float
+
+
+@dataclass(frozen=True)
+class KernelParm:
+    threads: tuple = (1, 1)
+    blocks: tuple = (1, 1)
+
+
+@dataclass
+class RHMCParm:
+    r_b: float
+    n: int
+    eps: float
+    A: float
+    rho: List[float]
+    mu: List[float]
+    nu: List[float]
+    delta: float
+    reweighting_N: int = 1
+    reweighting_Taylor: int = 5
+
+    def to_c(self) -> _lib.RhmcParams:
+        p = _lib.RhmcParams()
+        p.r_b, p.n, p.eps, p.A, p.delta = self.r_b, self.n, self.eps, self.A, self.delta
+        p.reweighting_N, p.reweighting_Taylor = self.reweighting_N, self.reweighting_Taylor
+        for i in range(self.n):
+            p.rho[i], p.mu[i], p.nu[i] = self.rho[i], self.mu[i], self.nu[i]
+        return p
+
+    @staticmethod
+    def from_c(p: _lib.RhmcParams) -> "RHMCParm":
+        n = p.n
+        return RHMCParm(p.r_b, n, p.eps, p.A, list(p.rho[:n]), list(p.mu[:n]), list(p.nu[:n]), p.delta,
+                        p.reweighting_N, p.reweighting_Taylor)
+
+
+class Integrators:
+    pass
+
+
+class Leapfrog(Integrators):
+    code = _lib.LEAPFROG
+
+
+class OMF4(Integrators):
+    code = _lib.OMF4
+
+
+# ---------------------------------------------------------------------------
+# contexts, RNG state, precision
+_ctx = {}
+_rng = {"seed": 1234, "counter": 0}
+_precision = {"value": _lib.PREC_F64}
+
+
+def seed(s: int) -> None:
+    """Random.seed! for the library's draws: reset the Philox key and counter."""
+    _rng["seed"] = int(s) & 0xFFFFFFFFFFFFFFFF
+    _rng["counter"] = 0
+
+
+def _next_counter() -> int:
+    c = _rng["counter"]
+    _rng["counter"] = (c + 1) & 0xFFFFFFFF
+    return c
+
+
+def set_precision(p) -> None:
+    """Solver path of every CG: "f64" (default), "mixed" (FP32 inner, FP64
+    reliable updates, FP64 stop rule) or "plain" (reference-structured)."""
+    m = {"f64": _lib.PREC_F64, "mixed": _lib.PREC_MIXED, "plain": _lib.PREC_PLAIN}
+    _precision["value"] = m[p] if isinstance(p, str) else int(p)
+    for h in _ctx.values():
+        check(lib().qed2d_ctx_set_precision(h, _precision["value"]))
+
+
+def context(L1: int, L2: int, beta: float = 0.0):
+    """The library context of an L1 x L2 lattice on the current device (cached)."""
+    dev = torch.cuda.current_device()
+    key = (int(L1), int(L2), dev)
+    h = _ctx.get(key)
+    if h is None:
+        hp = C.c_void_p()
+        check(lib().qed2d_ctx_create(int(L1), int(L2), float(beta), C.byref(hp)), "ctx_create")
+        h = hp.value
+        check(lib().qed2d_ctx_set_precision(h, _precision["value"]))
+        _ctx[key] = h
+    L = lib()
+    check(L.qed2d_ctx_set_beta(h, float(beta)))
+    check(L.qed2d_ctx_set_stream(h, C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    return h
+
+
+def _c(prm: LattParm):
+    return context(prm.iL[0], prm.iL[1], prm.beta)
+
+
+def cfield(L1, L2, device="cuda"):
+    """A zero complex field (spinor or links), Julia CuArray{ComplexF64}(L1, L2, 2)."""
+    return torch.zeros((2, L2, L1), dtype=torch.complex128, device=device)
+
+
+def rfield(L1, L2, device="cuda"):
+    """A zero real field (momenta, forces), Julia CuArray{Float64}(L1, L2, 2)."""
+    return torch.zeros((2, L2, L1), dtype=torch.float64, device=device)
+
+
+def _ptr(t: torch.Tensor, prm: LattParm, dtype, shape=None, name="array"):
+    L1, L2 = prm.iL
+    want = shape or (2, L2, L1)
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError(f"{name}: expected a CUDA tensor")
+    if t.dtype != dtype or tuple(t.shape) != tuple(want) or not t.is_contiguous():
+        raise ValueError(f"{name}: expected contiguous {dtype} of shape {want}, got {t.dtype} {tuple(t.shape)}")
+    return C.c_void_p(t.data_ptr())
+
+
+def _cp(t, prm, name="field"):
+    return _ptr(t, prm, torch.complex128, name=name)
+
+
+def _rp(t, prm, name="field"):
+    return _ptr(t, prm, torch.float64, name=name)
+
+
+def _prm_of(U: torch.Tensor, beta=0.0) -> LattParm:
+    return LattParm((U.shape[2], U.shape[1]), beta)
+
+
+# ---------------------------------------------------------------------------
+# gauge kernels (src/QED2dAction.jl)
+def plaquette_(plx, U, prm: LattParm):
+    """plaquette! (src/QED2dAction.jl:2-16)."""
+    h = _c(prm)
+    check(lib().qed2d_plaquette_field(h, _ptr(plx, prm, torch.float64, (prm.iL[1], prm.iL[0]), "plx"),
+                                      _cp(U, prm, "U")))
+
+
+def qtop_(plx, U, prm: LattParm):
+    """qtop! (src/QED2dAction.jl:18-32)."""
+    h = _c(prm)
+    check(lib().qed2d_qtop_field(h, _ptr(plx, prm, torch.float64, (prm.iL[1], prm.iL[0]), "plx"),
+                                 _cp(U, prm, "U")))
+
+
+def krnl_force_(frc1, frc2, U, prm: LattParm):
+    """krnl_force! (src/QED2dAction.jl:34-53)."""
+    h = _c(prm)
+    check(lib().qed2d_krnl_force(h, _rp(frc1, prm), _rp(frc2, prm), _cp(U, prm, "U")))
+
+
+def updt_fld_(U, mom, eps):
+    """updt_fld! (src/QED2dAction.jl:55-65)."""
+    prm = _prm_of(U)
+    h = _c(prm)
+    check(lib().qed2d_updt_fld(h, _cp(U, prm, "U"), _rp(mom, prm, "mom"), float(eps)))
+
+
+# ---------------------------------------------------------------------------
+# Dirac operator (src/QED2dDirac.jl)
+def gamm5Dw(so, U, si, am0, prm: LattParm, kprm=None):
+    """gamm5Dw (src/QED2dDirac.jl:2-33)."""
+    check(lib().qed2d_gamm5dw(_c(prm), _cp(so, prm), _cp(U, prm), _cp(si, prm), float(am0)), "gamm5Dw")
+
+
+def gamm5(so, si, am0, prm: LattParm, kprm=None):
+    """gamm5 (src/QED2dDirac.jl:130-146)."""
+    check(lib().qed2d_gamm5(_c(prm), _cp(so, prm), _cp(si, prm)), "gamm5")
+
+
+def Dw(so, U, si, am0, prm: LattParm, kprm=None):
+    """Dw (src/QED2dDirac.jl:157-169)."""
+    check(lib().qed2d_dw(_c(prm), _cp(so, prm), _cp(U, prm), _cp(si, prm), float(am0)), "Dw")
+
+
+def gamm5Dw_sqr(so, U, si, am0, prm: LattParm, kprm=None):
+    """gamm5Dw_sqr (src/QED2dDirac.jl:35-46)."""
+    check(lib().qed2d_gamm5dw_sqr(_c(prm), _cp(so, prm), _cp(U, prm), _cp(si, prm), float(am0)), "gamm5Dw_sqr")
+
+
+def gamm5Dw_sqr_sqr(so, U, si, am0, prm: LattParm, kprm=None):
+    """gamm5Dw_sqr_sqr (src/QED2dDirac.jl:48-67)."""
+    check(lib().qed2d_gamm5dw_sqr_sqr(_c(prm), _cp(so, prm), _cp(U, prm), _cp(si, prm), float(am0)))
+
+
+def gamm5Dw_sqr_msq(so, tmp, U, si, am0, prm: LattParm, kprm=None):
+    """gamm5Dw_sqr_msq (src/QED2dDirac.jl:69-81): (g5Dw)^2, no mass term; tmp unused."""
+    gamm5Dw_sqr(so, U, si, am0, prm)
+
+
+def gamm5Dw_sqr_musq(so, tmp, U, si, am0, mu_j, prm: LattParm, kprm=None):
+    """gamm5Dw_sqr_musq (src/QED2dDirac.jl:83-95); tmp unused."""
+    check(lib().qed2d_gamm5dw_sqr_musq(_c(prm), _cp(so, prm), _cp(U, prm), _cp(si, prm), float(am0),
+                                       float(mu_j)))
+
+
+def gamm5Dw_sqr_sqr_musq(so, tmp, U, si, am0, mu_j, prm: LattParm, kprm=None):
+    """gamm5Dw_sqr_sqr_musq (src/QED2dDirac.jl:97-117); tmp unused."""
+    check(lib().qed2d_gamm5dw_sqr_sqr_musq(_c(prm), _cp(so, prm), _cp(U, prm), _cp(si, prm), float(am0),
+                                           float(mu_j)))
+
+
+def tr_dQwdU(frc, U, X, g5DwX, prm: LattParm):
+    """tr_dQwdU (src/QED2dDirac.jl:172-199)."""
+    check(lib().qed2d_tr_dqwdu(_c(prm), _rp(frc, prm), _cp(U, prm), _cp(X, prm), _cp(g5DwX, prm)))
+
+
+# ---------------------------------------------------------------------------
+# CG (src/QED2dSolver.jl): both reference methods, dispatched on the arguments
+#   CG(so, U, si, am0, maxiter, eps, A, prm, kprm)                    method 1
+#   CG(so, U, si, am0, mu, maxiter, eps, A, prm, kprm; so_as_guess)   method 2
+def CG(so, U, si, am0, *args, so_as_guess=False):
+    if len(args) == 5:
+        maxiter, eps, A, prm, kprm = args
+        if A not in (gamm5Dw_sqr_msq, gamm5Dw_sqr):
+            raise ValueError("CG method 1 supports A = gamm5Dw_sqr_msq")
+        it = C.c_int(0)
+        st = lib().qed2d_cg(_c(prm), _cp(so, prm), _cp(U, prm), _cp(si, prm), float(am0), int(maxiter),
+                            float(eps), C.byref(it))
+        if st == _lib.NOT_CONVERGED:
+            raise Qed2dError(st, f"CG not converged after {maxiter} iterationss")
+        check(st, "CG")
+        return it.value
+    if len(args) == 6:
+        mu, maxiter, eps, A, prm, kprm = args
+        if A is not gamm5Dw_sqr_musq:
+            raise ValueError("CG method 2 supports A = gamm5Dw_sqr_musq")
+        it = C.c_int(0)
+        st = lib().qed2d_cg_shift(_c(prm), _cp(so, prm), _cp(U, prm), _cp(si, prm), float(am0), float(mu),
+                                  int(maxiter), float(eps), int(bool(so_as_guess)), C.byref(it))
+        if st == _lib.NOT_CONVERGED:
+            raise Qed2dError(st, f"CG not converged after {maxiter} iterationss")
+        check(st, "CG")
+        return it.value
+    raise TypeError("CG: unsupported argument list")
+
+
+def last_solve(prm: LattParm):
+    """(iterations, |r|^2/|b|^2, reliable updates) of the most recent solve on this lattice."""
+    it, rel, upd = C.c_int64(0), C.c_double(0), C.c_int64(0)
+    check(lib().qed2d_last_solve(_c(prm), C.byref(it), C.byref(rel), C.byref(upd)))
+    return it.value, rel.value, upd.value
+
+
+def multishift_CG(sos: Sequence[torch.Tensor], U, si, am0, mus, maxiter, eps, prm: LattParm):
+    """All shifted solves ((g5Dw)^2 + mu_i^2) so_i = si in one Krylov space."""
+    n = len(mus)
+    ptrs = (C.c_void_p * n)(*[_cp(s, prm).value for s in sos])
+    mu = (C.c_double * n)(*[float(m) for m in mus])
+    it = C.c_int(0)
+    check(lib().qed2d_multishift_cg(_c(prm), ptrs, _cp(U, prm), _cp(si, prm), float(am0), mu, n, int(maxiter),
+                                    float(eps), C.byref(it)), "multishift CG")
+    return it.value
+
+
+# ---------------------------------------------------------------------------
+# observables (src/QED2dHMC.jl:198-237)
+def Action(U, prm: LattParm, kprm=None) -> float:
+    v = C.c_double(0)
+    check(lib().qed2d_action(_c(prm), _cp(U, prm), C.byref(v)))
+    return v.value
+
+
+def Plaquette(U, prm: LattParm, kprm=None) -> float:
+    v = C.c_double(0)
+    check(lib().qed2d_plaquette(_c(prm), _cp(U, prm), C.byref(v)))
+    return v.value
+
+
+def Qtop(U, prm: LattParm, kprm=None) -> float:
+    v = C.c_double(0)
+    check(lib().qed2d_qtop(_c(prm), _cp(U, prm), C.byref(v), None))
+    return v.value
+
+
+def Qtop_rounded(U, prm: LattParm) -> int:
+    q = C.c_int64(0)
+    check(lib().qed2d_qtop(_c(prm), _cp(U, prm), None, C.byref(q)))
+    return q.value
+
+
+def Hamiltonian(mom, U, prm: LattParm, kprm=None) -> float:
+    v = C.c_double(0)
+    check(lib().qed2d_hamiltonian(_c(prm), _rp(mom, prm), _cp(U, prm), C.byref(v)))
+    return v.value
+
+
+# ---------------------------------------------------------------------------
+# fields and utilities
+def unfold_fld_(Uin, prm: LattParm, kprm=None):
+    """unfold_fld! (src/QED2dFields.jl:2-10): returns the (2 L1) x (2 L2) field."""
+    L1, L2 = prm.iL
+    Uout = torch.ones((2, 2 * L2, 2 * L1), dtype=torch.complex128, device=Uin.device)
+    check(lib().qed2d_unfold(_c(prm), C.c_void_p(Uout.data_ptr()), _cp(Uin, prm), 0))
+    return Uout
+
+
+def unfold_reflect_(Uin, prm: LattParm, kprm=None):
+    """unfold_reflect! (src/QED2dFields.jl:27-35)."""
+    L1, L2 = prm.iL
+    Uout = torch.ones((2, 2 * L2, 2 * L1), dtype=torch.complex128, device=Uin.device)
+    check(lib().qed2d_unfold(_c(prm), C.c_void_p(Uout.data_ptr()), _cp(Uin, prm), 1))
+    return Uout
+
+
+def plwv(so, k, prm: LattParm):
+    """plwv (src/QED2dUtils.jl:2-11)."""
+    check(lib().qed2d_plwv(_c(prm), _cp(so, prm), float(k[0]), float(k[1])))
+
+
+def random_normal(n, seed_, stream, counter, device="cuda", prm: LattParm = None):
+    """n N(0,1) numbers of Philox stream (seed, stream, counter), as the library draws them."""
+    out = torch.empty(int(n), dtype=torch.float64, device=device)
+    h = _c(prm) if prm is not None else context(2, 2)
+    check(lib().qed2d_random_normal(h, C.c_void_p(out.data_ptr()), int(n), int(seed_), int(stream), int(counter)))
+    return out
+
+
+def save_gauge(U, file: str, prm: LattParm):
+    """save_gauge (src/QED2dLoadSave.jl:1-10): one 'Re<TAB>Im' line per link,
+    i1 fastest, then i2, then mu (the reference's writedlm of reshape(U, 2V))."""
+    from . import io
+    io.save_gauge_text(U.detach().cpu().numpy(), file)
+
+
+def load_gauge(U, file: str, prm: LattParm):
+    """load_gauge (src/QED2dLoadSave.jl:12-19)."""
+    from . import io
+    arr = io.load_gauge_text(file, prm.iL[0], prm.iL[1])
+    U.copy_(torch.from_numpy(arr).to(U.device))
+
+
+# ---------------------------------------------------------------------------
+# RHMC (src/QED2dRHMC.jl)
+def get_rhmc_params(n_rhmc, r_a_rhmc, r_b_rhmc, reweighting_N=1, reweighting_Taylor=5):
+    """get_rhmc_params (:93-121); list arguments give a list of RHMCParm."""
+    if isinstance(n_rhmc, (list, tuple)):
+        # the reference's array method forwards no keyword arguments (:112-121)
+        return [get_rhmc_params(n, a, b) for n, a, b in zip(n_rhmc, r_a_rhmc, r_b_rhmc)]
+    p = _lib.RhmcParams()
+    check(lib().qed2d_get_rhmc_params(int(n_rhmc), float(r_a_rhmc), float(r_b_rhmc), C.byref(p)), "get_rhmc_params")
+    r = RHMCParm.from_c(p)
+    r.reweighting_N, r.reweighting_Taylor = int(reweighting_N), int(reweighting_Taylor)
+    return r
+
+
+def MultiCG(so, U, si, am0, maxiter, eps, A, rprm: RHMCParm, prm: LattParm, kprm=None):
+    """MultiCG (:281-290)."""
+    it = C.c_int(0)
+    rp = rprm.to_c()
+    check(lib().qed2d_multi_cg(_c(prm), _cp(so, prm), _cp(U, prm), _cp(si, prm), float(am0), int(maxiter),
+                               float(eps), C.byref(rp), C.byref(it)), "MultiCG")
+    return it.value
+
+
+def R(so, U, si, am0, maxiter, eps, A, rprm: RHMCParm, prm: LattParm, kprm=None):
+    """R (:261-271)."""
+    it = C.c_int(0)
+    rp = rprm.to_c()
+    check(lib().qed2d_rational(_c(prm), _cp(so, prm), _cp(U, prm), _cp(si, prm), float(am0), int(maxiter),
+                               float(eps), C.byref(rp), C.byref(it)), "R")
+    return it.value
+
+
+def generate_pseudofermion_(F, U, X, am0, CGmaxiter, CGtol, prm: LattParm, kprm, rprm: RHMCParm):
+    """generate_pseudofermion! (:298-319)."""
+    it = C.c_int(0)
+    rp = rprm.to_c()
+    check(lib().qed2d_generate_pseudofermion(_c(prm), _cp(F, prm), _cp(U, prm), _cp(X, prm), float(am0),
+                                             int(CGmaxiter), float(CGtol), C.byref(rp), C.byref(it)),
+          "generate_pseudofermion!")
+    return it.value
+
+
+def power_method(U, am0, prm: LattParm, kprm=None, iter: int = 1000):
+    """power_method (:135-170): (lambda_min, lambda_max) of (g5Dw)^2."""
+    lmin, lmax = C.c_double(0), C.c_double(0)
+    check(lib().qed2d_power_method(_c(prm), _cp(U, prm), float(am0), int(iter), _rng["seed"], _next_counter(),
+                                   C.byref(lmin), C.byref(lmax)), "power_method")
+    return lmin.value, lmax.value
+
+
+def LuscherZ(Z, U, X_in, am0, CGmaxiter, CGtol, rprm: RHMCParm, prm: LattParm, kprm=None):
+    """LuscherZ (:174-186)."""
+    rp = rprm.to_c()
+    check(lib().qed2d_luscher_z(_c(prm), _cp(Z, prm), _cp(U, prm), _cp(X_in, prm), float(am0), int(CGmaxiter),
+                                float(CGtol), C.byref(rp)), "LuscherZ")
+
+
+def reweighting_factor(U, am0, CGmaxiter, CGtol, prm: LattParm, kprm, rprm):
+    """reweighting_factor (:210-251); list arguments give the product over flavours."""
+    if isinstance(am0, (list, tuple)):
+        w = 1.0
+        for m, r in zip(am0, rprm):
+            w *= reweighting_factor(U, m, CGmaxiter, CGtol, prm, kprm, r)
+        return w
+    W = C.c_double(0)
+    rp = rprm.to_c()
+    check(lib().qed2d_reweighting_factor(_c(prm), _cp(U, prm), float(am0), int(CGmaxiter), float(CGtol),
+                                         C.byref(rp), _rng["seed"], _next_counter(), C.byref(W)),
+          "reweighting_factor")
+    return W.value
+
+
+# ---------------------------------------------------------------------------
+# molecular dynamics (src/QED2dHMC.jl)
+def OMF4_(mom, U, *args):
+    """OMF4! -- pure gauge (:239-305): OMF4_(mom, U, eps, ns, prm, kprm);
+    Nf=2 (:307-422): OMF4_(mom, U, X, F, g5DX, am0, eps, ns, maxiter, tol, prm, kprm)."""
+    if len(args) == 4:
+        eps, ns, prm, kprm = args
+        check(lib().qed2d_omf4_gauge(_c(prm), _rp(mom, prm), _cp(U, prm), float(eps), int(ns)), "OMF4!")
+        return None
+    X, F, g5DX, am0, eps, ns, maxiter, tol, prm, kprm = args
+    it = C.c_int64(0)
+    check(lib().qed2d_omf4_nf2(_c(prm), _rp(mom, prm), _cp(U, prm), _cp(X, prm), _cp(F, prm), _cp(g5DX, prm),
+                               float(am0), float(eps), int(ns), int(maxiter), float(tol), C.byref(it)), "OMF4!")
+    return it.value
+
+
+def _rhmc_arrays(F, am0, rprm):
+    nf = len(am0)
+    fp = (C.c_void_p * nf)(*[C.c_void_p(f.data_ptr()).value for f in F])
+    am = (C.c_double * nf)(*[float(a) for a in am0])
+    rp = (_lib.RhmcParams * nf)(*[r.to_c() for r in rprm])
+    return nf, fp, am, rp
+
+
+def leapfrog_(mom, U, X, F, g5DX, am0, eps, ns, CGmaxiter, tol, prm: LattParm, kprm=None, rprm=None):
+    """leapfrog! -- Nf=2 (:426-449) or RHMC when rprm is given (:485-513)."""
+    it = C.c_int64(0)
+    if rprm is None:
+        check(lib().qed2d_leapfrog_nf2(_c(prm), _rp(mom, prm), _cp(U, prm), _cp(X, prm), _cp(F, prm),
+                                       _cp(g5DX, prm), float(am0), float(eps), int(ns), int(CGmaxiter), float(tol),
+                                       C.byref(it)), "leapfrog!")
+        return it.value
+    nf, fp, am, rp = _rhmc_arrays(F, am0, rprm)
+    check(lib().qed2d_leapfrog_rhmc(_c(prm), _rp(mom, prm), _cp(U, prm), _cp(X, prm), fp, _cp(g5DX, prm), nf, am,
+                                    float(eps), int(ns), int(CGmaxiter), float(tol), rp, C.byref(it)), "leapfrog!")
+    return it.value
+
+
+def update_momenta_(mom, U, X, F, g5DX, am0, eps, ns, maxiter, tol, prm: LattParm, kprm=None, rprm=None):
+    """update_momenta! -- Nf=2 (:452-481) or RHMC when rprm is given (:516-557)."""
+    it = C.c_int64(0)
+    if rprm is None:
+        check(lib().qed2d_update_momenta_nf2(_c(prm), _rp(mom, prm), _cp(U, prm), _cp(X, prm), _cp(F, prm),
+                                             _cp(g5DX, prm), float(am0), float(eps), int(maxiter), float(tol),
+                                             C.byref(it)), "update_momenta!")
+        return it.value
+    nf, fp, am, rp = _rhmc_arrays(F, am0, rprm)
+    check(lib().qed2d_update_momenta_rhmc(_c(prm), _rp(mom, prm), _cp(U, prm), _cp(X, prm), fp, _cp(g5DX, prm),
+                                          nf, am, float(eps), int(maxiter), float(tol), rp, C.byref(it)),
+          "update_momenta!")
+    return it.value
+
+
+@dataclass
+class HMCInfo:
+    accepted: int
+    hini: float
+    hfin: float
+    dH: float
+    qtop: float
+    cg_iterations: int
+    counter: int
+
+
+def HMC_(U, *args, integrator: Integrators = None, qzero=False, reversibility_test=False, counter=None):
+    """HMC! with the reference's three methods (src/QED2dHMC.jl:19-195):
+        HMC_(U, eps, ns, acc, prm, kprm)                                   pure gauge (OMF4)
+        HMC_(U, am0, eps, ns, acc, CGmaxiter, tol, prm, kprm)              Nf=2 (Leapfrog)
+        HMC_(U, am0_list, eps, ns, acc, CGmaxiter, tol, prm, kprm, rprm)   RHMC (Leapfrog)
+    Appends 1/0 to `acc` like the reference and returns an HMCInfo."""
+    L = lib()
+    res = _lib.HmcResult()
+    ctr = _next_counter() if counter is None else int(counter)
+    sd = _rng["seed"]
+    if len(args) == 5:
+        eps, ns, acc, prm, kprm = args
+        integ = (integrator or OMF4()).code
+        st = L.qed2d_hmc_gauge(_c(prm), _cp(U, prm), float(eps), int(ns), integ, int(bool(qzero)), sd, ctr,
+                               C.byref(res))
+    elif len(args) == 8:
+        am0, eps, ns, acc, CGmaxiter, tol, prm, kprm = args
+        integ = (integrator or Leapfrog()).code
+        st = L.qed2d_hmc_nf2(_c(prm), _cp(U, prm), float(am0), float(eps), int(ns), integ, int(CGmaxiter),
+                             float(tol), int(bool(qzero)), sd, ctr, C.byref(res))
+    elif len(args) == 9:
+        am0, eps, ns, acc, CGmaxiter, tol, prm, kprm, rprm = args
+        nf = len(am0)
+        am = (C.c_double * nf)(*[float(a) for a in am0])
+        rp = (_lib.RhmcParams * nf)(*[r.to_c() for r in rprm])
+        st = L.qed2d_hmc_rhmc(_c(prm), _cp(U, prm), nf, am, float(eps), int(ns), int(CGmaxiter), float(tol), rp,
+                              int(bool(qzero)), int(bool(reversibility_test)), sd, ctr, C.byref(res))
+    else:
+        raise TypeError("HMC!: unsupported argument list")
+    if st == _lib.NOT_CONVERGED:
+        raise Qed2dError(st, "CG not converged")
+    check(st, "HMC!")
+    if not reversibility_test:
+        acc.append(int(res.accepted))
+    return HMCInfo(res.accepted, res.hini, res.hfin, res.dH, res.qtop, res.cg_iterations, ctr)

@@ -1,0 +1,59 @@
+"""Single-kernel cases for profiling (ncu) and bandwidth sweeps.
+
+    python -m qed2d.cases <case> --L 2048 [--maxiter 100] [--repeat 3]
+
+cases: g5dw (FP64 gamm5Dw apply), cg_mixed / cg_f64 (one persistent CG launch
+capped at --maxiter iterations), force (gamm5Dw + tr_dQwdU), updt (link update).  Seeded hot-start links and Gaussian sources; prints the
+per-launch time of the last repeat.
+"""
+import argparse
+import sys
+
+import numpy as np
+import torch
+
+import qed2d
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("case", choices=["g5dw", "cg_mixed", "cg_f64", "force", "updt"])
+    ap.add_argument("--L", type=int, default=2048)
+    ap.add_argument("--maxiter", type=int, default=100)
+    ap.add_argument("--repeat", type=int, default=3)
+    a = ap.parse_args(argv)
+    L = a.L
+    prm = qed2d.LattParm((L, L), 4.0)
+    g = torch.Generator(device="cuda").manual_seed(1234)
+    U = torch.polar(torch.ones(2, L, L, dtype=torch.float64, device="cuda"),
+                    (torch.rand(2, L, L, dtype=torch.float64, device="cuda", generator=g) * 2 - 1) * np.pi)
+    si = torch.randn(2, L, L, dtype=torch.complex128, device="cuda", generator=g)
+    so = torch.zeros_like(si)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(a.repeat):
+        ev0.record()
+        if a.case == "g5dw":
+            qed2d.gamm5Dw(so, U, si, 0.1, prm)
+        elif a.case in ("cg_mixed", "cg_f64"):
+            qed2d.set_precision("mixed" if a.case == "cg_mixed" else "f64")
+            try:
+                qed2d.CG(so, U, si, 0.1, a.maxiter, 1e-24, qed2d.gamm5Dw_sqr_msq, prm, None)
+            except qed2d.Qed2dError:
+                pass   # capped iteration count, as intended
+        elif a.case == "force":
+            g5 = torch.empty_like(si)
+            qed2d.gamm5Dw(g5, U, si, 0.1, prm)
+            f = torch.zeros(2, L, L, dtype=torch.float64, device="cuda")
+            qed2d.tr_dQwdU(f, U, si, g5, prm)
+        elif a.case == "updt":
+            mom = torch.randn(2, L, L, dtype=torch.float64, device="cuda", generator=g)
+            qed2d.updt_fld_(U, mom, 0.01)
+        ev1.record()
+        torch.cuda.synchronize()
+    it = qed2d.last_solve(prm) if a.case.startswith("cg") else None
+    print(f"{a.case} L={L}: {ev0.elapsed_time(ev1):.3f} ms  solve={it}")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

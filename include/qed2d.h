@@ -1,0 +1,232 @@
+/*
+ * qed2d.h -- C ABI of libqed2d, the B200 (sm_100a) engine for the simulation hot
+ * path of the QED2d Julia package (dalbandea/Dav-QED2d): 2D compact U(1) gauge
+ * theory with two-spin Wilson fermions, HMC and RHMC.
+ *
+ * Each entry point replaces one function of the reference's exported API
+ * (src/QED2d.jl:27-54); the comment above it gives the reference file:line.
+ * Paths are relative to the reference project root.
+ *
+ * Conventions
+ *  - Arrays are caller-owned DEVICE pointers in the reference's layout: the
+ *    Julia column-major arrays
+ *        U    :: CuArray{ComplexF64}(L1, L2, 2)   links, direction last
+ *        s    :: CuArray{ComplexF64}(L1, L2, 2)   spinors, spin last
+ *        mom  :: CuArray{Float64}(L1, L2, 2)      momenta / forces
+ *        plx  :: CuArray{Float64}(L1, L2)         per-site fields
+ *    i.e. element (i1, i2, k) (0-based) at offset i1 + L1*(i2 + L2*k).  A complex
+ *    array is passed as `double*` to interleaved (re, im) pairs.  Pointers must be
+ *    16-byte aligned; stencil operators reject an output that aliases an input.
+ *  - Every function returns a qed2d_status.  Work is issued on the context's
+ *    stream (default: the legacy default stream).  Functions that return host
+ *    scalars (observables, iteration counts, HMC results) synchronise that
+ *    stream; the others are asynchronous.
+ *  - A context is not thread-safe; use one context per host thread.
+ *  - CG tolerance: as in the reference (src/QED2dSolver.jl:13-29) a solve stops
+ *    when |r|^2 < eps * |b|^2, so eps = 1e-24 means a relative residual of 1e-12.
+ *  - Random numbers (momenta, pseudofermion noise, power-method start vectors,
+ *    reweighting noise, the Metropolis uniform) come from Philox4x32-10 keyed by
+ *    (seed, stream, counter); qed2d_random_normal() reproduces any stream.
+ */
+#ifndef QED2D_H
+#define QED2D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    QED2D_OK = 0,
+    QED2D_ERR_NOT_CONVERGED = 1, /* CG hit maxiter (reference: error(), src/QED2dSolver.jl:39-43,98-102) */
+    QED2D_ERR_TIMEOUT = 2,       /* a grid barrier inside a persistent kernel gave up waiting */
+    QED2D_ERR_BAD_ARG = 3,       /* bad size, NULL, misaligned or aliased pointer */
+    QED2D_ERR_CUDA = 4,          /* a CUDA runtime call failed (qed2d_last_error() has the text) */
+    QED2D_ERR_NO_MEMORY = 5,
+    QED2D_ERR_UNSUPPORTED = 6
+} qed2d_status;
+
+/* solver precision used by every CG inside the library */
+typedef enum {
+    QED2D_PREC_F64 = 0,   /* FP64 persistent fused CG; the reference's arithmetic and stop rule */
+    QED2D_PREC_MIXED = 1, /* FP32 inner CG with FP64 reliable updates; stops on the FP64 true residual */
+    QED2D_PREC_PLAIN = 2  /* reference-structured FP64: unfused kernels, host-synchronised CG loop */
+} qed2d_precision;
+
+typedef enum { QED2D_LEAPFROG = 0, QED2D_OMF4 = 1 } qed2d_integrator;   /* src/integrators/integrators.jl:1-3 */
+
+#define QED2D_MAXPOLES 32
+
+/* RHMCParm -- src/QED2d.jl:15-26 */
+typedef struct {
+    double r_b;
+    int32_t n;
+    double eps;
+    double A;
+    double rho[QED2D_MAXPOLES];
+    double mu[QED2D_MAXPOLES];
+    double nu[QED2D_MAXPOLES];
+    double delta;
+    int32_t reweighting_N;
+    int32_t reweighting_Taylor;
+} qed2d_rhmc_params;
+
+/* outcome of one HMC trajectory (the reference logs these, src/QED2dHMC.jl:53-57) */
+typedef struct {
+    int32_t accepted;
+    double hini;
+    double hfin;
+    double dH;
+    double qtop;            /* Qtop(U) of the final (accepted or restored) field */
+    int64_t cg_iterations;  /* summed over every solve of the trajectory */
+} qed2d_hmc_result;
+
+/* Philox streams used by the HMC entry points (counter = the trajectory counter) */
+#define QED2D_STREAM_MOMENTA 1u
+#define QED2D_STREAM_METROPOLIS 3u
+#define QED2D_STREAM_POWER 4u
+#define QED2D_STREAM_NOISE 16u      /* + flavour index j: pseudofermion noise X_j */
+#define QED2D_STREAM_REWEIGHT 64u   /* + sample index j: reweighting noise */
+
+typedef struct qed2d_ctx qed2d_ctx;
+
+/* ---- context: LattParm(iL, beta) -- src/QED2d.jl:5-8.  KernelParm (:10-13) has no
+ * counterpart: launch geometry is chosen by the library. ---- */
+int qed2d_ctx_create(int L1, int L2, double beta, qed2d_ctx** out);
+int qed2d_ctx_destroy(qed2d_ctx* ctx);
+int qed2d_ctx_set_beta(qed2d_ctx* ctx, double beta);
+int qed2d_ctx_set_stream(qed2d_ctx* ctx, void* cuda_stream);
+int qed2d_ctx_set_precision(qed2d_ctx* ctx, int precision);
+int qed2d_ctx_get_dims(const qed2d_ctx* ctx, int* L1, int* L2);
+/* iterations, final |r|^2/|b|^2 and (QED2D_PREC_MIXED) FP64 reliable updates of
+ * the most recent solve on this context; any pointer may be NULL */
+int qed2d_last_solve(const qed2d_ctx* ctx, int64_t* iterations, double* rel_residual_sq,
+                     int64_t* reliable_updates);
+const char* qed2d_status_string(int status);
+const char* qed2d_last_error(void);
+/* kernels launched by this process so far (all contexts) */
+int64_t qed2d_launch_count(void);
+
+/* ---- gauge kernels: src/QED2dAction.jl ---- */
+/* plaquette! -- src/QED2dAction.jl:2-16: plx = Re U1(x)U2(x+1)conj(U1(x+2)U2(x)) */
+int qed2d_plaquette_field(qed2d_ctx* ctx, double* plx, const double* U);
+/* qtop! -- src/QED2dAction.jl:18-32: plx = arg of the plaquette */
+int qed2d_qtop_field(qed2d_ctx* ctx, double* plx, const double* U);
+/* krnl_force! -- src/QED2dAction.jl:34-53 (two buffers, every element written) */
+int qed2d_krnl_force(qed2d_ctx* ctx, double* frc1, double* frc2, const double* U);
+/* updt_fld! -- src/QED2dAction.jl:55-65: U <- exp(i eps mom) U */
+int qed2d_updt_fld(qed2d_ctx* ctx, double* U, const double* mom, double eps);
+
+/* ---- Dirac operator: src/QED2dDirac.jl ---- */
+/* gamm5Dw -- src/QED2dDirac.jl:2-33 */
+int qed2d_gamm5dw(qed2d_ctx* ctx, double* so, const double* U, const double* si, double am0);
+/* gamm5 -- src/QED2dDirac.jl:130-146 */
+int qed2d_gamm5(qed2d_ctx* ctx, double* so, const double* si);
+/* Dw -- src/QED2dDirac.jl:157-169 */
+int qed2d_dw(qed2d_ctx* ctx, double* so, const double* U, const double* si, double am0);
+/* gamm5Dw_sqr -- src/QED2dDirac.jl:35-46; also gamm5Dw_sqr_msq (:69-81), which adds no mass term */
+int qed2d_gamm5dw_sqr(qed2d_ctx* ctx, double* so, const double* U, const double* si, double am0);
+/* gamm5Dw_sqr_sqr -- src/QED2dDirac.jl:48-67 */
+int qed2d_gamm5dw_sqr_sqr(qed2d_ctx* ctx, double* so, const double* U, const double* si, double am0);
+/* gamm5Dw_sqr_musq -- src/QED2dDirac.jl:83-95: so = (g5Dw)^2 si + mu^2 si */
+int qed2d_gamm5dw_sqr_musq(qed2d_ctx* ctx, double* so, const double* U, const double* si, double am0, double mu);
+/* gamm5Dw_sqr_sqr_musq -- src/QED2dDirac.jl:97-117 */
+int qed2d_gamm5dw_sqr_sqr_musq(qed2d_ctx* ctx, double* so, const double* U, const double* si, double am0,
+                               double mu);
+/* tr_dQwdU -- src/QED2dDirac.jl:172-199 */
+int qed2d_tr_dqwdu(qed2d_ctx* ctx, double* frc, const double* U, const double* X, const double* g5DwX);
+
+/* ---- fields and utilities ---- */
+/* unfold_fld! / unfold_reflect! -- src/QED2dFields.jl:2-50.  ctx describes the
+ * OLD (L1 x L2) lattice; Uout is a caller-owned (2 L1) x (2 L2) link array. */
+int qed2d_unfold(qed2d_ctx* ctx, double* Uout, const double* Uin, int reflect);
+/* plwv -- src/QED2dUtils.jl:2-11 */
+int qed2d_plwv(qed2d_ctx* ctx, double* so, double k1, double k2);
+/* n N(0,1) numbers of stream `stream` at counter `counter` (CUDA.randn's role) */
+int qed2d_random_normal(qed2d_ctx* ctx, double* out, int64_t n, uint64_t seed, uint32_t stream,
+                        uint32_t counter);
+/* the Metropolis uniform of trajectory `counter` (Julia rand()'s role), host only */
+double qed2d_random_uniform(uint64_t seed, uint32_t stream, uint32_t counter);
+
+/* ---- observables: src/QED2dHMC.jl:198-237 ---- */
+int qed2d_action(qed2d_ctx* ctx, const double* U, double* S);            /* Action   :206-215 */
+int qed2d_plaquette(qed2d_ctx* ctx, const double* U, double* P);         /* Plaquette :217-226 */
+/* Qtop :228-237 (unrounded, as the reference); q_round (may be NULL) = round(Q) */
+int qed2d_qtop(qed2d_ctx* ctx, const double* U, double* Q, int64_t* q_round);
+int qed2d_hamiltonian(qed2d_ctx* ctx, const double* mom, const double* U, double* H); /* :198-203 */
+
+/* ---- solvers: src/QED2dSolver.jl ---- */
+/* CG method 1 (:3-46) on gamm5Dw_sqr_msq: so = ((g5Dw)^2)^-1 si */
+int qed2d_cg(qed2d_ctx* ctx, double* so, const double* U, const double* si, double am0, int maxiter,
+             double eps, int* iterations);
+/* CG method 2 (:49-105) on gamm5Dw_sqr_musq: so = ((g5Dw)^2 + mu^2)^-1 si; so_as_guess != 0 warm-starts */
+int qed2d_cg_shift(qed2d_ctx* ctx, double* so, const double* U, const double* si, double am0, double mu,
+                   int maxiter, double eps, int so_as_guess, int* iterations);
+/* all n shifted systems ((g5Dw)^2 + mu_i^2) so[i] = si in one Krylov space.  No
+ * single reference counterpart: it replaces the n sequential CG calls of
+ * MultiCG (src/QED2dRHMC.jl:284-287) and update_momenta! (src/QED2dHMC.jl:529-544). */
+int qed2d_multishift_cg(qed2d_ctx* ctx, double* const* so, const double* U, const double* si, double am0,
+                        const double* mu, int n, int maxiter, double eps, int* iterations);
+
+/* ---- RHMC: src/QED2dRHMC.jl ---- */
+/* get_rhmc_params -- :93-110 (host; Zolotarev coefficients) */
+int qed2d_get_rhmc_params(int n, double r_a, double r_b, qed2d_rhmc_params* out);
+/* MultiCG -- :281-290: so = (1 + sum_j rho_j ((g5Dw)^2 + mu_j^2)^-1) si */
+int qed2d_multi_cg(qed2d_ctx* ctx, double* so, const double* U, const double* si, double am0, int maxiter,
+                   double eps, const qed2d_rhmc_params* rprm, int* iterations);
+/* R -- :261-271: so = (A / r_b) MultiCG(si) ~ ((g5Dw)^2)^-1/2 si */
+int qed2d_rational(qed2d_ctx* ctx, double* so, const double* U, const double* si, double am0, int maxiter,
+                   double eps, const qed2d_rhmc_params* rprm, int* iterations);
+/* generate_pseudofermion! -- :298-319 */
+int qed2d_generate_pseudofermion(qed2d_ctx* ctx, double* F, const double* U, const double* X, double am0,
+                                 int maxiter, double tol, const qed2d_rhmc_params* rprm, int* iterations);
+/* power_method -- :135-170 (start vector: stream QED2D_STREAM_POWER at `counter`;
+ * the second loop is applied out of place, see the reference's :159) */
+int qed2d_power_method(qed2d_ctx* ctx, const double* U, double am0, int iter, uint64_t seed, uint32_t counter,
+                       double* lambda_min, double* lambda_max);
+/* LuscherZ -- :174-186: Z = ((g5Dw)^2 R^2 - 1) Xin */
+int qed2d_luscher_z(qed2d_ctx* ctx, double* Z, const double* U, const double* Xin, double am0, int maxiter,
+                    double tol, const qed2d_rhmc_params* rprm);
+/* reweighting_factor -- :210-239 (noise: stream QED2D_STREAM_REWEIGHT + j at `counter`) */
+int qed2d_reweighting_factor(qed2d_ctx* ctx, const double* U, double am0, int maxiter, double tol,
+                             const qed2d_rhmc_params* rprm, uint64_t seed, uint32_t counter, double* W);
+
+/* ---- molecular dynamics: src/QED2dHMC.jl ---- */
+/* OMF4! pure gauge -- :239-305 */
+int qed2d_omf4_gauge(qed2d_ctx* ctx, double* mom, double* U, double eps, int ns);
+/* update_momenta! Nf=2 -- :452-481 (iterations may be NULL; accumulates otherwise) */
+int qed2d_update_momenta_nf2(qed2d_ctx* ctx, double* mom, const double* U, double* X, const double* F,
+                             double* g5DX, double am0, double eps, int maxiter, double tol, int64_t* iterations);
+/* leapfrog! Nf=2 -- :426-449 */
+int qed2d_leapfrog_nf2(qed2d_ctx* ctx, double* mom, double* U, double* X, const double* F, double* g5DX,
+                       double am0, double eps, int ns, int maxiter, double tol, int64_t* iterations);
+/* OMF4! Nf=2 -- :307-422 */
+int qed2d_omf4_nf2(qed2d_ctx* ctx, double* mom, double* U, double* X, const double* F, double* g5DX,
+                   double am0, double eps, int ns, int maxiter, double tol, int64_t* iterations);
+/* update_momenta! RHMC -- :516-557 (F: nf pseudofermion fields) */
+int qed2d_update_momenta_rhmc(qed2d_ctx* ctx, double* mom, const double* U, double* X, const double* const* F,
+                              double* g5DX, int nf, const double* am0, double eps, int maxiter, double tol,
+                              const qed2d_rhmc_params* rprm, int64_t* iterations);
+/* leapfrog! RHMC -- :485-513 */
+int qed2d_leapfrog_rhmc(qed2d_ctx* ctx, double* mom, double* U, double* X, const double* const* F,
+                        double* g5DX, int nf, const double* am0, double eps, int ns, int maxiter, double tol,
+                        const qed2d_rhmc_params* rprm, int64_t* iterations);
+
+/* ---- HMC steps (U updated in place; restored on rejection) ---- */
+/* HMC! pure gauge -- :19-60 (integrator: OMF4 as the reference; LEAPFROG is an extension) */
+int qed2d_hmc_gauge(qed2d_ctx* ctx, double* U, double eps, int ns, int integrator, int qzero, uint64_t seed,
+                    uint32_t counter, qed2d_hmc_result* res);
+/* HMC! Nf=2 -- :64-113 */
+int qed2d_hmc_nf2(qed2d_ctx* ctx, double* U, double am0, double eps, int ns, int integrator, int maxiter,
+                  double tol, int qzero, uint64_t seed, uint32_t counter, qed2d_hmc_result* res);
+/* HMC! RHMC -- :116-195 (reversibility != 0: the reference's reversibility_test mode) */
+int qed2d_hmc_rhmc(qed2d_ctx* ctx, double* U, int nf, const double* am0, double eps, int ns, int maxiter,
+                   double tol, const qed2d_rhmc_params* rprm, int qzero, int reversibility, uint64_t seed,
+                   uint32_t counter, qed2d_hmc_result* res);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QED2D_H */
