@@ -24,6 +24,7 @@
 // unfused kernels and two device-to-host reads per iteration.
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 
 #include "stencil.cuh"
@@ -63,27 +64,45 @@ __device__ __forceinline__ void write_partials(double* part, const double* v, in
         for (int k = 0; k < nv; k++) part[(size_t)k * kMaxPartBlocks + blockIdx.x] = v[k];
 }
 
+// Grid-wide sum of NV values (NV <= 4), deterministic: every block writes its
+// partials; the last block to arrive sums them in a fixed order (thread t takes
+// partials t, t+blockDim, ..., then a fixed-shape tree), publishes the sums in
+// ctl->red and releases the barrier; every block then reads the sums.  Partials
+// and sums alternate between two buffers: reduction n+2 overwrites buffer n's
+// only after every block has passed barrier n+1, i.e. has read the result of n.
 template <int NV>
-__device__ __forceinline__ bool reduce_sync(GridSync& gs, double (&v)[NV], double* part, double* smem) {
+__device__ __forceinline__ bool reduce_sync(GridSync& gs, double (&v)[NV], double* part_base, double* red_base,
+                                            double* smem) {
+    static_assert(NV <= kMaxPartVals / 2, "too many values for the double-buffered partials");
+    __shared__ int s_last;
+    const int buf = gs.nred++ & 1;
+    double* part = part_base + (size_t)buf * (kMaxPartVals / 2) * kMaxPartBlocks;
+    double* red = red_base + buf * 4;
     block_sum<NV>(v, smem);
     write_partials(part, v, NV);
-    if (!gs.sync()) return false;
-    __syncthreads();
-    if (threadIdx.x < 32) {
+    const bool last = gs.arrive(&s_last);
+    if (last) {
+        __threadfence();
+        double w[NV];
 #pragma unroll
         for (int k = 0; k < NV; k++) {
             double s = 0.0;
-            for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) s += __ldcg(part + (size_t)k * kMaxPartBlocks + i);
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (threadIdx.x == 0) smem[k] = s;
+            for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) s += __ldcg(part + (size_t)k * kMaxPartBlocks + i);
+            w[k] = s;
         }
+        block_sum<NV>(w, smem);
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int k = 0; k < NV; k++) red[k] = w[k];
+            gs.release();
+        }
+    } else if (threadIdx.x == 0) {
+        gs.wait();
     }
     __syncthreads();
 #pragma unroll
-    for (int k = 0; k < NV; k++) v[k] = smem[k];
-    __syncthreads();
-    return true;
+    for (int k = 0; k < NV; k++) v[k] = __ldcg(red + k);
+    return ld_volatile_int(gs.err) == 0;
 }
 
 __device__ __forceinline__ void finish_solve(const CGP& P, int iters, bool conv, double rr, double bb,
@@ -111,7 +130,7 @@ __device__ __forceinline__ void finish_solve(const CGP& P, int iters, bool conv,
 // FP64 persistent CG
 __global__ void __launch_bounds__(TILE) k_cg_f64(const CGP P) {
     __shared__ double smem[32 * 2];
-    GridSync gs{&P.ctl->bar, &P.ctl->err, 0};
+    GridSync gs{&P.ctl->bar, &P.ctl->gen, &P.ctl->err};
     const long long ntiles = num_tiles(P.g), V = P.g.V;
     const LkD L{P.U, V};
     const double m2 = P.m2, mu2 = P.mu2;
@@ -132,7 +151,7 @@ __global__ void __launch_bounds__(TILE) k_cg_f64(const CGP P) {
                 st_d(P.t, V, q.x, g5dw_at<double>(SpD{P.x, V}, L, q, m2));
             }
         }
-        if (!reduce_sync<1>(gs, v, P.part, smem)) goto done;
+        if (!reduce_sync<1>(gs, v, P.part, P.ctl->red, smem)) goto done;
         bb = v[0];
     }
     if (bb == 0.0) {   // zero source: zero solution
@@ -154,7 +173,7 @@ __global__ void __launch_bounds__(TILE) k_cg_f64(const CGP P) {
                 st_d(P.r, V, q.x, r);
                 v[0] += norm2(r.a) + norm2(r.b);
             }
-            if (!reduce_sync<1>(gs, v, P.part, smem)) goto done;
+            if (!reduce_sync<1>(gs, v, P.part, P.ctl->red, smem)) goto done;
             rr = v[0];
             if (rr < tol) { conv = true; goto epilogue; }
         } else {
@@ -173,7 +192,7 @@ __global__ void __launch_bounds__(TILE) k_cg_f64(const CGP P) {
                 st_d(P.t, V, q.x, tt);
                 v[0] += norm2(tt.a) + norm2(tt.b) + mu2 * (norm2(c.a) + norm2(c.b));
             }
-            if (!reduce_sync<1>(gs, v, P.part, smem)) goto done;
+            if (!reduce_sync<1>(gs, v, P.part, P.ctl->red, smem)) goto done;
             const double alpha = rr / v[0];
             v[0] = 0.0;
             FOR_TILES(q) {
@@ -188,7 +207,7 @@ __global__ void __launch_bounds__(TILE) k_cg_f64(const CGP P) {
                 st_d(P.r, V, q.x, r);
                 v[0] += norm2(r.a) + norm2(r.b);
             }
-            if (!reduce_sync<1>(gs, v, P.part, smem)) goto done;
+            if (!reduce_sync<1>(gs, v, P.part, P.ctl->red, smem)) goto done;
             const double rn = v[0];
             if (rn < tol) { rr = rn; conv = true; break; }
             beta = rn / rr;
@@ -206,7 +225,7 @@ done:
 // mixed FP32/FP64 reliable-update CG
 __global__ void __launch_bounds__(TILE) k_cg_mixed(const CGP P) {
     __shared__ double smem[32 * 2];
-    GridSync gs{&P.ctl->bar, &P.ctl->err, 0};
+    GridSync gs{&P.ctl->bar, &P.ctl->gen, &P.ctl->err};
     const long long ntiles = num_tiles(P.g), V = P.g.V;
     const LkD L{P.U, V};
     const LkF Lf{P.U32};
@@ -225,7 +244,7 @@ __global__ void __launch_bounds__(TILE) k_cg_mixed(const CGP P) {
             if (!P.guess) st_d(P.x, V, q.x, Pair<double>{make_double2(0, 0), make_double2(0, 0)});
             else st_d(t64, V, q.x, g5dw_at<double>(SpD{P.x, V}, L, q, m2));
         }
-        if (!reduce_sync<1>(gs, v, P.part, smem)) goto done;
+        if (!reduce_sync<1>(gs, v, P.part, P.ctl->red, smem)) goto done;
         bb = v[0];
     }
     if (bb == 0.0) {
@@ -249,7 +268,7 @@ __global__ void __launch_bounds__(TILE) k_cg_mixed(const CGP P) {
                 st_d(P.r, V, q.x, r);
                 v[0] += norm2(r.a) + norm2(r.b);
             }
-            if (!reduce_sync<1>(gs, v, P.part, smem)) goto done;
+            if (!reduce_sync<1>(gs, v, P.part, P.ctl->red, smem)) goto done;
             rr64 = v[0];
             if (rr64 < tol) { conv = true; goto done; }
         } else {
@@ -267,7 +286,7 @@ __global__ void __launch_bounds__(TILE) k_cg_mixed(const CGP P) {
                 st_f(P.x32, q.x, Pair<float>{make_float2(0, 0), make_float2(0, 0)});
                 v[0] += (double)norm2(r32.a) + (double)norm2(r32.b);
             }
-            if (!reduce_sync<1>(gs, v, P.part, smem)) goto done;
+            if (!reduce_sync<1>(gs, v, P.part, P.ctl->red, smem)) goto done;
             rr = v[0];
         }
         double maxrr = rr, beta = 0.0;
@@ -285,7 +304,7 @@ __global__ void __launch_bounds__(TILE) k_cg_mixed(const CGP P) {
                 st_f(P.t32, q.x, tt);
                 v[0] += (double)(norm2(tt.a) + norm2(tt.b)) + mu2 * (double)(norm2(c.a) + norm2(c.b));
             }
-            if (!reduce_sync<1>(gs, v, P.part, smem)) goto done;
+            if (!reduce_sync<1>(gs, v, P.part, P.ctl->red, smem)) goto done;
             const float alpha = (float)(rr / v[0]);
             v[0] = 0.0;
             FOR_TILES(q) {
@@ -300,7 +319,7 @@ __global__ void __launch_bounds__(TILE) k_cg_mixed(const CGP P) {
                 st_f(P.r32, q.x, r);
                 v[0] += (double)(norm2(r.a) + norm2(r.b));
             }
-            if (!reduce_sync<1>(gs, v, P.part, smem)) goto done;
+            if (!reduce_sync<1>(gs, v, P.part, P.ctl->red, smem)) goto done;
             const double rn = v[0];
             maxrr = fmax(maxrr, rn);
             const bool cand = rn < tol * s * s;
@@ -329,7 +348,7 @@ __global__ void __launch_bounds__(TILE) k_cg_mixed(const CGP P) {
                     st_d(P.r, V, q.x, r);
                     w[0] += norm2(r.a) + norm2(r.b);
                 }
-                if (!reduce_sync<1>(gs, w, P.part, smem)) goto done;
+                if (!reduce_sync<1>(gs, w, P.part, P.ctl->red, smem)) goto done;
                 const double rrt = w[0];
                 rr64 = rrt;
                 if (rrt < tol) { conv = true; break; }
@@ -341,7 +360,7 @@ __global__ void __launch_bounds__(TILE) k_cg_mixed(const CGP P) {
                     st_f(P.r32, q.x, r32);
                     w[0] += (double)(norm2(r32.a) + norm2(r32.b));
                 }
-                if (!reduce_sync<1>(gs, w, P.part, smem)) goto done;
+                if (!reduce_sync<1>(gs, w, P.part, P.ctl->red, smem)) goto done;
                 beta = (rrt * s * s / rr) * (s_new / s);
                 s = s_new;
                 rr = w[0];
@@ -395,7 +414,7 @@ __global__ void __launch_bounds__(TILE) k_cg_multishift(const MSP P) {
     __shared__ double smem[32 * 2];
     __shared__ double z[kMaxShifts], zp[kMaxShifts], ai[kMaxShifts], bi[kMaxShifts];
     __shared__ int upd[kMaxShifts], act[kMaxShifts];
-    GridSync gs{&P.ctl->bar, &P.ctl->err, 0};
+    GridSync gs{&P.ctl->bar, &P.ctl->gen, &P.ctl->err};
     const long long ntiles = num_tiles(P.g), V = P.g.V;
     const LkD L{P.U, V};
     const double m2 = P.m2, mu2 = P.mu2b;
@@ -414,7 +433,7 @@ __global__ void __launch_bounds__(TILE) k_cg_multishift(const MSP P) {
             st_d(P.r, V, q.x, bv);
             for (int i = 0; i < P.n; i++) st_d(P.x[i], V, q.x, Pair<double>{make_double2(0, 0), make_double2(0, 0)});
         }
-        if (!reduce_sync<1>(gs, v, P.part, smem)) goto done;
+        if (!reduce_sync<1>(gs, v, P.part, P.ctl->red, smem)) goto done;
         bb = v[0];
     }
     if (bb == 0.0) { conv = true; goto done; }
@@ -453,7 +472,7 @@ __global__ void __launch_bounds__(TILE) k_cg_multishift(const MSP P) {
                     }
                 }
             }
-            if (!reduce_sync<1>(gs, v, P.part, smem)) goto done;
+            if (!reduce_sync<1>(gs, v, P.part, P.ctl->red, smem)) goto done;
             const double alpha = rr / v[0];
             v[0] = 0.0;
             FOR_TILES(q) {
@@ -468,7 +487,7 @@ __global__ void __launch_bounds__(TILE) k_cg_multishift(const MSP P) {
                 st_d(P.r, V, q.x, r);
                 v[0] += norm2(r.a) + norm2(r.b);
             }
-            if (!reduce_sync<1>(gs, v, P.part, smem)) goto done;
+            if (!reduce_sync<1>(gs, v, P.part, P.ctl->red, smem)) goto done;
             const double rn = v[0];
             const double beta_new = rn / rr;
             // shift scalars (identical in every block)
@@ -526,21 +545,28 @@ done:
 
 // ---------------------------------------------------------------------------
 // host side
+static_assert(offsetof(DevCtl, gen) == sizeof(unsigned long long) &&
+                  offsetof(DevCtl, err) == 2 * sizeof(unsigned long long),
+              "reset_barrier zeroes bar, gen and err as one range");
+
+// Cooperative grid: at most the co-resident limit, then as few blocks as give
+// every block the same number of tiles (fewer arrivals per barrier, no tail).
 template <class K>
 static int coop_grid(Ctx& c, K kernel, int* grid) {
     int per_sm = 0;
     QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, TILE, 0));
     if (per_sm < 1) return QED2D_ERR_UNSUPPORTED;
     long long g = (long long)per_sm * c.num_sms;
-    const long long nt = num_tiles(c.g);
-    if (g > nt) g = nt;
     if (g > kMaxPartBlocks) g = kMaxPartBlocks;
+    const long long nt = num_tiles(c.g);
+    const long long per_block = (nt + g - 1) / g;
+    g = (nt + per_block - 1) / per_block;
     *grid = (int)g;
     return QED2D_OK;
 }
 
-static int reset_barrier(Ctx& c) {
-    QCHECK(cudaMemsetAsync(&c.ctl->bar, 0, sizeof(unsigned long long) + sizeof(int), c.stream));
+static int reset_barrier(Ctx& c) {   // bar, gen and err are contiguous
+    QCHECK(cudaMemsetAsync(&c.ctl->bar, 0, 2 * sizeof(unsigned long long) + sizeof(int), c.stream));
     return QED2D_OK;
 }
 

@@ -115,39 +115,68 @@ __device__ __forceinline__ void normal_pair(uint64_t seed, uint32_t stream, uint
 
 // ---------------------------------------------------------------------------
 // Grid-wide barrier for persistent kernels launched cooperatively (all blocks
-// co-resident).  The counter is zeroed before each launch and only grows; a
-// barrier's target is (barrier index) * gridDim.x.  The wait is bounded: after
-// ~2^26 polls (seconds) the block records QED2D_ERR_TIMEOUT in *err and leaves
-// the barrier, and every block stops at its next check of *err.
+// co-resident).  Every block adds one arrival to `arrivals`; the block that
+// arrives last (it sees target-1) does the barrier's completion work (e.g. the
+// final sum of a reduction) and then publishes the barrier's generation in
+// `gen`; the others poll `gen`.  Both counters only grow within a launch and
+// are zeroed before it.  The wait is bounded: after ~2^26 polls (seconds) a
+// block records QED2D_ERR_TIMEOUT in *err and leaves, and every block stops at
+// its next check of *err.
 __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
     unsigned long long v;
     asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" : : "l"(p), "l"(v) : "memory");
 }
 __device__ __forceinline__ int ld_volatile_int(const int* p) {
     return *reinterpret_cast<const volatile int*>(p);
 }
 
 struct GridSync {
-    unsigned long long* counter;
+    unsigned long long* arrivals;
+    unsigned long long* gen;
     int* err;
-    unsigned long long target;
-    __device__ __forceinline__ bool sync() {
+    unsigned long long target = 0;
+    int nred = 0;   // reductions done so far: selects the double-buffered partials/results
+
+    // Arrive (thread 0 of each block).  Returns true in the last-arriving block.
+    __device__ __forceinline__ bool arrive(int* s_last) {
         __syncthreads();
         target += gridDim.x;
         if (threadIdx.x == 0) {
             __threadfence();
-            atomicAdd(counter, 1ULL);
-            unsigned long long polls = 0;
-            while (ld_acquire_u64(counter) < target) {
-                if (ld_volatile_int(err) != 0) break;
-                if (++polls > (1ULL << 26)) {
-                    atomicExch(err, 2 /* QED2D_ERR_TIMEOUT */);
-                    break;
-                }
-                __nanosleep(32);
+            const unsigned long long old = atomicAdd(arrivals, 1ULL);
+            *s_last = old == target - 1;
+        }
+        __syncthreads();
+        return *s_last != 0;
+    }
+    // Release (called by thread 0 of the last block after its completion work).
+    __device__ __forceinline__ void release() {
+        __threadfence();
+        st_release_u64(gen, target);
+    }
+    // Wait for the release (thread 0 of the other blocks), bounded.
+    __device__ __forceinline__ void wait() {
+        unsigned long long polls = 0;
+        while (ld_acquire_u64(gen) < target) {
+            if (ld_volatile_int(err) != 0) break;
+            if (++polls > (1ULL << 26)) {
+                atomicExch(err, 2 /* QED2D_ERR_TIMEOUT */);
+                break;
             }
-            __threadfence();
+            __nanosleep(32);
+        }
+        __threadfence();
+    }
+    __device__ __forceinline__ bool sync() {
+        __shared__ int s_last;
+        const bool last = arrive(&s_last);
+        if (threadIdx.x == 0) {
+            if (last) release();
+            else wait();
         }
         __syncthreads();
         return ld_volatile_int(err) == 0;

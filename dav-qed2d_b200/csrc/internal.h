@@ -21,8 +21,9 @@ struct Lat {
 
 // Device control block shared by the kernels of one context.
 struct DevCtl {
-    unsigned long long bar;   // grid-barrier counter, zeroed before each persistent launch
-    int err;                  // barrier timeout flag, zeroed before each persistent launch
+    unsigned long long bar;   // grid-barrier arrivals, zeroed before each persistent launch
+    unsigned long long gen;   // grid-barrier release generation, zeroed likewise
+    int err;                  // barrier timeout flag, zeroed likewise
     int status;               // sticky: first failing status of the current sequence
     long long iters_total;    // CG iterations accumulated since the last reset
     int last_iters;           // iterations of the most recent solve
@@ -31,6 +32,7 @@ struct DevCtl {
     unsigned ticket;          // completion ticket of single-launch reductions
     int last_updates;         // reliable updates of the most recent (mixed) solve
     double scal[32];          // results of reductions
+    double red[8];            // grid-reduction results of persistent kernels (double buffered)
 };
 
 constexpr int kMaxPartBlocks = 2048;   // partial-sum slots per reduced quantity

@@ -190,3 +190,24 @@ def test_zero_source_and_errors(q):
     with pytest.raises(Qed2dError):
         q.CG(x, Ud, to_dev(bn), 0.2, 50, 1e-24, q.gamm5Dw_sqr_msq, prm, None)
     assert q.CG(x, Ud, bd, 0.2, 10000, 1e-24, q.gamm5Dw_sqr_msq, prm, None) > 0
+
+
+@pytest.mark.parametrize("prec", ["f64", "mixed"])
+@pytest.mark.parametrize("L1,L2", [(512, 512), (96, 64)])
+def test_persistent_solver_deterministic(q, prec, L1, L2):
+    """Every block of a persistent solve takes the same decisions from the same
+    fixed-order reductions: repeated solves are bitwise identical, with the
+    same iteration count, and never time out."""
+    import torch
+    q.set_precision(prec)
+    prm = q.LattParm((L1, L2), 4.0)
+    U, b = setup(L1, L2)
+    Ud, bd = to_dev(U), to_dev(b)
+    x = q.cfield(L1, L2)
+    ref_it = q.CG(x, Ud, bd, 0.1, 50000, 1e-24, q.gamm5Dw_sqr_msq, prm, None)
+    ref = x.clone()
+    for _ in range(30):
+        it = q.CG(x, Ud, bd, 0.1, 50000, 1e-24, q.gamm5Dw_sqr_msq, prm, None)
+        assert it == ref_it
+        assert torch.equal(x, ref)
+    q.set_precision("f64")
