@@ -10,7 +10,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/qed2d.h"
+#include "qed2d.h"   // include/ (on the include path)
 
 namespace qed2d {
 

@@ -42,6 +42,28 @@ __host__ __device__ __forceinline__ long long num_tiles(const Lat& g) {
     return (long long)((g.L1 + TX - 1) / TX) * ((g.L2 + TY - 1) / TY);
 }
 
+// the same for a BX x BY tile visited by BX*BY threads (thread t -> (t % BX, t / BX))
+template <int BX, int BY>
+__device__ __forceinline__ Site site_of_tile_t(const Lat& g, long long tile, int t) {
+    const int nt1 = (g.L1 + BX - 1) / BX;
+    const long long t2 = tile / nt1;
+    const int t1 = (int)(tile - t2 * nt1);
+    Site s;
+    s.i1 = t1 * BX + (t % BX);
+    s.i2 = (int)t2 * BY + (t / BX);
+    s.ok = s.i1 < g.L1 && s.i2 < g.L2;
+    s.x = s.i1 + (long long)g.L1 * s.i2;
+    s.xp1 = (s.i1 + 1 == g.L1) ? s.x - (g.L1 - 1) : s.x + 1;
+    s.xm1 = (s.i1 == 0) ? s.x + (g.L1 - 1) : s.x - 1;
+    s.xp2 = (s.i2 + 1 == g.L2) ? (long long)s.i1 : s.x + g.L1;
+    s.xm2 = (s.i2 == 0) ? s.x + (g.V - g.L1) : s.x - g.L1;
+    return s;
+}
+template <int BX, int BY>
+__host__ __device__ __forceinline__ long long num_tiles_t(const Lat& g) {
+    return (long long)((g.L1 + BX - 1) / BX) * ((g.L2 + BY - 1) / BY);
+}
+
 // ---------------------------------------------------------------------------
 // spinor accessors
 struct SpD {   // FP64 planes (reference layout): spin k of site x at p[x + k V]
