@@ -26,6 +26,8 @@
 #include <cmath>
 #include <cstddef>
 #include <cstring>
+#include <mutex>
+#include <string>
 
 #include "stencil.cuh"
 
@@ -758,3 +760,134 @@ int read_ctl(Ctx& c, bool reset_sequence) {
 }
 
 }  // namespace qed2d
+
+namespace qed2d {
+
+// ---------------------------------------------------------------------------
+// Allocation-free CG (qed2d_cg_noalloc).  Some callers must not allocate device
+// memory once they are running: a host loop that has handed all device memory
+// to its own pool allocator up front (CUDA.jl's or PyTorch's caching allocator
+// would see an out-of-band cudaMalloc as lost capacity), or a latency-bound loop
+// in which the implicit device synchronisation of cudaMalloc/cudaFree would stall
+// the pipeline.  This entry point runs the same persistent FP64 CG kernel as
+// qed2d_cg (method 1) without a context: its scratch -- the control block, the
+// reduction partials and the four solver vectors r, p (x2), t -- is one
+// file-scope device array, sized for at most QED2D_NOALLOC_MAX_SITES sites, that
+// every GPU which loads this library holds until the process exits.
+//
+// Set-up: the first call on a device looks up the array's device address with
+// cudaGetSymbolAddress (this can also load the library's device code) and caches
+// it per device; make that first call before any stream capture.  Every call
+// shares the one array, so calls that overlap on the GPU (two streams, two host
+// threads) race; serialise them.  The control block is zeroed by each call; the
+// vectors are always written before they are read.
+namespace {
+constexpr size_t kNaCtlBytes = 512;
+constexpr size_t kNaPartBytes = sizeof(double) * kMaxPartVals * kMaxPartBlocks;
+constexpr size_t kNaFieldBytes = sizeof(double2) * 2 * (size_t)QED2D_NOALLOC_MAX_SITES;
+constexpr size_t kNaBytes = kNaCtlBytes + kNaPartBytes + 4 * kNaFieldBytes;
+static_assert(sizeof(DevCtl) <= kNaCtlBytes, "control block does not fit its slot");
+static_assert(kNaPartBytes % 256 == 0 && kNaFieldBytes % 256 == 0, "scratch slices must stay 256-byte aligned");
+constexpr int kNaMaxDevices = 64;
+std::mutex g_na_mutex;
+void* g_na_base[kNaMaxDevices] = {};
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+// device address of g_noalloc_scratch on the current device (looked up once per device)
+static int noalloc_scratch(void** base) {
+    int dev = 0;
+    QCHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNaMaxDevices) {
+        set_error("qed2d_cg_noalloc: device ordinal out of range");
+        return QED2D_ERR_UNSUPPORTED;
+    }
+    std::lock_guard<std::mutex> lock(g_na_mutex);
+    if (!g_na_base[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_status(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        g_na_base[dev] = p;
+    }
+    *base = g_na_base[dev];
+    return QED2D_OK;
+}
+
+}  // namespace qed2d
+
+extern "C" int qed2d_cg_noalloc(int L1, int L2, double* so, const double* U, const double* si, double am0,
+                                int maxiter, double eps, void* stream, int* iterations) {
+    using namespace qed2d;
+    if (L1 < 2 || L2 < 2) {
+        set_error("qed2d_cg_noalloc: lattice extents must be >= 2");
+        return QED2D_ERR_BAD_ARG;
+    }
+    const long long V = (long long)L1 * L2;
+    if (V > QED2D_NOALLOC_MAX_SITES) {
+        set_error("qed2d_cg_noalloc: " + std::to_string(L1) + "x" + std::to_string(L2) + " = " + std::to_string(V) +
+                  " sites exceeds the static scratch limit of " + std::to_string(QED2D_NOALLOC_MAX_SITES) +
+                  " sites; use qed2d_cg");
+        return QED2D_ERR_BAD_ARG;
+    }
+    if (!so || !U || !si || maxiter < 0 || (reinterpret_cast<uintptr_t>(so) | reinterpret_cast<uintptr_t>(U) |
+                                            reinterpret_cast<uintptr_t>(si)) % 16 != 0) {
+        set_error("qed2d_cg_noalloc: NULL or misaligned array, or maxiter < 0");
+        return QED2D_ERR_BAD_ARG;
+    }
+    const size_t fb = sizeof(double2) * 2 * (size_t)V;
+    const char *a = (const char*)so, *b = (const char*)si;
+    if (a < b + fb && b < a + fb) {
+        set_error("qed2d_cg_noalloc: so aliases si");
+        return QED2D_ERR_BAD_ARG;
+    }
+    void* base = nullptr;
+    QTRY(noalloc_scratch(&base));
+    char* p = (char*)base;
+    DevCtl* ctl = (DevCtl*)p;
+    double* part = (double*)(p + kNaCtlBytes);
+    double2* fields = (double2*)(p + kNaCtlBytes + kNaPartBytes);
+    cudaStream_t s = (cudaStream_t)stream;
+
+    CGP P{};
+    P.g.L1 = L1;
+    P.g.L2 = L2;
+    P.g.V = V;
+    P.U = (const double2*)U;
+    P.b = (const double2*)si;
+    P.x = (double2*)so;
+    P.r = fields;
+    P.p0 = fields + 2 * QED2D_NOALLOC_MAX_SITES;
+    P.p1 = fields + 4 * QED2D_NOALLOC_MAX_SITES;
+    P.t = fields + 6 * QED2D_NOALLOC_MAX_SITES;
+    P.g5x = nullptr;
+    P.m2 = 2.0 + am0;
+    P.mu2 = 0.0;
+    P.eps = eps;
+    P.maxiter = maxiter;
+    P.guess = 0;
+    P.ctl = ctl;
+    P.part = part;
+
+    int dev = 0, sms = 0, per_sm = 0;
+    QCHECK(cudaGetDevice(&dev));
+    QCHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_f64, TILE, 0));
+    if (per_sm < 1) return QED2D_ERR_UNSUPPORTED;
+    long long grid = (long long)per_sm * sms;
+    if (grid > kMaxPartBlocks) grid = kMaxPartBlocks;
+    const long long nt = num_tiles(P.g);
+    const long long per_block = (nt + grid - 1) / grid;
+    grid = (nt + per_block - 1) / per_block;
+
+    QCHECK(cudaMemsetAsync(ctl, 0, sizeof(DevCtl), s));
+    void* args[] = {(void*)&P};
+    QCHECK(cudaLaunchCooperativeKernel((const void*)k_cg_f64, dim3((unsigned)grid), dim3(TILE), args, 0, s));
+    count_launch();
+    DevCtl h;
+    QCHECK(cudaMemcpyAsync(&h, ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, s));
+    QCHECK(cudaStreamSynchronize(s));
+    if (iterations) *iterations = h.last_iters;
+    if (h.status != QED2D_OK) set_error(std::string("qed2d_cg_noalloc: ") + qed2d_status_string(h.status));
+    return h.status;
+}

@@ -10,6 +10,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libqed2d.so")
 
 MAXPOLES = 32
+NOALLOC_MAX_SITES = 16384
 OK, NOT_CONVERGED, TIMEOUT, BAD_ARG, CUDA_ERR, NO_MEMORY, UNSUPPORTED = range(7)
 PREC_F64, PREC_MIXED, PREC_PLAIN = 0, 1, 2
 LEAPFROG, OMF4 = 0, 1
@@ -72,6 +73,7 @@ SIGNATURES = {
     "qed2d_cg": (I, [P, P, P, P, D, I, D, PI]),
     "qed2d_cg_shift": (I, [P, P, P, P, D, D, I, D, I, PI]),
     "qed2d_multishift_cg": (I, [P, PP, P, P, D, PD, I, I, D, PI]),
+    "qed2d_cg_noalloc": (I, [I, I, P, P, P, D, I, D, P, PI]),
     "qed2d_get_rhmc_params": (I, [I, D, D, PR]),
     "qed2d_multi_cg": (I, [P, P, P, P, D, I, D, PR, PI]),
     "qed2d_rational": (I, [P, P, P, P, D, I, D, PR, PI]),

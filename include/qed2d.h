@@ -170,6 +170,20 @@ int qed2d_cg_shift(qed2d_ctx* ctx, double* so, const double* U, const double* si
 int qed2d_multishift_cg(qed2d_ctx* ctx, double* const* so, const double* U, const double* si, double am0,
                         const double* mu, int n, int maxiter, double eps, int* iterations);
 
+/* No counterpart in the reference.  CG method 1 exactly as qed2d_cg, for callers
+ * that cannot allocate device memory while they run (a loop whose device memory
+ * is owned by its own pool allocator, or one that cannot afford the implicit
+ * device synchronisation of cudaMalloc): it needs no context and allocates
+ * nothing.  Its scratch is one static device array, held by every GPU that loads
+ * the library, sized for at most QED2D_NOALLOC_MAX_SITES = L1*L2 sites (larger
+ * lattices are rejected with QED2D_ERR_BAD_ARG).  The first call on a device looks
+ * up that array's address (make it before any stream capture).  All calls share
+ * the array: calls that overlap on the GPU race.  Work runs on `stream` (NULL:
+ * the legacy default stream); the call synchronises it. */
+#define QED2D_NOALLOC_MAX_SITES 16384
+int qed2d_cg_noalloc(int L1, int L2, double* so, const double* U, const double* si, double am0, int maxiter,
+                     double eps, void* stream, int* iterations);
+
 /* ---- RHMC: src/QED2dRHMC.jl ---- */
 /* get_rhmc_params -- :93-110 (host; Zolotarev coefficients) */
 int qed2d_get_rhmc_params(int n, double r_a, double r_b, qed2d_rhmc_params* out);
