@@ -551,3 +551,44 @@ def HMC_(U, *args, integrator: Integrators = None, qzero=False, reversibility_te
     if not reversibility_test:
         acc.append(int(res.accepted))
     return HMCInfo(res.accepted, res.hini, res.hfin, res.dH, res.qtop, res.cg_iterations, ctr)
+
+
+# ---------------------------------------------------------------------------
+# batched replicas (no single reference counterpart; include/qed2d.h)
+class Batch:
+    """nrep independent L1 x L2 lattices advanced together.  A batch field is a
+    CUDA tensor of shape (2, nrep, L2, L1): plane k of replica r is field[k, r],
+    itself in the reference layout.  Every replica follows HMC! Nf=2 with leapfrog
+    (src/QED2dHMC.jl:64-113) using the mixed solver; replica r draws exactly as a
+    single-lattice HMC_ with seed seeds[r]."""
+
+    def __init__(self, nrep, L1, L2, beta):
+        betas = [float(beta)] * nrep if not isinstance(beta, (list, tuple)) else [float(b) for b in beta]
+        self.nrep, self.L1, self.L2, self.beta = int(nrep), int(L1), int(L2), betas
+        h = C.c_void_p()
+        arr = (C.c_double * nrep)(*betas)
+        check(lib().qed2d_batch_create(self.nrep, self.L1, self.L2, arr, C.byref(h)), "batch_create")
+        self.h = h.value
+
+    def field(self, dtype=torch.complex128):
+        return torch.zeros((2, self.nrep, self.L2, self.L1), dtype=dtype, device="cuda")
+
+    def hmc_nf2(self, U, am0, eps, ns, CGmaxiter, tol, seeds, counter, qzero=False):
+        if tuple(U.shape) != (2, self.nrep, self.L2, self.L1) or U.dtype != torch.complex128 or not U.is_contiguous():
+            raise ValueError("U: expected a contiguous complex128 tensor of shape (2, nrep, L2, L1)")
+        ams = [float(am0)] * self.nrep if not isinstance(am0, (list, tuple)) else [float(a) for a in am0]
+        res = (_lib.HmcResult * self.nrep)()
+        L = lib()
+        check(L.qed2d_batch_set_stream(self.h, C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        st = L.qed2d_batch_hmc_nf2(self.h, C.c_void_p(U.data_ptr()), (C.c_double * self.nrep)(*ams), float(eps),
+                                   int(ns), int(CGmaxiter), float(tol), int(bool(qzero)),
+                                   (C.c_uint64 * self.nrep)(*[int(s) for s in seeds]), int(counter), res)
+        check(st, "batch HMC!")
+        return [HMCInfo(r.accepted, r.hini, r.hfin, r.dH, r.qtop, r.cg_iterations, int(counter)) for r in res]
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                lib().qed2d_batch_destroy(self.h)
+        except Exception:
+            pass

@@ -240,6 +240,21 @@ int qed2d_hmc_rhmc(qed2d_ctx* ctx, double* U, int nf, const double* am0, double 
                    double tol, const qed2d_rhmc_params* rprm, int qzero, int reversibility, uint64_t seed,
                    uint32_t counter, qed2d_hmc_result* res);
 
+/* ---- batched replicas (no single reference counterpart: the reference runs one
+ * chain per process; this runs nrep independent chains of the same lattice size
+ * together, each following HMC! Nf=2 with leapfrog, src/QED2dHMC.jl:64-113,426-481).
+ * A batch field is the reference layout of an L1 x (nrep*L2) lattice: element
+ * (i1, i2, replica r, plane k) at i1 + L1*(i2 + L2*(r + nrep*k)); direction 2
+ * wraps inside each replica.  Solves use the mixed FP32/FP64 solver. ---- */
+typedef struct qed2d_batch qed2d_batch;
+int qed2d_batch_create(int nrep, int L1, int L2, const double* beta, qed2d_batch** out);
+int qed2d_batch_destroy(qed2d_batch* batch);
+int qed2d_batch_set_stream(qed2d_batch* batch, void* cuda_stream);
+/* one trajectory of every replica: am0[nrep], seeds[nrep] (replica r draws as a
+ * single-lattice qed2d_hmc_nf2 with seed seeds[r] and the same counter); res[nrep] */
+int qed2d_batch_hmc_nf2(qed2d_batch* batch, double* U, const double* am0, double eps, int ns, int maxiter,
+                        double tol, int qzero, const uint64_t* seeds, uint32_t counter, qed2d_hmc_result* res);
+
 #ifdef __cplusplus
 }
 #endif
