@@ -1,14 +1,15 @@
 #!/usr/bin/env python
-"""Headline benchmark: Nf=2 HMC trajectories/s on a 512x512 lattice.
+"""Headline benchmark: Nf=2 HMC trajectories/s on 512x512 lattices.
 
-    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+    python bench.py [--gpus N --steps K --warmup W] [--batch B] [--impl reference]
 
-Workload (one "step" = one HMC trajectory): Nf=2 Wilson fermions, beta=4.0,
-m0=0.1, leapfrog ns=20, eps=0.05 (tau=1), every CG solved to |r|/|b| < 1e-12
-(the reference's stop rule with eps=1e-24), FP32-inner/FP64-reliable-update
-solver.  Synthetic data: a seeded hot start thermalised by 10 untimed pure-gauge
-trajectories.  The working set (~60 MB) fits in L2, so L2 is flushed (256 MiB
-write) between timed trajectories.
+Workload: Nf=2 Wilson fermions, beta=4.0, m0=0.1, leapfrog ns=20, eps=0.05
+(tau=1), every CG solved to |r|/|b| < 1e-12 (the reference's stop rule with
+eps=1e-24), mixed FP32-inner/FP64-reliable-update solver, B replica chains per
+GPU advanced together ("batched"); one "step" = one batched trajectory = B
+trajectories.  Synthetic data: a seeded hot start thermalised by 10 untimed
+pure-gauge trajectories, copied to every replica (distinct seeds).  L2 is
+flushed (256 MiB write) between timed steps.
 
 Prints one JSON line (rank 0).  Under torchrun every rank runs an independent
 replica chain (no collective on the data path): value = all ranks' trajectories
@@ -195,22 +196,28 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     dev = torch.device("cuda", local)
     Lb = _lib.lib()
+    B = args.batch
     prm = qed2d.LattParm((L, L), BETA)
-    seed = SEED + 7919 * rank
-    qed2d.seed(seed + 1)
+    seed0 = SEED + 7919 * rank
+    seeds = [seed0 + 101 * r for r in range(B)]
 
-    # --- set-up: hot start + pure-gauge thermalisation (untimed)
-    U = torch.from_numpy(hot_start(L, L, SEED)).to(dev)
+    # --- set-up (untimed): hot start, pure-gauge thermalisation, copied to every replica
+    U1 = torch.from_numpy(hot_start(L, L, SEED)).to(dev)
+    qed2d.seed(SEED + 1)
     for _ in range(THERM_TRAJ):
-        qed2d.HMC_(U, 0.1, 10, [], prm, None)
-    qed2d.set_precision("mixed")
-    qed2d.seed(seed)
+        qed2d.HMC_(U1, 0.1, 10, [], prm, None)
+    batch = qed2d.Batch(B, L, L, BETA)
+    U = batch.field()
+    for r in range(B):
+        U[:, r] = U1
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    acc = []
+    counter = [0]
 
     def step():
         flush.fill_(1.0)
-        return qed2d.HMC_(U, AM0, EPS, NS, acc, MAXITER, TOL, prm, None)
+        c = counter[0]
+        counter[0] += 1
+        return batch.hmc_nf2(U, AM0, EPS, NS, MAXITER, TOL, seeds, c)
 
     for _ in range(args.warmup):
         step()
@@ -232,23 +239,24 @@ def run_ours(args):
         t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         elapsed = float(t.item())
-    value = world * args.steps / elapsed
-    iters = [i.cg_iterations for i in infos]
+    value = world * B * args.steps / elapsed
+    flat = [i for step_infos in infos for i in step_infos]
 
-    # --- e2e: the same step through the C ABI with host buffers (H2D of the
-    # links from pinned memory, the trajectory, D2H of links + result)
-    h = qed2d.context(L, L, BETA)
+    # --- e2e: the same step through the C ABI with host buffers: H2D of the
+    # links from pinned memory, the batched trajectory, D2H of links + results
     U_host = U.cpu().pin_memory()
-    res = _lib.HmcResult()
-    e2e_steps = max(1, args.steps)
+    res = (_lib.HmcResult * B)()
+    am = (C.c_double * B)(*([AM0] * B))
+    sd = (C.c_uint64 * B)(*seeds)
+    Lb.qed2d_batch_set_stream(batch.h, C.c_void_p(torch.cuda.current_stream().cuda_stream))
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    for k in range(e2e_steps):
+    for k in range(args.steps):
         U.copy_(U_host, non_blocking=True)
-        st = Lb.qed2d_hmc_nf2(h, C.c_void_p(U.data_ptr()), AM0, EPS, NS, _lib.LEAPFROG, MAXITER, TOL, 0,
-                              seed, 50000 + k, C.byref(res))
-        _lib.check(st, "hmc_nf2")
+        st = Lb.qed2d_batch_hmc_nf2(batch.h, C.c_void_p(U.data_ptr()), am, EPS, NS, MAXITER, TOL, 0, sd,
+                                    50000 + k, res)
+        _lib.check(st, "batch_hmc_nf2")
         U_host.copy_(U, non_blocking=True)
     e1.record()
     torch.cuda.synchronize()
@@ -257,7 +265,7 @@ def run_ours(args):
         t = torch.tensor([e2e_t], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_t = float(t.item())
-    e2e = {"value": world * e2e_steps / e2e_t, "unit": "traj/s",
+    e2e = {"value": world * B * args.steps / e2e_t, "unit": "traj/s",
            "h2d_bytes_per_step": U.numel() * 16, "d2h_bytes_per_step": U.numel() * 16 + C.sizeof(res)}
 
     if dist:
@@ -266,58 +274,52 @@ def run_ours(args):
     if rank != 0:
         return 0
 
-    # --- roofline of the dominant kernel: one mixed CG solve (a single
-    # persistent launch) at the workload's field, timed with CUDA events
+    # --- roofline of the dominant kernel: one batched mixed CG launch solving
+    # every replica's (g5Dw)^2 x = b at the workload's fields, CUDA events
     peak, peak_kind = load_peaks()
-    X = qed2d.cfield(L, L)
-    X.copy_(torch.randn(2, L, L, dtype=torch.complex128, device=dev) / np.sqrt(2.0))
-    F = qed2d.cfield(L, L)
-    qed2d.gamm5Dw(F, U, X, AM0, prm)
-    Xs = qed2d.cfield(L, L)
+    src = (torch.randn(U.shape, dtype=torch.complex128, device=dev) / np.sqrt(2.0)).contiguous()
+    xs = torch.zeros_like(src)
     kern = []
-    for _ in range(4):
+    for _ in range(3):
         flush.fill_(1.0)
         a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a0.record()
-        it = qed2d.CG(Xs, U, F, AM0, MAXITER, TOL, qed2d.gamm5Dw_sqr_msq, prm, None)
+        its, upd = batch.cg(xs, U, src, AM0, MAXITER, TOL)
         a1.record()
         torch.cuda.synchronize()
-        it, _, upd = qed2d.last_solve(prm)
-        kern.append((a0.elapsed_time(a1) / 1e3, it, upd))
-    t_k, it_k, upd_k = min(kern[1:])
+        kern.append((a0.elapsed_time(a1) / 1e3, its, upd))
+    t_k, its, upd = min(kern[1:], key=lambda z: z[0])
     V = L * L
-    bytes_k = V * (B_MIXED_SETUP + it_k * B_MIXED_ITER + upd_k * B_MIXED_UPDATE)
+    bytes_k = V * sum(B_MIXED_SETUP + i * B_MIXED_ITER + u * B_MIXED_UPDATE for i, u in zip(its, upd))
     achieved = bytes_k / t_k / 1e9
     traffic = None
-    prof = os.path.join(REPO, "profiles", "cg_mixed_512_traffic.json")
-    if os.path.exists(prof):
-        try:
-            pj = json.load(open(prof))
-            traffic = pj["dram_bytes_per_iteration"] * it_k
-        except Exception:
-            traffic = None
-    roofline = {"kernel": "k_cg_mixed", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+    roofline = {"kernel": "k_b_cg_mixed", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                "note": f"one launch = one solve: {it_k} FP32 iterations x {B_MIXED_ITER:.0f} B/site + "
-                        f"{upd_k} FP64 reliable updates x {B_MIXED_UPDATE:.0f} B/site; working set L2-resident "
-                        f"at {L}^2 (effective bandwidth)"}
+                "note": f"one launch = one solve of all {B} replicas: per replica iterations {min(its)}-{max(its)} "
+                        f"x {B_MIXED_ITER:.0f} B/site + reliable updates {min(upd)}-{max(upd)} x "
+                        f"{B_MIXED_UPDATE:.0f} B/site; {B} x {L}^2 working set exceeds L2"}
 
-    # --- the plain FP64 GPU path (reference-structured) and the fused FP64 path,
-    # same trajectory (same seed and counter) as the first timed step
+    # --- single-chain baselines on the same field and draws as replica 0's first
+    # timed step: mixed (no batching), fused FP64, and the plain FP64 GPU path
     base = {}
-    for prec in (() if args.skip_baselines else ("plain", "f64")):
-        qed2d.set_precision(prec)
-        Ub = U.clone()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        info = qed2d.HMC_(Ub, AM0, EPS, NS, [], MAXITER, TOL, prm, None, counter=infos[0].counter)
-        torch.cuda.synchronize()
-        base[prec] = (time.perf_counter() - t0, info.cg_iterations)
-    qed2d.set_precision("mixed")
+    if not args.skip_baselines:
+        for prec in ("mixed", "f64", "plain"):
+            qed2d.set_precision(prec)
+            Ub = U1.clone()
+            qed2d.seed(seeds[0])
+            qed2d.HMC_(Ub.clone(), AM0, EPS, NS, [], MAXITER, TOL, prm, None, counter=args.warmup)   # warm-up
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            info = qed2d.HMC_(Ub, AM0, EPS, NS, [], MAXITER, TOL, prm, None, counter=args.warmup)
+            torch.cuda.synchronize()
+            base[prec] = (time.perf_counter() - t0, info.cg_iterations)
+        qed2d.set_precision("f64")
 
     # --- Dslash / CG-iteration HBM bandwidth at 8192^2 (working set >> L2)
     dslash = None
     if not args.skip_sweep:
+        del batch, U, xs, src
+        torch.cuda.empty_cache()
         Lbig = 8192
         pb = qed2d.LattParm((Lbig, Lbig), BETA)
         Ub = torch.polar(torch.ones(2, Lbig, Lbig, dtype=torch.float64, device=dev),
@@ -336,57 +338,63 @@ def run_ours(args):
         t_ap = a0.elapsed_time(a1) / 1e3 / n_ap
         Vb = Lbig * Lbig
         f64_gbs = B_DSLASH_F64 * Vb / t_ap / 1e9
-        # FP32 fused CG iterations (mixed solver capped at 60 iterations)
-        xs = torch.zeros_like(si)
+        qed2d.set_precision("mixed")
+        xb = torch.zeros_like(si)
         cg_runs = []
         for _ in range(2):
             a0.record()
             try:
-                qed2d.CG(xs, Ub, si, AM0, 60, TOL, qed2d.gamm5Dw_sqr_msq, pb, None)
+                qed2d.CG(xb, Ub, si, AM0, 60, TOL, qed2d.gamm5Dw_sqr_msq, pb, None)
             except qed2d.Qed2dError:
                 pass
             a1.record()
             torch.cuda.synchronize()
-            it, _, upd = qed2d.last_solve(pb)
-            cg_runs.append((a0.elapsed_time(a1) / 1e3, it, upd))
+            it, _, up = qed2d.last_solve(pb)
+            cg_runs.append((a0.elapsed_time(a1) / 1e3, it, up))
+        qed2d.set_precision("f64")
         t_cg, it_cg, upd_cg = cg_runs[-1]
         cg_gbs = Vb * (B_MIXED_SETUP + it_cg * B_MIXED_ITER + upd_cg * B_MIXED_UPDATE) / t_cg / 1e9
         dslash = {"lattice": f"{Lbig}x{Lbig}", "g5dw_f64_GBs": f64_gbs, "g5dw_f64_frac": f64_gbs / peak,
                   "g5dw_f64_us": t_ap * 1e6, "cg_mixed_GBs": cg_gbs, "cg_mixed_frac": cg_gbs / peak,
                   "cg_mixed_iters": it_cg, "cg_mixed_updates": upd_cg, "peak_GBs": peak, "peak_kind": peak_kind}
-        del Ub, si, so, xs
+        del Ub, si, so, xb
         torch.cuda.empty_cache()
 
     # --- CPU baseline: the oracle on the host cores, bounded sample
     cpu = None
     if not args.skip_cpu:
         from oracle import oracle as O
-        Uh = U.cpu().numpy()
-        dt, it = oracle_sample(Uh, seed, 999)
+        dt, it = oracle_sample(U1.cpu().numpy(), seeds[0], 999)
         cpu = {"value": 1.0 / ((NS + 1) * dt), "unit": "traj/s", "cores": O.num_threads(), "kind": "port",
                "sample": f"one update_momenta! (CG to 1e-24, {it} iterations, + forces) of the {L}x{L} workload "
-                         f"on the benchmark's field, x{NS + 1} per trajectory"}
+                         f"on the benchmark's field, x{NS + 1} per trajectory (one chain)"}
 
     line = {
         "metric": METRIC, "value": value, "unit": "traj/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
-        "data": f"synthetic: seeded hot start thermalised by {THERM_TRAJ} pure-gauge trajectories",
-        "config": {"workload": WORKLOAD, "L1": L, "L2": L, "beta": BETA, "m0": AM0, "ns": NS, "eps": EPS,
-                   "cg_tol_sq": TOL, "solver": "mixed FP32 inner / FP64 reliable updates, FP64 stop rule",
-                   "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"},
+        "data": f"synthetic: seeded hot start thermalised by {THERM_TRAJ} pure-gauge trajectories, copied to "
+                f"{B} replica chains with distinct seeds",
+        "config": {"workload": WORKLOAD, "replicas_per_gpu": B, "L1": L, "L2": L, "beta": BETA, "m0": AM0, "ns": NS,
+                   "eps": EPS, "cg_tol_sq": TOL,
+                   "solver": "batched mixed FP32 inner / FP64 reliable updates, FP64 stop rule",
+                   "step": f"one batched trajectory = {B} trajectories (one per replica chain)",
+                   "l2": f"flushed between steps (256 MiB write); working set {B} x ~60 MB",
+                   "parallelism": f"replicas x{world * B}"},
         "e2e": e2e,
         "roofline": roofline,
         "cpu_baseline": cpu,
         "clocks": clk,
         "gpu_launches": int(launches),
-        "trajectories": {"cg_iterations_mean": statistics.mean(iters), "accepted": sum(acc[-args.steps:]),
-                         "dH": [round(i.dH, 6) for i in infos]},
+        "trajectories": {"cg_iterations_per_trajectory_mean": statistics.mean(i.cg_iterations for i in flat),
+                         "accepted": sum(i.accepted for i in flat), "of": len(flat),
+                         "dH_replica0": [round(st[0].dH, 6) for st in infos]},
         "baselines": None if not base else {
-            "plain_f64_gpu_traj_s": 1.0 / base["plain"][0], "plain_f64_cg_iterations": base["plain"][1],
+            "single_chain_mixed_traj_s": 1.0 / base["mixed"][0],
             "f64_fused_gpu_traj_s": 1.0 / base["f64"][0], "f64_fused_cg_iterations": base["f64"][1],
-            "mixed_vs_plain": value / world / (1.0 / base["plain"][0]),
-            "mixed_vs_f64_fused": value / world / (1.0 / base["f64"][0])},
+            "plain_f64_gpu_traj_s": 1.0 / base["plain"][0], "plain_f64_cg_iterations": base["plain"][1],
+            "batched_vs_plain": value / world / (1.0 / base["plain"][0]),
+            "batched_vs_f64_fused": value / world / (1.0 / base["f64"][0])},
         "dslash_hbm": dslash,
     }
     print(json.dumps(line), flush=True)
@@ -399,6 +407,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch", type=int, default=16, help="replica chains per GPU advanced together")
     ap.add_argument("--skip-sweep", action="store_true", help="skip the 8192^2 Dslash bandwidth sweep")
     ap.add_argument("--skip-cpu", action="store_true", help="skip the oracle CPU baseline")
     ap.add_argument("--skip-baselines", action="store_true",

@@ -195,6 +195,7 @@ struct BCGP {
     double* part;
     int* out_iters;   // [B] iterations of this solve
     int* out_conv;    // [B]
+    int* out_upd;     // [B] FP64 reliable updates
 };
 
 __device__ __forceinline__ bool breduce(GridSync& gs, double v, const BCGP& P, double* smem, double* out) {
@@ -236,7 +237,7 @@ __global__ void __launch_bounds__(TILE) k_b_cg_mixed(const BCGP P) {
     __shared__ double s_bb[kMaxBatch], s_tol[kMaxBatch], s_rr[kMaxBatch], s_maxrr[kMaxBatch], s_s[kMaxBatch],
         s_beta[kMaxBatch], s_alpha[kMaxBatch], s_rr64[kMaxBatch], s_tmp[kMaxBatch], s_snew[kMaxBatch];
     __shared__ int s_act[kMaxBatch], s_it[kMaxBatch], s_conv[kMaxBatch], s_upd[kMaxBatch], s_r4[kMaxBatch],
-        s_first[kMaxBatch], s_any[2];
+        s_first[kMaxBatch], s_nupd[kMaxBatch], s_any[2];
     GridSync gs{&P.ctl->bar, &P.ctl->gen, &P.ctl->err};
     const int B = P.g.B;
     const int myr = blockIdx.x / P.bpr, lb = blockIdx.x % P.bpr;
@@ -268,6 +269,7 @@ __global__ void __launch_bounds__(TILE) k_b_cg_mixed(const BCGP P) {
         s_s[r] = s_bb[r] > 0.0 ? 1.0 / sqrt(s_bb[r]) : 0.0;
         s_first[r] = 1;
         s_beta[r] = 0.0;
+        s_nupd[r] = 0;
     }
     __syncthreads();
     // r32 = s b, x32 = 0 (and g5Dw x = 0 for a zero source)
@@ -350,6 +352,7 @@ __global__ void __launch_bounds__(TILE) k_b_cg_mixed(const BCGP P) {
                 const bool cand = rn < s_tol[r] * s_s[r] * s_s[r];
                 if (rn < P.delta2 * s_maxrr[r] || cand || k == P.maxiter) {
                     s_upd[r] = 1;
+                    s_nupd[r]++;
                     any = 1;
                 } else {
                     s_beta[r] = rn / s_rr[r];
@@ -438,6 +441,7 @@ done:
         for (int r = threadIdx.x; r < B; r += blockDim.x) {
             P.out_iters[r] = s_conv[r] ? s_it[r] : (s_it[r] ? s_it[r] : P.maxiter);
             P.out_conv[r] = ok && s_conv[r];
+            P.out_upd[r] = s_nupd[r];
         }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -476,7 +480,7 @@ struct qed2d_batch {
     double* dscal = nullptr;    // [kMaxBatch*5 * 2] per-replica sums (start, end)
     double* dpar = nullptr;     // [kMaxBatch * 2]: m2 (2+m0), beta
     uint64_t* dseed = nullptr;  // [kMaxBatch]
-    int* dint = nullptr;        // [kMaxBatch * 2]: iterations, converged of the last solve
+    int* dint = nullptr;        // [kMaxBatch * 3]: iterations, converged, reliable updates of the last solve
     long long* diters = nullptr;   // [kMaxBatch] accumulated iterations
     std::map<std::string, std::pair<void*, size_t>> ws;
     void* buf(const std::string& name, size_t bytes) {
@@ -540,6 +544,7 @@ int b_solve(qed2d_batch* h, const double2* U, const float4* U32, const double2* 
     P.part = h->part;
     P.out_iters = h->dint;
     P.out_conv = h->dint + kMaxBatch;
+    P.out_upd = h->dint + 2 * kMaxBatch;
     int per_sm = 0;
     QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_b_cg_mixed, TILE, 0));
     if (per_sm < 1) return QED2D_ERR_UNSUPPORTED;
@@ -607,7 +612,7 @@ int qed2d_batch_create(int nrep, int L1, int L2, const double* beta, qed2d_batch
     if (e == cudaSuccess) e = cudaMalloc(&h->dscal, sizeof(double) * kMaxBatch * 5 * 2);
     if (e == cudaSuccess) e = cudaMalloc(&h->dpar, sizeof(double) * kMaxBatch * 2);
     if (e == cudaSuccess) e = cudaMalloc(&h->dseed, sizeof(uint64_t) * kMaxBatch);
-    if (e == cudaSuccess) e = cudaMalloc(&h->dint, sizeof(int) * kMaxBatch * 2);
+    if (e == cudaSuccess) e = cudaMalloc(&h->dint, sizeof(int) * kMaxBatch * 3);
     if (e == cudaSuccess) e = cudaMalloc(&h->diters, sizeof(long long) * kMaxBatch);
     if (e == cudaSuccess) e = cudaMemset(h->ctl, 0, sizeof(DevCtl));
     if (e == cudaSuccess) e = cudaMemcpy(h->dpar + kMaxBatch, beta, sizeof(double) * nrep, cudaMemcpyHostToDevice);
@@ -641,6 +646,47 @@ int qed2d_batch_set_stream(qed2d_batch* h, void* stream) {
     if (!h) return QED2D_ERR_BAD_ARG;
     h->stream = (cudaStream_t)stream;
     return QED2D_OK;
+}
+
+int qed2d_batch_cg(qed2d_batch* h, double* x, const double* U, const double* b, const double* am0, int maxiter,
+                   double eps, int* iterations, int* updates) {
+    if (!h || !x || !U || !b || !am0 || maxiter < 0 ||
+        ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(U) | reinterpret_cast<uintptr_t>(b)) % 16)) {
+        set_error("qed2d_batch_cg: bad argument");
+        return QED2D_ERR_BAD_ARG;
+    }
+    const int B = h->g.B;
+    const size_t fb = sizeof(double2) * 2 * (size_t)h->g.V;
+    if ((const char*)x < (const char*)b + fb && (const char*)b < (const char*)x + fb) {
+        set_error("qed2d_batch_cg: x aliases b");
+        return QED2D_ERR_BAD_ARG;
+    }
+    cudaStream_t s = h->stream;
+    float4* U32 = h->field32("b_U32");
+    double2* G = h->field("b_G");
+    if (!U32 || !G) return QED2D_ERR_NO_MEMORY;
+    h->m2.assign(B, 0.0);
+    for (int r = 0; r < B; r++) h->m2[r] = 2.0 + am0[r];
+    QCHECK(cudaMemsetAsync(&h->ctl->status, 0, sizeof(int), s));
+    QCHECK(cudaMemsetAsync(h->diters, 0, sizeof(long long) * B, s));
+    Ctx tmp;
+    tmp.g.L1 = h->g.L1;
+    tmp.g.L2 = h->g.L2r * B;
+    tmp.g.V = h->g.V;
+    tmp.stream = s;
+    QTRY(launch_pack_links(tmp, U32, (const double2*)U));
+    QTRY(b_solve(h, (const double2*)U, U32, (const double2*)b, (double2*)x, G, maxiter, eps));
+    int hi[3 * kMaxBatch];
+    QCHECK(cudaMemcpyAsync(hi, h->dint, sizeof(hi), cudaMemcpyDeviceToHost, s));
+    QCHECK(cudaMemcpyAsync(h->ctl_host, h->ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, s));
+    QCHECK(cudaStreamSynchronize(s));
+    for (int r = 0; r < B; r++) {
+        if (iterations) iterations[r] = hi[r];
+        if (updates) updates[r] = hi[2 * kMaxBatch + r];
+    }
+    const int st = h->ctl_host->status;
+    if (st != QED2D_OK) set_error(std::string("qed2d_batch_cg: ") + qed2d_status_string(st));
+    return st;
 }
 
 int qed2d_batch_hmc_nf2(qed2d_batch* h, double* Ud, const double* am0, double eps, int ns, int maxiter, double tol,

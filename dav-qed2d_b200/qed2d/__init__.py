@@ -573,6 +573,22 @@ class Batch:
     def field(self, dtype=torch.complex128):
         return torch.zeros((2, self.nrep, self.L2, self.L1), dtype=dtype, device="cuda")
 
+    def cg(self, x, U, b, am0, maxiter, eps):
+        """Every replica's CG method 1 in one launch; returns (iterations, reliable updates) per replica."""
+        for t in (x, U, b):
+            if tuple(t.shape) != (2, self.nrep, self.L2, self.L1) or t.dtype != torch.complex128:
+                raise ValueError("expected complex128 tensors of shape (2, nrep, L2, L1)")
+        ams = [float(am0)] * self.nrep if not isinstance(am0, (list, tuple)) else [float(a) for a in am0]
+        its, upd = (C.c_int * self.nrep)(), (C.c_int * self.nrep)()
+        L = lib()
+        check(L.qed2d_batch_set_stream(self.h, C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        st = L.qed2d_batch_cg(self.h, C.c_void_p(x.data_ptr()), C.c_void_p(U.data_ptr()), C.c_void_p(b.data_ptr()),
+                              (C.c_double * self.nrep)(*ams), int(maxiter), float(eps), its, upd)
+        if st == _lib.NOT_CONVERGED:
+            raise Qed2dError(st, "CG not converged")
+        check(st, "batch CG")
+        return list(its), list(upd)
+
     def hmc_nf2(self, U, am0, eps, ns, CGmaxiter, tol, seeds, counter, qzero=False):
         if tuple(U.shape) != (2, self.nrep, self.L2, self.L1) or U.dtype != torch.complex128 or not U.is_contiguous():
             raise ValueError("U: expected a contiguous complex128 tensor of shape (2, nrep, L2, L1)")

@@ -93,6 +93,7 @@ SIGNATURES = {
     "qed2d_batch_create": (I, [I, I, I, PD, C.POINTER(C.c_void_p)]),
     "qed2d_batch_destroy": (I, [P]),
     "qed2d_batch_set_stream": (I, [P, P]),
+    "qed2d_batch_cg": (I, [P, P, P, P, PD, I, D, PI, PI]),
     "qed2d_batch_hmc_nf2": (I, [P, P, PD, D, I, I, D, I, C.POINTER(C.c_uint64), U32, PH]),
 }
 

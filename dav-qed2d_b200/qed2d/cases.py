@@ -3,7 +3,8 @@
     python -m qed2d.cases <case> --L 2048 [--maxiter 100] [--repeat 3]
 
 cases: g5dw (FP64 gamm5Dw apply), cg_mixed / cg_f64 (one persistent CG launch
-capped at --maxiter iterations), force (gamm5Dw + tr_dQwdU), updt (link update).  Seeded hot-start links and Gaussian sources; prints the
+capped at --maxiter iterations), force (gamm5Dw + tr_dQwdU), updt (link update),
+bcg (one batched mixed CG launch over --batch replicas).  Seeded hot-start links and Gaussian sources; prints the
 per-launch time of the last repeat.
 """
 import argparse
@@ -17,7 +18,8 @@ import qed2d
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["g5dw", "cg_mixed", "cg_f64", "force", "updt"])
+    ap.add_argument("case", choices=["g5dw", "cg_mixed", "cg_f64", "force", "updt", "bcg"])
+    ap.add_argument("--batch", type=int, default=4)
     ap.add_argument("--L", type=int, default=2048)
     ap.add_argument("--maxiter", type=int, default=100)
     ap.add_argument("--repeat", type=int, default=3)
@@ -30,6 +32,12 @@ def main(argv=None):
     si = torch.randn(2, L, L, dtype=torch.complex128, device="cuda", generator=g)
     so = torch.zeros_like(si)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if a.case == "bcg":
+        bt = qed2d.Batch(a.batch, L, L, 4.0)
+        Ub, bb, xb = bt.field(), bt.field(), bt.field()
+        for r in range(a.batch):
+            Ub[:, r] = U
+            bb[:, r] = torch.randn(2, L, L, dtype=torch.complex128, device="cuda", generator=g)
     for _ in range(a.repeat):
         ev0.record()
         if a.case == "g5dw":
@@ -45,12 +53,17 @@ def main(argv=None):
             qed2d.gamm5Dw(g5, U, si, 0.1, prm)
             f = torch.zeros(2, L, L, dtype=torch.float64, device="cuda")
             qed2d.tr_dQwdU(f, U, si, g5, prm)
+        elif a.case == "bcg":
+            try:
+                it = bt.cg(xb, Ub, bb, 0.1, a.maxiter, 1e-24)
+            except qed2d.Qed2dError:
+                it = "capped"
         elif a.case == "updt":
             mom = torch.randn(2, L, L, dtype=torch.float64, device="cuda", generator=g)
             qed2d.updt_fld_(U, mom, 0.01)
         ev1.record()
         torch.cuda.synchronize()
-    it = qed2d.last_solve(prm) if a.case.startswith("cg") else None
+    it = qed2d.last_solve(prm) if a.case.startswith("cg") else (it if a.case == "bcg" else None)
     print(f"{a.case} L={L}: {ev0.elapsed_time(ev1):.3f} ms  solve={it}")
     return 0
 

@@ -250,6 +250,11 @@ typedef struct qed2d_batch qed2d_batch;
 int qed2d_batch_create(int nrep, int L1, int L2, const double* beta, qed2d_batch** out);
 int qed2d_batch_destroy(qed2d_batch* batch);
 int qed2d_batch_set_stream(qed2d_batch* batch, void* cuda_stream);
+/* every replica's CG method 1 (src/QED2dSolver.jl:3-46) in one launch:
+ * x_r = ((g5Dw)^2)^-1 b_r with mass am0[r]; iterations[nrep] and updates[nrep]
+ * (FP64 reliable updates) may be NULL */
+int qed2d_batch_cg(qed2d_batch* batch, double* x, const double* U, const double* b, const double* am0, int maxiter,
+                   double eps, int* iterations, int* updates);
 /* one trajectory of every replica: am0[nrep], seeds[nrep] (replica r draws as a
  * single-lattice qed2d_hmc_nf2 with seed seeds[r] and the same counter); res[nrep] */
 int qed2d_batch_hmc_nf2(qed2d_batch* batch, double* U, const double* am0, double eps, int ns, int maxiter,

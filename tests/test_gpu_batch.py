@@ -56,3 +56,27 @@ def test_batch_rejects_bad_shape():
     with pytest.raises(ValueError):
         b.hmc_nf2(torch.zeros((2, 3, 16, 16), dtype=torch.complex128, device="cuda"), 0.3, 0.1, 2, 100, 1e-20,
                   [1, 2], 0)
+
+
+def test_batch_cg_matches_single_cg():
+    """qed2d_batch_cg: replica r's solution equals the single-lattice mixed solve (1e-9)."""
+    import torch
+
+    import qed2d
+    nrep, L1, L2 = 4, 48, 40
+    am0s = [0.2, 0.3, 0.4, 0.5]
+    b = qed2d.Batch(nrep, L1, L2, 4.0)
+    U, src, x = b.field(), b.field(), b.field()
+    for r in range(nrep):
+        U[:, r] = to_dev(hot_links(L1, L2, 200 + r))
+        src[:, r] = to_dev(cgauss(L1, L2, 300 + r, 2))
+    its, upd = b.cg(x, U, src, am0s, 20000, 1e-24)
+    qed2d.set_precision("mixed")
+    prm = qed2d.LattParm((L1, L2), 4.0)
+    for r in range(nrep):
+        xs = qed2d.cfield(L1, L2)
+        it = qed2d.CG(xs, U[:, r].contiguous(), src[:, r].contiguous(), am0s[r], 20000, 1e-24,
+                      qed2d.gamm5Dw_sqr_msq, prm, None)
+        assert rel(to_host(x[:, r]), to_host(xs)) < 1e-9
+        assert abs(its[r] - it) <= max(3, it // 20) and upd[r] >= 1
+    qed2d.set_precision("f64")
