@@ -58,6 +58,20 @@ __device__ __forceinline__ Site bsite(const BLat& g, int r, long long lt, int t)
     return s;
 }
 
+// the same without division: tile (t1, t2) of replica r
+__device__ __forceinline__ Site bsite_at(const BLat& g, int r, int t1, int t2, int t) {
+    Site s;
+    s.i1 = t1 * TX + (t & (TX - 1));
+    s.i2 = t2 * TY + (t >> 5);
+    s.ok = s.i1 < g.L1 && s.i2 < g.L2r;
+    s.x = s.i1 + g.L1 * (r * g.L2r + s.i2);   // 32-bit: V < 2^30 is checked at creation
+    s.xp1 = (s.i1 + 1 == g.L1) ? s.x - (g.L1 - 1) : s.x + 1;
+    s.xm1 = (s.i1 == 0) ? s.x + (g.L1 - 1) : s.x - 1;
+    s.xp2 = (s.i2 + 1 == g.L2r) ? s.x - (long long)(g.L2r - 1) * g.L1 : s.x + g.L1;
+    s.xm2 = (s.i2 == 0) ? s.x + (long long)(g.L2r - 1) * g.L1 : s.x - g.L1;
+    return s;
+}
+
 // ---------------------------------------------------------------------------
 // standalone batched kernels: grid = (tiles per replica, B)
 __global__ void __launch_bounds__(TILE) k_b_g5dw(double2* __restrict__ so, const double2* __restrict__ U,
@@ -190,7 +204,7 @@ struct BCGP {
     float4* x32;
     double m2[kMaxBatch];
     double eps, delta2;
-    int maxiter, bpr;
+    int maxiter, bpr, per_block;
     DevCtl* ctl;
     double* part;
     int* out_iters;   // [B] iterations of this solve
@@ -228,11 +242,13 @@ __device__ __forceinline__ bool breduce(GridSync& gs, double v, const BCGP& P, d
     return ld_volatile_int(gs.err) == 0;
 }
 
-#define FOR_MY_TILES(q)                                                              \
-    for (long long lt_ = lb; lt_ < P.g.ntr; lt_ += P.bpr)                            \
-        if (const Site q = bsite(P.g, myr, lt_, threadIdx.x); q.ok)
+// this block's contiguous range of its replica's tiles, walked without division
+#define FOR_MY_TILES(q)                                                                            \
+    for (int tt_ = TR.lo, t1_ = TR.s1, t2_ = TR.s2; tt_ < TR.hi;                                 \
+         ++tt_, (++t1_ == TR.nt1 ? (t1_ = 0, ++t2_) : 0))                                          \
+        if (const Site q = bsite_at(P.g, myr, t1_, t2_, threadIdx.x); q.ok)
 
-__global__ void __launch_bounds__(TILE) k_b_cg_mixed(const BCGP P) {
+__global__ void __launch_bounds__(TILE, 4) k_b_cg_mixed(const BCGP P) {
     __shared__ double smem[64];
     __shared__ double s_bb[kMaxBatch], s_tol[kMaxBatch], s_rr[kMaxBatch], s_maxrr[kMaxBatch], s_s[kMaxBatch],
         s_beta[kMaxBatch], s_alpha[kMaxBatch], s_rr64[kMaxBatch], s_tmp[kMaxBatch], s_snew[kMaxBatch];
@@ -241,6 +257,7 @@ __global__ void __launch_bounds__(TILE) k_b_cg_mixed(const BCGP P) {
     GridSync gs{&P.ctl->bar, &P.ctl->gen, &P.ctl->err};
     const int B = P.g.B;
     const int myr = blockIdx.x / P.bpr, lb = blockIdx.x % P.bpr;
+    const TileRange TR = tile_range(P.g.ntr, P.g.nt1, P.per_block, lb);
     const long long V = P.g.V;
     const LkD L{P.U, V};
     const LkF Lf{P.U32};
@@ -305,7 +322,7 @@ __global__ void __launch_bounds__(TILE) k_b_cg_mixed(const BCGP P) {
         const bool act = s_act[myr];
         // phase A: p = r + beta p_old, t = g5Dw p, <p,Ap>
         {
-            double v = 0.0;
+            float f = 0.f;   // per-thread sum in FP32, one conversion per phase
             if (act) {
                 const SpAxpy<float, SpF> Q{SpF{P.r32}, SpF{qo}, (float)s_beta[myr], !s_first[myr]};
                 FOR_MY_TILES(q) {
@@ -313,17 +330,17 @@ __global__ void __launch_bounds__(TILE) k_b_cg_mixed(const BCGP P) {
                     const Pair<float> tt = g5dw_at_c<float>(Q, c, Lf, q, m2f);
                     st_f(qn, q.x, c);
                     st_f(P.t32, q.x, tt);
-                    v += (double)(norm2(tt.a) + norm2(tt.b));
+                    f += norm2(tt.a) + norm2(tt.b);
                 }
             }
-            if (!breduce(gs, v, P, smem, s_tmp)) { ok = false; goto done; }
+            if (!breduce(gs, (double)f, P, smem, s_tmp)) { ok = false; goto done; }
         }
         for (int r = threadIdx.x; r < B; r += blockDim.x)
             if (s_act[r]) s_alpha[r] = s_rr[r] / s_tmp[r];
         __syncthreads();
         // phase B: x += alpha p, r -= alpha g5Dw t
         {
-            double v = 0.0;
+            float f = 0.f;
             if (act) {
                 const float alpha = (float)s_alpha[myr];
                 FOR_MY_TILES(q) {
@@ -336,10 +353,10 @@ __global__ void __launch_bounds__(TILE) k_b_cg_mixed(const BCGP P) {
                     r.b = r.b - alpha * a.b;
                     st_f(P.x32, q.x, xv);
                     st_f(P.r32, q.x, r);
-                    v += (double)(norm2(r.a) + norm2(r.b));
+                    f += norm2(r.a) + norm2(r.b);
                 }
             }
-            if (!breduce(gs, v, P, smem, s_tmp)) { ok = false; goto done; }
+            if (!breduce(gs, (double)f, P, smem, s_tmp)) { ok = false; goto done; }
         }
         // per-replica reliable-update decisions (identical in every block)
         if (threadIdx.x == 0) {
@@ -555,6 +572,7 @@ int b_solve(qed2d_batch* h, const double2* U, const float4* U32, const double2* 
     const long long per_block = (h->g.ntr + bpr - 1) / bpr;
     bpr = (h->g.ntr + per_block - 1) / per_block;
     P.bpr = (int)bpr;
+    P.per_block = (int)per_block;
     QCHECK(cudaMemsetAsync(&h->ctl->bar, 0, 2 * sizeof(unsigned long long) + sizeof(int), h->stream));
     void* args[] = {(void*)&P};
     QCHECK(cudaLaunchCooperativeKernel((const void*)k_b_cg_mixed, dim3((unsigned)(bpr * h->g.B)), dim3(TILE), args, 0,
@@ -597,8 +615,9 @@ extern "C" {
 int qed2d_batch_create(int nrep, int L1, int L2, const double* beta, qed2d_batch** out) {
     if (!out) return QED2D_ERR_BAD_ARG;
     *out = nullptr;
-    if (nrep < 1 || nrep > kMaxBatch || L1 < 2 || L2 < 2 || !beta) {
-        set_error("qed2d_batch_create: need 1 <= nrep <= 64, L1, L2 >= 2 and a beta per replica");
+    if (nrep < 1 || nrep > kMaxBatch || L1 < 2 || L2 < 2 || !beta ||
+        (long long)nrep * L1 * L2 > (1LL << 30)) {
+        set_error("qed2d_batch_create: need 1 <= nrep <= 64, L1, L2 >= 2, nrep*L1*L2 <= 2^30 and a beta per replica");
         return QED2D_ERR_BAD_ARG;
     }
     auto* h = new qed2d_batch();

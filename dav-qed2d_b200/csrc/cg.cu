@@ -57,6 +57,7 @@ struct CGP {
     double delta2;   // reliable-update threshold delta^2 (mixed)
     int maxiter;
     int guess;
+    int per_block;   // tiles per block (a contiguous range)
     DevCtl* ctl;
     double* part;
 };
@@ -124,16 +125,15 @@ __device__ __forceinline__ void finish_solve(const CGP& P, int iters, bool conv,
     }
 }
 
-#define FOR_TILES(q)                                                                     \
-    for (long long tile_ = blockIdx.x; tile_ < ntiles; tile_ += gridDim.x)              \
-        if (const Site q = site_of_tile(P.g, tile_, threadIdx.x); q.ok)
+#define FOR_TILES(q) FOR_RANGE(q, P.g, TR)
 
 // ---------------------------------------------------------------------------
 // FP64 persistent CG
-__global__ void __launch_bounds__(TILE) k_cg_f64(const CGP P) {
+__global__ void __launch_bounds__(TILE, 3) k_cg_f64(const CGP P) {
     __shared__ double smem[32 * 2];
     GridSync gs{&P.ctl->bar, &P.ctl->gen, &P.ctl->err};
     const long long ntiles = num_tiles(P.g), V = P.g.V;
+    const TileRange TR = tile_range(ntiles, (P.g.L1 + TX - 1) / TX, P.per_block, blockIdx.x);
     const LkD L{P.U, V};
     const double m2 = P.m2, mu2 = P.mu2;
     int k = 0;
@@ -225,10 +225,11 @@ done:
 
 // ---------------------------------------------------------------------------
 // mixed FP32/FP64 reliable-update CG
-__global__ void __launch_bounds__(TILE) k_cg_mixed(const CGP P) {
+__global__ void __launch_bounds__(TILE, 4) k_cg_mixed(const CGP P) {
     __shared__ double smem[32 * 2];
     GridSync gs{&P.ctl->bar, &P.ctl->gen, &P.ctl->err};
     const long long ntiles = num_tiles(P.g), V = P.g.V;
+    const TileRange TR = tile_range(ntiles, (P.g.L1 + TX - 1) / TX, P.per_block, blockIdx.x);
     const LkD L{P.U, V};
     const LkF Lf{P.U32};
     const double m2 = P.m2, mu2 = P.mu2;
@@ -298,17 +299,19 @@ __global__ void __launch_bounds__(TILE) k_cg_mixed(const CGP P) {
             float4* qn = cur ? P.q1 : P.q0;
             const float4* qo = cur ? P.q0 : P.q1;
             const SpAxpy<float, SpF> Q{SpF{P.r32}, SpF{qo}, (float)beta, !first};
-            double v[1] = {0.0};
+            float ft = 0.f, fc = 0.f;   // per-thread sums in FP32: one conversion per phase
             FOR_TILES(q) {
                 const Pair<float> c = Q.ld(q.x);
                 const Pair<float> tt = g5dw_at_c<float>(Q, c, Lf, q, m2f);
                 st_f(qn, q.x, c);
                 st_f(P.t32, q.x, tt);
-                v[0] += (double)(norm2(tt.a) + norm2(tt.b)) + mu2 * (double)(norm2(c.a) + norm2(c.b));
+                ft += norm2(tt.a) + norm2(tt.b);
+                fc += norm2(c.a) + norm2(c.b);
             }
+            double v[1] = {(double)ft + mu2 * (double)fc};
             if (!reduce_sync<1>(gs, v, P.part, P.ctl->red, smem)) goto done;
             const float alpha = (float)(rr / v[0]);
-            v[0] = 0.0;
+            float fr = 0.f;
             FOR_TILES(q) {
                 const Pair<float> pc = SpF{qn}.ld(q.x);
                 const Pair<float> a = g5dw_at<float>(SpF{P.t32}, Lf, q, m2f);
@@ -319,8 +322,9 @@ __global__ void __launch_bounds__(TILE) k_cg_mixed(const CGP P) {
                 r.b = r.b - alpha * (a.b + mu2f * pc.b);
                 st_f(P.x32, q.x, xv);
                 st_f(P.r32, q.x, r);
-                v[0] += (double)(norm2(r.a) + norm2(r.b));
+                fr += norm2(r.a) + norm2(r.b);
             }
+            v[0] = (double)fr;
             if (!reduce_sync<1>(gs, v, P.part, P.ctl->red, smem)) goto done;
             const double rn = v[0];
             maxrr = fmax(maxrr, rn);
@@ -408,16 +412,18 @@ struct MSP {
     double mu2b;
     double eps;
     int maxiter;
+    int per_block;
     DevCtl* ctl;
     double* part;
 };
 
-__global__ void __launch_bounds__(TILE) k_cg_multishift(const MSP P) {
+__global__ void __launch_bounds__(TILE, 3) k_cg_multishift(const MSP P) {
     __shared__ double smem[32 * 2];
     __shared__ double z[kMaxShifts], zp[kMaxShifts], ai[kMaxShifts], bi[kMaxShifts];
     __shared__ int upd[kMaxShifts], act[kMaxShifts];
     GridSync gs{&P.ctl->bar, &P.ctl->gen, &P.ctl->err};
     const long long ntiles = num_tiles(P.g), V = P.g.V;
+    const TileRange TR = tile_range(ntiles, (P.g.L1 + TX - 1) / TX, P.per_block, blockIdx.x);
     const LkD L{P.U, V};
     const double m2 = P.m2, mu2 = P.mu2b;
     int k = 0;
@@ -573,9 +579,11 @@ static int reset_barrier(Ctx& c) {   // bar, gen and err are contiguous
 }
 
 template <class K, class Par>
-static int launch_coop(Ctx& c, K kernel, const Par& P) {
+static int launch_coop(Ctx& c, K kernel, Par P) {
     int grid = 0;
     QTRY(coop_grid(c, kernel, &grid));
+    const long long nt = num_tiles(c.g);
+    P.per_block = (int)((nt + grid - 1) / grid);
     QTRY(reset_barrier(c));
     void* args[] = {(void*)&P};
     QCHECK(cudaLaunchCooperativeKernel((const void*)kernel, dim3(grid), dim3(TILE), args, 0, c.stream));
@@ -879,6 +887,7 @@ extern "C" int qed2d_cg_noalloc(int L1, int L2, double* so, const double* U, con
     const long long nt = num_tiles(P.g);
     const long long per_block = (nt + grid - 1) / grid;
     grid = (nt + per_block - 1) / per_block;
+    P.per_block = (int)per_block;
 
     QCHECK(cudaMemsetAsync(ctl, 0, sizeof(DevCtl), s));
     void* args[] = {(void*)&P};

@@ -341,6 +341,7 @@ int qed2d_ctx_create(int L1, int L2, double beta, qed2d_ctx** out) {
     if (!out) return bad_arg("out is NULL");
     *out = nullptr;
     if (L1 < 2 || L2 < 2) return bad_arg("lattice extents must be >= 2");
+    if ((long long)L1 * L2 > (1LL << 30)) return bad_arg("lattice volume above 2^30 sites");
     auto* h = new qed2d_ctx();
     Ctx& c = h->c;
     c.g.L1 = L1;

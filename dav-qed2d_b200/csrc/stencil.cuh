@@ -42,6 +42,39 @@ __host__ __device__ __forceinline__ long long num_tiles(const Lat& g) {
     return (long long)((g.L1 + TX - 1) / TX) * ((g.L2 + TY - 1) / TY);
 }
 
+// site of thread t in tile (t1, t2) -- no division; the persistent solvers walk
+// a block's contiguous tile range and advance (t1, t2) incrementally
+__device__ __forceinline__ Site site_at(const Lat& g, int t1, int t2, int t) {
+    Site s;
+    s.i1 = t1 * TX + (t & (TX - 1));
+    s.i2 = t2 * TY + (t >> 5);
+    s.ok = s.i1 < g.L1 && s.i2 < g.L2;
+    s.x = s.i1 + g.L1 * s.i2;   // 32-bit arithmetic: 2*V < 2^31 is checked at context creation
+    s.xp1 = (s.i1 + 1 == g.L1) ? s.x - (g.L1 - 1) : s.x + 1;
+    s.xm1 = (s.i1 == 0) ? s.x + (g.L1 - 1) : s.x - 1;
+    s.xp2 = (s.i2 + 1 == g.L2) ? (long long)s.i1 : s.x + g.L1;
+    s.xm2 = (s.i2 == 0) ? s.x + (g.V - g.L1) : s.x - g.L1;
+    return s;
+}
+
+// the block's contiguous tile range [lo, hi) and the coordinates of tile lo
+struct TileRange {
+    int lo, hi, s1, s2, nt1;
+};
+__device__ __forceinline__ TileRange tile_range(long long ntiles, int nt1, int per_block, int b) {
+    TileRange r;
+    r.lo = b * per_block;
+    r.hi = (int)min((long long)r.lo + per_block, ntiles);
+    r.s2 = r.lo / nt1;
+    r.s1 = r.lo - r.s2 * nt1;
+    r.nt1 = nt1;
+    return r;
+}
+#define FOR_RANGE(q, G, R)                                                                                    \
+    for (int tt_ = (R).lo, t1_ = (R).s1, t2_ = (R).s2; tt_ < (R).hi;                                        \
+         ++tt_, (++t1_ == (R).nt1 ? (t1_ = 0, ++t2_) : 0))                                                    \
+        if (const Site q = site_at((G), t1_, t2_, threadIdx.x); q.ok)
+
 // the same for a BX x BY tile visited by BX*BY threads (thread t -> (t % BX, t / BX))
 template <int BX, int BY>
 __device__ __forceinline__ Site site_of_tile_t(const Lat& g, long long tile, int t) {
