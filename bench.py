@@ -407,7 +407,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--batch", type=int, default=16, help="replica chains per GPU advanced together")
+    ap.add_argument("--batch", type=int, default=4, help="replica chains per GPU advanced together")
     ap.add_argument("--skip-sweep", action="store_true", help="skip the 8192^2 Dslash bandwidth sweep")
     ap.add_argument("--skip-cpu", action="store_true", help="skip the oracle CPU baseline")
     ap.add_argument("--skip-baselines", action="store_true",
