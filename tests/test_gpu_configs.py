@@ -1,0 +1,102 @@
+"""Parity cases at the sizes of the benchmark configurations.
+
+* Nf=1 RHMC at 128x128 with 12 Zolotarev poles on [lambda_min, lambda_max] from
+  the power method (src/QED2dHMC.jl:116-195, test/rhmc_pf_forcetest.jl:29-32):
+  one trajectory against the oracle replaying the same draws.
+* Master field at 8192x8192 built the reference's way (main/master_field.jl:
+  148-167: thermalise a small lattice, unfold it 2x2 repeatedly): checked through
+  size-independent properties -- OMF4 reversibility of the FP64 link and momentum
+  masters, a finite small Delta H, and Sum arg P / 2 pi equal to an integer.
+* Nf=2 at 64x64 with the mixed solver against the FP64 path and the oracle."""
+import numpy as np
+import pytest
+
+from helpers import cgauss, hot_links, rel, to_dev, to_host
+from oracle.oracle import Oracle, zolotarev
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def q():
+    import qed2d
+    yield qed2d
+    qed2d.set_precision("f64")
+
+
+def test_rhmc_128_twelve_poles_vs_oracle(q):
+    L, beta, am0 = 128, 4.0, [0.3]
+    prm = q.LattParm((L, L), beta)
+    o = Oracle(L, L, beta)
+    U0 = hot_links(L, L, 77)
+    Ud = to_dev(U0)
+    q.seed(5)
+    lmin, lmax = q.power_method(Ud, am0[0], prm, None, iter=300)
+    rp = [q.get_rhmc_params(12, np.sqrt(0.9 * lmin), np.sqrt(1.1 * lmax))]
+    ro = [zolotarev(12, np.sqrt(0.9 * lmin), np.sqrt(1.1 * lmax))]
+    info = q.HMC_(Ud, am0, 0.05, 4, [], 20000, 1e-24, prm, None, rp)
+    ctr = info.counter
+    mom0 = Oracle.normal(2 * L * L, 5, 1, ctr).reshape(2, L, L)
+    noise = [cgauss(L, L, 5, 16, ctr)]
+    st, Uo, acc, hi, hf, _ = o.hmc_rhmc(U0, am0, 0.05, 4, 20000, 1e-24, ro, mom0, noise, Oracle.uniform(5, 3, ctr))
+    assert st == 0
+    assert abs(info.hini - hi) < 1e-9 * abs(hi)
+    assert abs(info.dH - (hf - hi)) < 1e-7
+    assert info.accepted == acc
+    assert rel(to_host(Ud), Uo) < 1e-9
+
+
+def test_master_field_8192(q):
+    import torch
+    beta = 11.25
+    L = 16
+    U = torch.ones((2, L, L), dtype=torch.complex128, device="cuda")
+    q.seed(1234)
+    while True:
+        prm = q.LattParm((L, L), beta)
+        for _ in range(3):
+            q.HMC_(U, 0.1, 10, [], prm, None)
+        if L == 8192:
+            break
+        U = q.unfold_fld_(U, prm)
+        L *= 2
+    prm = q.LattParm((L, L), beta)
+    # integer topological charge of the unfolded field
+    Q = q.Qtop(U, prm)
+    assert abs(Q - round(Q)) < 1e-6
+    # OMF4 reversibility at 8192^2 (ns=20, eps=0.025 as the master-field config)
+    U0 = U.clone()
+    mom = torch.randn((2, L, L), dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(3))
+    H0 = q.Hamiltonian(mom, U, prm)
+    q.OMF4_(mom, U, 0.025, 20, prm, None)
+    H1 = q.Hamiltonian(mom, U, prm)
+    assert abs(H1 - H0) < 1e-2 * L * L / 1e6 + 50.0   # OMF4 energy error: small, extensive
+    mom.neg_()
+    q.OMF4_(mom, U, 0.025, 20, prm, None)
+    assert float((U - U0).abs().max()) < 1e-9
+    assert abs(q.Hamiltonian(mom, U, prm) - H0) < 1e-6 * abs(H0)
+
+
+def test_nf2_64_mixed_vs_f64_and_oracle(q):
+    L, beta, am0 = 64, 4.0, 0.1
+    prm = q.LattParm((L, L), beta)
+    U0 = hot_links(L, L, 31)
+    out = {}
+    for prec in ("f64", "mixed"):
+        q.set_precision(prec)
+        Ud = to_dev(U0)
+        q.seed(64)
+        out[prec] = (q.HMC_(Ud, am0, 0.05, 20, [], 20000, 1e-24, prm, None), to_host(Ud))
+    q.set_precision("f64")
+    info = out["f64"][0]
+    o = Oracle(L, L, beta)
+    mom0 = Oracle.normal(2 * L * L, 64, 1, info.counter).reshape(2, L, L)
+    noise = cgauss(L, L, 64, 16, info.counter)
+    st, Uo, acc, hi, hf, _ = o.hmc_nf2(U0, am0, 0.05, 20, 20000, 1e-24, mom0, noise,
+                                        Oracle.uniform(64, 3, info.counter))
+    assert st == 0
+    for prec in ("f64", "mixed"):
+        i, Uh = out[prec]
+        assert abs(i.dH - (hf - hi)) < 1e-7, prec
+        assert i.accepted == acc, prec
+        assert rel(Uh, Uo) < 1e-8, prec
