@@ -209,7 +209,7 @@ def run_ours(args):
     batch = qed2d.Batch(B, L, L, BETA)
     U = batch.field()
     for r in range(B):
-        U[:, r] = U1
+        U[r] = U1
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     counter = [0]
 

@@ -1,505 +1,706 @@
-// batch.cu -- batched replicas: B independent lattices of the same size advanced
-// together.  Every kernel of an Nf=2 trajectory covers all replicas, and every
-// force evaluation is ONE persistent mixed-precision CG launch that solves the B
-// systems at once (per-replica scalars, convergence and reliable updates), so
-// the grid barriers and launch latencies of a solve are paid once for B
-// lattices.  This is the batching of independent Markov chains (ensemble
-// generation); every replica follows exactly the algorithm of HMC! Nf=2
+// batch.cu -- batches of independent replica lattices, of equal or uneven sizes,
+// advanced together (ensemble generation: many Markov chains per GPU).  Every
+// kernel of an Nf=2 trajectory covers all replicas, and every force evaluation
+// is ONE persistent mixed-precision CG launch that solves all replicas' systems
+// at once, so the grid barriers and launch latencies of a solve are paid once
+// for the whole batch.  Each replica follows exactly the algorithm of HMC! Nf=2
 // (src/QED2dHMC.jl:64-113) with leapfrog (:426-481).
 //
-// Layout: a batch field is the reference layout of an L1 x (B*L2) lattice,
-//   element (i1, i2, replica r, plane k) at  i1 + L1*(i2 + L2*(r + B*k)),
-// so plane k of replica r is one contiguous reference-layout block of L1*L2
-// elements at offset (r + B*k)*L1*L2.  Neighbours in direction 2 wrap inside each
-// replica.  Random draws of replica r use its own seed and the element index of
-// a single lattice, so replica r reproduces a single-lattice run with seed r.
+// Layout (replica-major): replica r's field is an ordinary reference-layout
+// array ([L1_r, L2_r, 2], i1 fastest) starting at complex element 2*off_r, with
+// off_r the number of sites of the replicas before r; real fields (momenta)
+// start at real element 2*off_r.  Random draws of replica r use its own seed
+// and the single-lattice element order, so replica r reproduces a
+// single-lattice run with that seed.
+//
+// Work decomposition: a table lists every 32x8 tile of every replica, replica
+// after replica; a persistent block owns a contiguous range of the table and
+// walks it without division.  The tiles of one replica inside one block form a
+// "segment"; each segment writes one partial sum (fixed order inside), so
+// per-replica sums are deterministic.  The block arriving last at a barrier
+// sums each replica's segments, runs that replica's CG scalar recurrences
+// (state in global memory) and releases the others.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "stencil.cuh"
 
 namespace qed2d {
 
-constexpr int kMaxBatch = 64;
+constexpr int kMaxReplicas = 1024;
 
-struct BLat {
-    int L1, L2r, B;
-    long long Vr, V;   // sites per replica, total
-    int nt1;           // tiles along i1
-    long long ntr;     // tiles per replica
+struct RepInfo {
+    int L1, L2, nt1, nt;   // extents, tiles along i1, tiles of the replica
+    long long V, off;      // sites, first site of the replica in the batch
+    int tile0, pad;        // first entry of the replica in the tile table
 };
 
-static BLat make_blat(int B, int L1, int L2) {
-    BLat g;
-    g.L1 = L1;
-    g.L2r = L2;
-    g.B = B;
-    g.Vr = (long long)L1 * L2;
-    g.V = g.Vr * B;
-    g.nt1 = (L1 + TX - 1) / TX;
-    g.ntr = (long long)g.nt1 * ((L2 + TY - 1) / TY);
-    return g;
-}
+__host__ __device__ __forceinline__ Lat lat_of(const RepInfo& R) { return Lat{R.L1, R.L2, R.V}; }
 
-// site of thread t in local tile lt of replica r; neighbours wrap inside the replica
-__device__ __forceinline__ Site bsite(const BLat& g, int r, long long lt, int t) {
-    const int t2 = (int)(lt / g.nt1), t1 = (int)(lt - (long long)t2 * g.nt1);
-    Site s;
-    s.i1 = t1 * TX + (t & (TX - 1));
-    s.i2 = t2 * TY + (t >> 5);
-    s.ok = s.i1 < g.L1 && s.i2 < g.L2r;
-    s.x = s.i1 + (long long)g.L1 * ((long long)r * g.L2r + s.i2);
-    s.xp1 = (s.i1 + 1 == g.L1) ? s.x - (g.L1 - 1) : s.x + 1;
-    s.xm1 = (s.i1 == 0) ? s.x + (g.L1 - 1) : s.x - 1;
-    s.xp2 = (s.i2 + 1 == g.L2r) ? s.x - (long long)(g.L2r - 1) * g.L1 : s.x + g.L1;
-    s.xm2 = (s.i2 == 0) ? s.x + (long long)(g.L2r - 1) * g.L1 : s.x - g.L1;
-    return s;
-}
-
-// the same without division: tile (t1, t2) of replica r
-__device__ __forceinline__ Site bsite_at(const BLat& g, int r, int t1, int t2, int t) {
-    Site s;
-    s.i1 = t1 * TX + (t & (TX - 1));
-    s.i2 = t2 * TY + (t >> 5);
-    s.ok = s.i1 < g.L1 && s.i2 < g.L2r;
-    s.x = s.i1 + g.L1 * (r * g.L2r + s.i2);   // 32-bit: V < 2^30 is checked at creation
-    s.xp1 = (s.i1 + 1 == g.L1) ? s.x - (g.L1 - 1) : s.x + 1;
-    s.xm1 = (s.i1 == 0) ? s.x + (g.L1 - 1) : s.x - 1;
-    s.xp2 = (s.i2 + 1 == g.L2r) ? s.x - (long long)(g.L2r - 1) * g.L1 : s.x + g.L1;
-    s.xm2 = (s.i2 == 0) ? s.x + (long long)(g.L2r - 1) * g.L1 : s.x - g.L1;
-    return s;
-}
+struct TileView {
+    const RepInfo* reps;
+    const int4* tiles;   // (replica, t1, t2, 0)
+};
 
 // ---------------------------------------------------------------------------
-// standalone batched kernels: grid = (tiles per replica, B)
-__global__ void __launch_bounds__(TILE) k_b_g5dw(double2* __restrict__ so, const double2* __restrict__ U,
-                                                 const double2* __restrict__ si, BLat g, const double* __restrict__ m2) {
-    const int r = blockIdx.y;
-    const Site q = bsite(g, r, blockIdx.x, threadIdx.x);
+// standalone kernels: one block per entry of the tile table
+__global__ void __launch_bounds__(TILE) k_r_g5dw(double2* __restrict__ so, const double2* __restrict__ U,
+                                                 const double2* __restrict__ si, TileView tv,
+                                                 const double* __restrict__ m2) {
+    const int4 T = __ldg(tv.tiles + blockIdx.x);
+    const RepInfo R = tv.reps[T.x];
+    const Site q = site_at(lat_of(R), T.y, T.z, threadIdx.x);
     if (!q.ok) return;
-    st_d(so, g.V, q.x, g5dw_at<double>(SpDro{si, g.V}, LkD{U, g.V}, q, m2[r]));
+    const long long o = 2 * R.off;
+    st_d(so + o, R.V, q.x, g5dw_at<double>(SpDro{si + o, R.V}, LkD{U + o, R.V}, q, m2[T.x]));
 }
 
-__device__ __forceinline__ double b_im_plaq(const double2* U, const BLat& g, int r, int i1, int i2) {
-    const int iu1 = (i1 + 1 == g.L1) ? 0 : i1 + 1;
-    const int iu2 = (i2 + 1 == g.L2r) ? 0 : i2 + 1;
-    const long long row = (long long)r * g.L2r;
-    const long long x = i1 + (long long)g.L1 * (row + i2);
-    const double2 p = plaquette_of(__ldg(U + x), __ldg(U + g.V + iu1 + (long long)g.L1 * (row + i2)),
-                                   __ldg(U + i1 + (long long)g.L1 * (row + iu2)), __ldg(U + g.V + x));
-    return p.y;
-}
-
-// mom += eps (gauge force with beta_r + fermion force from (X, G)) -- k_mom_kick per replica
-__global__ void __launch_bounds__(TILE) k_b_mom_kick(double* __restrict__ mom, const double2* __restrict__ U,
-                                                     BLat g, const double* __restrict__ beta, double eps,
+// mom += eps (gauge force with beta_r + fermion force from (X, G = g5Dw X));
+// gauge part as krnl_force! (src/QED2dAction.jl:25-52)
+__global__ void __launch_bounds__(TILE) k_r_mom_kick(double* __restrict__ mom, const double2* __restrict__ U,
+                                                     TileView tv, const double* __restrict__ beta, double eps,
                                                      const double2* __restrict__ X, const double2* __restrict__ G) {
-    const int r = blockIdx.y;
-    const Site q = bsite(g, r, blockIdx.x, threadIdx.x);
+    const int4 T = __ldg(tv.tiles + blockIdx.x);
+    const RepInfo R = tv.reps[T.x];
+    const Lat g = lat_of(R);
+    const Site q = site_at(g, T.y, T.z, threadIdx.x);
     if (!q.ok) return;
-    const int im1 = (q.i1 == 0) ? g.L1 - 1 : q.i1 - 1;
-    const int im2 = (q.i2 == 0) ? g.L2r - 1 : q.i2 - 1;
-    const double b = beta[r];
-    const double v = b * b_im_plaq(U, g, r, q.i1, q.i2);
-    const double vm2 = b * b_im_plaq(U, g, r, q.i1, im2);
-    const double vm1 = b * b_im_plaq(U, g, r, im1, q.i2);
-    double F1 = -v + vm2, F2 = v - vm1;
+    const long long o = 2 * R.off;
+    double F1, F2;
+    gauge_force_at(U + o, g, q, beta[T.x], F1, F2);
     if (X) {
         double f1, f2;
-        fermion_force_at(U, X, G, g.V, q, f1, f2);
+        fermion_force_at(U + o, X + o, G + o, g.V, q, f1, f2);
         F1 = F1 + f1;
         F2 = F2 + f2;
     }
-    mom[q.x] = mom[q.x] + eps * F1;
-    mom[q.x + g.V] = mom[q.x + g.V] + eps * F2;
+    double* m = mom + o;
+    m[q.x] = m[q.x] + eps * F1;
+    m[q.x + g.V] = m[q.x + g.V] + eps * F2;
 }
 
-// N(0,1) fields of every replica: replica r draws with seed seeds[r] the doubles of
-// a single-lattice array of 2 Vr elements of dbl_per_elem doubles each (1: real
-// momenta, 2: complex noise), in the single-lattice order, and stores them in the
-// batch layout
-__global__ void k_b_random_normal(double* __restrict__ out, BLat g, int dbl_per_elem, const uint64_t* __restrict__ seeds,
-                                  uint32_t stream, uint32_t counter, double scale) {
-    // one thread per pair of doubles of one replica's single-lattice array
-    const int r = blockIdx.y;
-    const long long n = 2 * g.Vr * dbl_per_elem;   // doubles of one replica
-    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (2 * j >= n) return;
-    double z0, z1;
-    normal_pair(seeds[r], stream, counter, (uint64_t)j, z0, z1);
-    // double index d of the single-lattice array -> (plane, site, component)
-    for (int h = 0; h < 2; h++) {
-        const long long d = 2 * j + h;
-        if (d >= n) break;
-        const long long e = d / dbl_per_elem, comp = d - e * dbl_per_elem;
-        const long long k = e / g.Vr, x = e - k * g.Vr;
-        out[((k * g.B + r) * g.Vr + x) * dbl_per_elem + comp] = scale * (h ? z1 : z0);
+// U <- exp(i eps mom) U (updt_fld!, src/QED2dAction.jl:55-65) and the packed FP32
+// copy of the links; eps == 0 only packs
+__global__ void __launch_bounds__(TILE) k_r_updt(double2* __restrict__ U, const double* __restrict__ mom, double eps,
+                                                 float4* __restrict__ U32, TileView tv) {
+    const int4 T = __ldg(tv.tiles + blockIdx.x);
+    const RepInfo R = tv.reps[T.x];
+    const Site q = site_at(lat_of(R), T.y, T.z, threadIdx.x);
+    if (!q.ok) return;
+    double2* u = U + 2 * R.off;
+    double2 u1 = u[q.x], u2 = u[q.x + R.V];
+    if (eps != 0.0) {
+        const double* m = mom + 2 * R.off;
+        double s1, c1, s2, c2;
+        sincos(eps * m[q.x], &s1, &c1);
+        sincos(eps * m[q.x + R.V], &s2, &c2);
+        u1 = cmul(make_double2(c1, s1), u1);
+        u2 = cmul(make_double2(c2, s2), u2);
+        u[q.x] = u1;
+        u[q.x + R.V] = u2;
     }
+    U32[R.off + q.x] = make_float4((float)u1.x, (float)u1.y, (float)u2.x, (float)u2.y);
 }
 
-// per-replica sums: (Re P, arg P, mom^2, |X|^2, Re<X,F>) -- grid = (nb, B)
-constexpr int RBB = 256;
-__global__ void __launch_bounds__(RBB) k_b_reduce(const double2* __restrict__ U, const double* __restrict__ mom,
-                                                  const double2* __restrict__ X, const double2* __restrict__ F,
-                                                  BLat g, double* __restrict__ part, double* __restrict__ out) {
-    const int r = blockIdx.y;
+// N(0,1) doubles: one thread per pair of doubles of the batch array; the replica
+// is found by binary search over the replicas' first doubles dbase[0..nrep], and
+// the pair index inside the replica is the single-lattice one
+__global__ void k_r_random_normal(double* __restrict__ out, const long long* __restrict__ dbase, int nrep,
+                                  long long npairs, const uint64_t* __restrict__ seeds, uint32_t stream,
+                                  uint32_t counter, double scale) {
+    const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (p >= npairs) return;
+    const long long d = 2 * p;
+    int lo = 0, hi = nrep;   // find dbase[lo] <= d < dbase[lo + 1]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(dbase + mid) <= d) lo = mid;
+        else hi = mid;
+    }
+    double z0, z1;
+    normal_pair(seeds[lo], stream, counter, (uint64_t)((d - __ldg(dbase + lo)) >> 1), z0, z1);
+    out[d] = scale * z0;
+    out[d + 1] = scale * z1;
+}
+
+// per-tile sums (Re P, arg P, mom^2, |X|^2, Re<X,F>) -> part[tile*5 + k]
+__global__ void __launch_bounds__(TILE) k_r_reduce_tiles(const double2* __restrict__ U, const double* __restrict__ mom,
+                                                         const double2* __restrict__ X, const double2* __restrict__ F,
+                                                         TileView tv, double* __restrict__ part) {
+    const int4 T = __ldg(tv.tiles + blockIdx.x);
+    const RepInfo R = tv.reps[T.x];
+    const Lat g = lat_of(R);
+    const Site q = site_at(g, T.y, T.z, threadIdx.x);
+    const long long o = 2 * R.off;
     double v[5] = {0, 0, 0, 0, 0};
-    const long long row0 = (long long)r * g.L2r;
-    for (long long s = blockIdx.x * (long long)RBB + threadIdx.x; s < g.Vr; s += (long long)gridDim.x * RBB) {
-        const int i2 = (int)(s / g.L1), i1 = (int)(s - (long long)i2 * g.L1);
-        const long long x = i1 + (long long)g.L1 * (row0 + i2);
-        if (U) {
-            const int iu1 = (i1 + 1 == g.L1) ? 0 : i1 + 1, iu2 = (i2 + 1 == g.L2r) ? 0 : i2 + 1;
-            const double2 p = plaquette_of(__ldg(U + x), __ldg(U + g.V + iu1 + (long long)g.L1 * (row0 + i2)),
-                                           __ldg(U + i1 + (long long)g.L1 * (row0 + iu2)), __ldg(U + g.V + x));
-            v[0] += p.x;
-            v[1] += atan2(p.y, p.x);
-        }
-        if (mom) v[2] += mom[x] * mom[x] + mom[x + g.V] * mom[x + g.V];
+    if (q.ok) {
+        const double2* u = U + o;
+        const double2 p = plaquette_of(__ldg(u + q.x), __ldg(u + g.V + q.xp1), __ldg(u + q.xp2), __ldg(u + g.V + q.x));
+        v[0] = p.x;
+        v[1] = atan2(p.y, p.x);
+        if (mom) v[2] = mom[o + q.x] * mom[o + q.x] + mom[o + q.x + g.V] * mom[o + q.x + g.V];
         if (X) {
-            const double2 a = X[x], b = X[x + g.V];
-            v[3] += norm2(a) + norm2(b);
-            if (F) v[4] += cjmul(a, F[x]).x + cjmul(b, F[x + g.V]).x;
+            const double2 a = X[o + q.x], b = X[o + q.x + g.V];
+            v[3] = norm2(a) + norm2(b);
+            if (F) v[4] = cjmul(a, F[o + q.x]).x + cjmul(b, F[o + q.x + g.V]).x;
         }
     }
     __shared__ double smem[32 * 5];
     block_sum<5>(v, smem);
     if (threadIdx.x == 0)
-        for (int k = 0; k < 5; k++) part[((size_t)r * 5 + k) * gridDim.x + blockIdx.x] = v[k];
+        for (int k = 0; k < 5; k++) part[(size_t)blockIdx.x * 5 + k] = v[k];
 }
 
-// fixed-order final sums of k_b_reduce's partials: out[r*5 + k]
-__global__ void k_b_reduce_final(const double* __restrict__ part, int nb, int B, double* __restrict__ out) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    for (int rk = warp; rk < B * 5; rk += nw) {
-        double s = 0.0;
-        for (int i = lane; i < nb; i += 32) s += part[(size_t)rk * nb + i];
+// per-replica sums of the per-tile partials (one warp per replica, fixed order)
+__global__ void k_r_reduce_final(const double* __restrict__ part, const RepInfo* __restrict__ reps, int nrep,
+                                 double* __restrict__ out) {
+    const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (r >= nrep) return;   // whole warps leave together
+    const RepInfo R = reps[r];
+    double s[5] = {0, 0, 0, 0, 0};
+    for (int t = lane; t < R.nt; t += 32)
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) out[rk] = s;
+        for (int k = 0; k < 5; k++) s[k] += part[(size_t)(R.tile0 + t) * 5 + k];
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s[k] += __shfl_xor_sync(0xffffffffu, s[k], o);
+        if (lane == 0) out[(size_t)r * 5 + k] = s[k];
     }
 }
 
 // ---------------------------------------------------------------------------
-// Batched persistent mixed CG.  Block b serves replica b / bpr and that
-// replica's tiles lb, lb + bpr, ... (lb = b % bpr); its partial sums belong to
-// one replica, and the last block at a barrier sums each replica's partials in
-// a fixed order (deterministic).  Per-replica scalars live in shared memory,
-// computed identically in every block.  Replicas that have converged stop
-// working but keep joining the barriers until all are done.
-struct BCGP {
-    BLat g;
+// The persistent batched mixed CG: per replica, CG method 1 on (g5Dw)^2 + 0
+// (src/QED2dSolver.jl:3-46) with FP32 iterations on unit-norm rescaled vectors,
+// FP64 reliable updates, and the reference's FP64 stop rule |r|^2 < eps |b|^2.
+
+// Per-replica solver state: one 96-byte record per replica.  With at most
+// kSharedReps replicas every block keeps all records in shared memory and runs
+// the recurrences itself on the per-replica sums published by the block that
+// arrives last at a barrier (one L2 round trip per barrier).  Larger batches
+// keep the records in global memory; the last block updates them (one record =
+// six 16-byte loads issued together) and publishes the flags.
+constexpr int kSharedReps = 64;
+
+struct __align__(16) RepState {
+    double tol, rr, maxrr, s, beta, alpha, rr64, snew;
+    int act, conv, it, upd, r4, first, nupd, pad;
+};
+static_assert(sizeof(RepState) == 96, "RepState is six 16-byte words");
+
+// one record = four double2 + two int4 words, loaded and stored field-wise
+__device__ __forceinline__ RepState ld_state(const RepState* p) {
+    const double2* d = reinterpret_cast<const double2*>(p);
+    const int4* w = reinterpret_cast<const int4*>(p) + 4;
+    const double2 a = __ldcg(d), b = __ldcg(d + 1), c = __ldcg(d + 2), e = __ldcg(d + 3);
+    const int4 f = __ldcg(w), g = __ldcg(w + 1);
+    return RepState{a.x, a.y, b.x, b.y, c.x, c.y, e.x, e.y, f.x, f.y, f.z, f.w, g.x, g.y, g.z, g.w};
+}
+__device__ __forceinline__ void st_state(RepState* p, const RepState& s) {
+    double2* d = reinterpret_cast<double2*>(p);
+    int4* w = reinterpret_cast<int4*>(p) + 4;
+    d[0] = make_double2(s.tol, s.rr);
+    d[1] = make_double2(s.maxrr, s.s);
+    d[2] = make_double2(s.beta, s.alpha);
+    d[3] = make_double2(s.rr64, s.snew);
+    w[0] = make_int4(s.act, s.conv, s.it, s.upd);
+    w[1] = make_int4(s.r4, s.first, s.nupd, s.pad);
+}
+
+enum { FL_ACT, FL_UPD, FL_R4, FL_N };   // any replica active / updating / rescaling
+enum { RED_BB, RED_RR0, RED_PAP, RED_RN, RED_TRUE, RED_R4 };
+enum { PH_SETUP, PH_START, PH_A, PH_B, PH_R1, PH_R2, PH_R3, PH_R4 };
+
+struct RCGP {
+    int nrep, ntiles, per_block, lg;   // lg: log2 of the lanes summing one replica's segments
+    int nseg;
+    const RepInfo* reps;
+    const int4* tiles;
+    const int* seg0;      // [grid] first segment of each block
+    const int* rep_seg;   // [nrep+1] segments of replica r: rep_seg[r] .. rep_seg[r+1]-1
+    const double* m2;     // 2 + m0 per replica
     const double2* U;
     const float4* U32;
     const double2* b;
     double2* x;
     double2* r64;
     double2* t64;   // g5Dw x of the solution (the force needs it)
-    float4* r32;
-    float4* q0;
-    float4* q1;
-    float4* t32;
-    float4* x32;
-    double m2[kMaxBatch];
+    float4 *r32, *q0, *q1, *t32, *x32;
     double eps, delta2;
-    int maxiter, bpr, per_block;
+    int maxiter;
+    RepState* st;   // [nrep] (final state in both modes)
+    int* flags;     // [FL_N] (global-state mode)
+    double* red;    // [nrep] per-replica sums (shared-state mode)
+    double* part;   // one partial per segment
     DevCtl* ctl;
-    double* part;
-    int* out_iters;   // [B] iterations of this solve
-    int* out_conv;    // [B]
-    int* out_upd;     // [B] FP64 reliable updates
 };
 
-__device__ __forceinline__ bool breduce(GridSync& gs, double v, const BCGP& P, double* smem, double* out) {
-    __shared__ int s_last;
-    const int buf = gs.nred++ & 1;
-    double* part = P.part + (size_t)buf * (kMaxPartVals / 2) * kMaxPartBlocks;
-    double* red = part + kMaxPartBlocks;
-    double vv[1] = {v};
-    block_sum<1>(vv, smem);
-    if (threadIdx.x == 0) part[blockIdx.x] = vv[0];
+// where a block finds the records: shared memory or global memory
+template <bool SH>
+struct StateView {
+    RepState* sh;
+    const RepState* gl;
+    __device__ __forceinline__ RepState get(int r) const { return SH ? sh[r] : ld_state(gl + r); }
+};
+
+template <int PH>
+using acc_t = typename std::conditional<PH == PH_A || PH == PH_B, float, double>::type;
+
+// a replica's scalars for one phase (loaded once per segment)
+struct RepVals {
+    bool work, act, first;
+    double s, beta, alpha, snew, m2;
+};
+
+template <int PH, bool SH>
+__device__ __forceinline__ RepVals rep_vals(const StateView<SH>& sv, int r, double m2) {
+    RepVals v{};
+    v.m2 = m2;
+    if constexpr (PH == PH_SETUP) {
+        v.work = true;
+    } else {
+        const RepState st = sv.get(r);
+        v.act = st.act;
+        v.first = st.first;
+        v.s = st.s;
+        v.beta = st.beta;
+        v.alpha = st.alpha;
+        v.snew = st.snew;
+        if constexpr (PH == PH_START) v.work = true;
+        else if constexpr (PH == PH_A || PH == PH_B) v.work = st.act;
+        else if constexpr (PH == PH_R4) v.work = st.r4;
+        else v.work = st.upd;   // R1, R2, R3
+    }
+    return v;
+}
+
+// the work of phase PH on this thread's site of tile (t1, t2) of replica R;
+// returns the site's contribution to the phase's per-replica sum
+template <int PH>
+__device__ __forceinline__ acc_t<PH> tile_work(const RCGP& P, const RepVals& v, const RepInfo& R, int t1, int t2,
+                                               int cur) {
+    const Lat g = lat_of(R);
+    const Site q = site_at(g, t1, t2, threadIdx.x);
+    if (!q.ok) return 0;
+    const long long o2 = 2 * R.off, o1 = R.off, V = R.V;
+    const Pair<double> z{make_double2(0, 0), make_double2(0, 0)};
+    const Pair<float> zf{make_float2(0, 0), make_float2(0, 0)};
+    if constexpr (PH == PH_SETUP) {   // |b|^2, x = 0
+        const Pair<double> bv{__ldg(P.b + o2 + q.x), __ldg(P.b + o2 + q.x + V)};
+        st_d(P.x + o2, V, q.x, z);
+        return norm2(bv.a) + norm2(bv.b);
+    } else if constexpr (PH == PH_START) {   // r32 = s b, x32 = 0; a zero source keeps x = 0 and g5Dw x = 0
+        if (!v.act) {
+            st_d(P.t64 + o2, V, q.x, z);
+            return 0;
+        }
+        const Pair<float> r32{to_f(v.s * __ldg(P.b + o2 + q.x)), to_f(v.s * __ldg(P.b + o2 + q.x + V))};
+        st_f(P.r32 + o1, q.x, r32);
+        st_f(P.x32 + o1, q.x, zf);
+        return (double)(norm2(r32.a) + norm2(r32.b));
+    } else if constexpr (PH == PH_A) {   // p = r + beta p_old, t = g5Dw p, |t|^2 = <p, (g5Dw)^2 p>
+        float4* qn = cur ? P.q1 : P.q0;
+        const float4* qo = cur ? P.q0 : P.q1;
+        const SpAxpy<float, SpF> Q{SpF{P.r32 + o1}, SpF{qo + o1}, (float)v.beta, !v.first};
+        const Pair<float> c = Q.ld(q.x);
+        const Pair<float> tt = g5dw_at_c<float>(Q, c, LkF{P.U32 + o1}, q, (float)v.m2);
+        st_f(qn + o1, q.x, c);
+        st_f(P.t32 + o1, q.x, tt);
+        return norm2(tt.a) + norm2(tt.b);
+    } else if constexpr (PH == PH_B) {   // x += alpha p, r -= alpha g5Dw t
+        const float4* qn = cur ? P.q1 : P.q0;
+        const float alpha = (float)v.alpha;
+        const Pair<float> pc = SpF{qn + o1}.ld(q.x);
+        const Pair<float> a = g5dw_at<float>(SpF{P.t32 + o1}, LkF{P.U32 + o1}, q, (float)v.m2);
+        Pair<float> xv = SpF{P.x32 + o1}.ld(q.x), rv = SpF{P.r32 + o1}.ld(q.x);
+        xv.a = xv.a + alpha * pc.a;
+        xv.b = xv.b + alpha * pc.b;
+        rv.a = rv.a - alpha * a.a;
+        rv.b = rv.b - alpha * a.b;
+        st_f(P.x32 + o1, q.x, xv);
+        st_f(P.r32 + o1, q.x, rv);
+        return norm2(rv.a) + norm2(rv.b);
+    } else if constexpr (PH == PH_R1) {   // x += x32 / s, x32 = 0
+        const double inv_s = 1.0 / v.s;
+        const Pair<float> d = SpF{P.x32 + o1}.ld(q.x);
+        Pair<double> xv = SpD{P.x + o2, V}.ld(q.x);
+        xv.a = xv.a + inv_s * to_d(d.a);
+        xv.b = xv.b + inv_s * to_d(d.b);
+        st_d(P.x + o2, V, q.x, xv);
+        st_f(P.x32 + o1, q.x, zf);
+        return 0;
+    } else if constexpr (PH == PH_R2) {   // t64 = g5Dw x
+        st_d(P.t64 + o2, V, q.x, g5dw_at<double>(SpD{P.x + o2, V}, LkD{P.U + o2, V}, q, v.m2));
+        return 0;
+    } else if constexpr (PH == PH_R3) {   // r64 = b - g5Dw t64, |r64|^2
+        const Pair<double> a = g5dw_at<double>(SpD{P.t64 + o2, V}, LkD{P.U + o2, V}, q, v.m2);
+        Pair<double> rv;
+        rv.a = __ldg(P.b + o2 + q.x) - a.a;
+        rv.b = __ldg(P.b + o2 + q.x + V) - a.b;
+        st_d(P.r64 + o2, V, q.x, rv);
+        return norm2(rv.a) + norm2(rv.b);
+    } else {   // PH_R4: r32 = s_new r64
+        const Pair<float> r32{to_f(v.snew * P.r64[o2 + q.x]), to_f(v.snew * P.r64[o2 + q.x + V])};
+        st_f(P.r32 + o1, q.x, r32);
+        return (double)(norm2(r32.a) + norm2(r32.b));
+    }
+}
+
+// A block's place in the tile table (set once per launch, kept in shared
+// memory) and the records of its first kSegCache replicas, so that a phase
+// starts without global loads.
+constexpr int kSegCache = 16;
+struct BlockCtx {
+    int r0, t1, t2, seg, lo, hi, nsb;   // first replica and tile, first segment, tile range, segments
+};
+struct SegInfo {
+    RepInfo R;
+    double m2;
+};
+
+__device__ __forceinline__ void block_ctx_init(const RCGP& P, BlockCtx& bc, SegInfo* seg) {
+    if (threadIdx.x == 0) {
+        const int lo = blockIdx.x * P.per_block;
+        const int4 T0 = P.tiles[lo];
+        const int s0 = P.seg0[blockIdx.x];
+        const int s1 = blockIdx.x + 1 < gridDim.x ? P.seg0[blockIdx.x + 1] : P.nseg;
+        bc = BlockCtx{T0.x, T0.y, T0.z, s0, lo, min(lo + P.per_block, P.ntiles), s1 - s0};
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < min(bc.nsb, kSegCache); i += blockDim.x) {
+        seg[i].R = P.reps[bc.r0 + i];
+        seg[i].m2 = P.m2[bc.r0 + i];
+    }
+    __syncthreads();
+}
+
+// One phase over the block's tile range: the tiles of each replica form one
+// segment with one partial sum (phases R1 and R2 sum nothing).
+template <int PH, bool SH>
+__device__ __forceinline__ void run_phase(const RCGP& P, const StateView<SH>& sv, int cur, const BlockCtx& bcs,
+                                          const SegInfo* segs, double* smem) {
+    constexpr bool kSum = PH != PH_R1 && PH != PH_R2;
+    int t1 = bcs.t1, t2 = bcs.t2, tt = bcs.lo;
+    for (int i = 0;; i++) {
+        const int r = bcs.r0 + i;
+        const RepInfo R = i < kSegCache ? segs[i].R : P.reps[r];
+        const double m2 = i < kSegCache ? segs[i].m2 : __ldg(P.m2 + r);
+        const int n = min(bcs.hi - tt, R.nt - (t2 * R.nt1 + t1));
+        const RepVals v = rep_vals<PH, SH>(sv, r, m2);
+        acc_t<PH> acc = 0;
+        if (v.work)
+            for (int j = 0; j < n; j++) {
+                acc += tile_work<PH>(P, v, R, t1, t2, cur);
+                if (++t1 == R.nt1) {
+                    t1 = 0;
+                    ++t2;
+                }
+            }
+        if constexpr (kSum) {
+            double red[1] = {(double)acc};
+            block_sum<1>(red, smem);
+            if (threadIdx.x == 0) P.part[bcs.seg + i] = red[0];
+        }
+        tt += n;
+        if (tt >= bcs.hi) break;
+        t1 = 0;
+        t2 = 0;
+    }
+}
+
+// the CG scalar recurrences of one replica after reduction `kind` gave sum s
+// (the scalar steps of the single-lattice mixed solver)
+__device__ __forceinline__ void rep_step(RepState& st, int kind, double s, int k, double eps, double delta2,
+                                         int maxiter, int* fl) {
+    switch (kind) {
+        case RED_BB:
+            st.tol = eps * s;
+            st.act = s > 0.0;
+            st.conv = s == 0.0;
+            st.it = 0;
+            st.first = 1;
+            st.nupd = 0;
+            st.upd = 0;
+            st.r4 = 0;
+            st.rr64 = s;
+            st.s = s > 0.0 ? 1.0 / sqrt(s) : 0.0;
+            st.beta = 0.0;
+            fl[FL_ACT] |= st.act;
+            break;
+        case RED_RR0:
+            st.rr = s;
+            st.maxrr = s;
+            fl[FL_ACT] |= st.act;
+            break;
+        case RED_PAP:
+            if (st.act) st.alpha = st.rr / s;
+            break;
+        case RED_RN:
+            st.upd = 0;
+            if (st.act) {
+                st.maxrr = fmax(st.maxrr, s);
+                const bool cand = s < st.tol * st.s * st.s;
+                if (s < delta2 * st.maxrr || cand || k == maxiter) {
+                    st.upd = 1;
+                    st.nupd += 1;
+                    fl[FL_UPD] = 1;
+                } else {
+                    st.beta = s / st.rr;
+                    st.rr = s;
+                    st.rr64 = s / (st.s * st.s);
+                }
+                st.first = 0;
+            }
+            break;
+        case RED_TRUE:
+            st.r4 = 0;
+            if (st.upd) {
+                st.rr64 = s;
+                if (s < st.tol) {
+                    st.act = 0;
+                    st.conv = 1;
+                    st.it = k;
+                } else if (k == maxiter) {
+                    st.act = 0;
+                    st.it = k;
+                } else {
+                    st.r4 = 1;
+                    st.snew = 1.0 / sqrt(s);
+                    fl[FL_R4] = 1;
+                }
+            }
+            fl[FL_ACT] |= st.act;
+            break;
+        case RED_R4:
+            if (st.r4) {
+                st.beta = (st.rr64 * st.s * st.s / st.rr) * (st.snew / st.s);
+                st.s = st.snew;
+                st.rr = s;
+                st.maxrr = s;
+            }
+            fl[FL_ACT] |= st.act;
+            break;
+    }
+}
+
+// which flags reduction `kind` recomputes
+__device__ __forceinline__ void clear_flags(int kind, int* fl) {
+    if (kind == RED_BB || kind == RED_RR0 || kind == RED_TRUE || kind == RED_R4) fl[FL_ACT] = 0;
+    if (kind == RED_RN) fl[FL_UPD] = 0;
+    if (kind == RED_TRUE) fl[FL_R4] = 0;
+}
+
+// The last block's part of a barrier: per-replica sums of the segments (2^lg
+// lanes per replica, fixed order); SH publishes them, otherwise the records and
+// flags are updated here.
+template <bool SH>
+__device__ __forceinline__ void last_block_sums(const RCGP& P, const int* rseg, int* s_fl, int* s_bits, int kind,
+                                                int k) {
+    const int G = 1 << P.lg, span = P.nrep << P.lg;
+    int fl[FL_N] = {0, 0, 0};
+    for (int base = 0; base < span; base += blockDim.x) {   // same trip count in every thread
+        const int idx = base + threadIdx.x, r = idx >> P.lg, j = idx & (G - 1);
+        RepState st{};
+        if (!SH && idx < span && j == 0) st = ld_state(P.st + r);   // issued before the sums
+        double s = 0.0;
+        if (idx < span)
+            for (int i = rseg[r] + j, e = rseg[r + 1]; i < e; i += G) s += __ldcg(P.part + i);
+        for (int o = G >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (idx < span && j == 0) {
+            if (SH) {
+                P.red[r] = s;
+            } else {
+                rep_step(st, kind, s, k, P.eps, P.delta2, P.maxiter, fl);
+                st_state(P.st + r, st);
+            }
+        }
+    }
+    if (!SH) {
+        const int bits = __reduce_or_sync(0xffffffffu, fl[FL_ACT] | fl[FL_UPD] << 1 | fl[FL_R4] << 2);
+        if ((threadIdx.x & 31) == 0 && bits) atomicOr(s_bits, bits);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int g[FL_N] = {s_fl[FL_ACT], s_fl[FL_UPD], s_fl[FL_R4]};
+            clear_flags(kind, g);
+            g[FL_ACT] |= *s_bits & 1;
+            g[FL_UPD] |= (*s_bits >> 1) & 1;
+            g[FL_R4] |= (*s_bits >> 2) & 1;
+            for (int i = 0; i < FL_N; i++) {
+                s_fl[i] = g[i];
+                P.flags[i] = g[i];
+            }
+        }
+    }
+}
+
+// Grid barrier with per-replica sums (2^lg lanes per replica, fixed order).
+// SH: the last block publishes the sums and every block updates its shared
+// records; otherwise the last block updates the global records and flags.
+// s_fl (shared) holds the flags afterwards in every block.
+template <bool SH>
+__device__ __forceinline__ bool rbarrier(GridSync& gs, const RCGP& P, RepState* s_st, int* s_fl, const int* s_rseg,
+                                         int kind, int k) {
+    __shared__ int s_last, s_bits;
+    if (threadIdx.x == 0) s_bits = 0;   // arrive() begins with __syncthreads
     const bool last = gs.arrive(&s_last);
     if (last) {
         __threadfence();
-        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-        for (int r = warp; r < P.g.B; r += nw) {
-            double s = 0.0;
-            for (int i = lane; i < P.bpr; i += 32) s += __ldcg(part + (size_t)r * P.bpr + i);
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == 0) red[r] = s;
-        }
+        last_block_sums<SH>(P, SH ? s_rseg : P.rep_seg, s_fl, &s_bits, kind, k);
         __syncthreads();
         if (threadIdx.x == 0) gs.release();
     } else if (threadIdx.x == 0) {
         gs.wait();
+        if (!SH)
+            for (int i = 0; i < FL_N; i++) s_fl[i] = __ldcg(P.flags + i);
     }
     __syncthreads();
-    for (int r = threadIdx.x; r < P.g.B; r += blockDim.x) out[r] = __ldcg(red + r);
-    __syncthreads();
+    if (SH) {   // every block: the recurrences of every replica on the published sums
+        int fl[FL_N] = {0, 0, 0};
+        if (threadIdx.x < P.nrep) {   // nrep <= kSharedReps <= blockDim.x
+            const int r = threadIdx.x;
+            RepState st = s_st[r];
+            rep_step(st, kind, __ldcg(P.red + r), k, P.eps, P.delta2, P.maxiter, fl);
+            s_st[r] = st;
+        }
+        const int bits = __reduce_or_sync(0xffffffffu, fl[FL_ACT] | fl[FL_UPD] << 1 | fl[FL_R4] << 2);
+        if ((threadIdx.x & 31) == 0 && bits) atomicOr(&s_bits, bits);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            clear_flags(kind, s_fl);
+            s_fl[FL_ACT] |= s_bits & 1;
+            s_fl[FL_UPD] |= (s_bits >> 1) & 1;
+            s_fl[FL_R4] |= (s_bits >> 2) & 1;
+        }
+        __syncthreads();
+    }
     return ld_volatile_int(gs.err) == 0;
 }
 
-// this block's contiguous range of its replica's tiles, walked without division
-#define FOR_MY_TILES(q)                                                                            \
-    for (int tt_ = TR.lo, t1_ = TR.s1, t2_ = TR.s2; tt_ < TR.hi;                                 \
-         ++tt_, (++t1_ == TR.nt1 ? (t1_ = 0, ++t2_) : 0))                                          \
-        if (const Site q = bsite_at(P.g, myr, t1_, t2_, threadIdx.x); q.ok)
-
-__global__ void __launch_bounds__(TILE, 4) k_b_cg_mixed(const BCGP P) {
-    __shared__ double smem[64];
-    __shared__ double s_bb[kMaxBatch], s_tol[kMaxBatch], s_rr[kMaxBatch], s_maxrr[kMaxBatch], s_s[kMaxBatch],
-        s_beta[kMaxBatch], s_alpha[kMaxBatch], s_rr64[kMaxBatch], s_tmp[kMaxBatch], s_snew[kMaxBatch];
-    __shared__ int s_act[kMaxBatch], s_it[kMaxBatch], s_conv[kMaxBatch], s_upd[kMaxBatch], s_r4[kMaxBatch],
-        s_first[kMaxBatch], s_nupd[kMaxBatch], s_any[2];
-    GridSync gs{&P.ctl->bar, &P.ctl->gen, &P.ctl->err};
-    const int B = P.g.B;
-    const int myr = blockIdx.x / P.bpr, lb = blockIdx.x % P.bpr;
-    const TileRange TR = tile_range(P.g.ntr, P.g.nt1, P.per_block, lb);
-    const long long V = P.g.V;
-    const LkD L{P.U, V};
-    const LkF Lf{P.U32};
-    const double m2 = P.m2[myr];
-    const float m2f = (float)m2;
-    const Pair<double> z{make_double2(0, 0), make_double2(0, 0)};
-    bool ok = true;
-    int k = 0, cur = 0;
-
-    // |b|^2 per replica; x = 0
-    {
-        double v = 0.0;
-        FOR_MY_TILES(q) {
-            const Pair<double> bv{__ldg(P.b + q.x), __ldg(P.b + q.x + V)};
-            v += norm2(bv.a) + norm2(bv.b);
-            st_d(P.x, V, q.x, z);
-        }
-        if (!breduce(gs, v, P, smem, s_bb)) { ok = false; goto done; }
-    }
-    for (int r = threadIdx.x; r < B; r += blockDim.x) {
-        s_tol[r] = P.eps * s_bb[r];
-        s_act[r] = s_bb[r] > 0.0;
-        s_conv[r] = s_bb[r] == 0.0;
-        s_it[r] = 0;
-        s_rr64[r] = s_bb[r];
-        s_s[r] = s_bb[r] > 0.0 ? 1.0 / sqrt(s_bb[r]) : 0.0;
-        s_first[r] = 1;
-        s_beta[r] = 0.0;
-        s_nupd[r] = 0;
-    }
-    __syncthreads();
-    // r32 = s b, x32 = 0 (and g5Dw x = 0 for a zero source)
-    {
-        double v = 0.0;
-        const double s = s_s[myr];
-        const bool act = s_act[myr];
-        FOR_MY_TILES(q) {
-            if (act) {
-                const Pair<float> r32{to_f(s * __ldg(P.b + q.x)), to_f(s * __ldg(P.b + q.x + V))};
-                st_f(P.r32, q.x, r32);
-                st_f(P.x32, q.x, Pair<float>{make_float2(0, 0), make_float2(0, 0)});
-                v += (double)(norm2(r32.a) + norm2(r32.b));
-            } else {
-                st_d(P.t64, V, q.x, z);
-            }
-        }
-        if (!breduce(gs, v, P, smem, s_rr)) { ok = false; goto done; }
-    }
-    for (int r = threadIdx.x; r < B; r += blockDim.x) s_maxrr[r] = s_rr[r];
-    __syncthreads();
-
+// the solve; false when a barrier gave up
+template <bool SH>
+__device__ __forceinline__ bool r_body(const RCGP& P, GridSync& gs, int& k, double* smem, RepState* s_st, int* s_fl,
+                                       const int* s_rseg, const BlockCtx& bc, const SegInfo* segs) {
+    const StateView<SH> sv{s_st, P.st};
+    int cur = 0;
+    run_phase<PH_SETUP, SH>(P, sv, cur, bc, segs, smem);
+    if (!rbarrier<SH>(gs, P, s_st, s_fl, s_rseg, RED_BB, 0)) return false;
+    run_phase<PH_START, SH>(P, sv, cur, bc, segs, smem);
+    if (!rbarrier<SH>(gs, P, s_st, s_fl, s_rseg, RED_RR0, 0)) return false;
     for (k = 1; k <= P.maxiter; k++) {
-        if (threadIdx.x == 0) {
-            int any = 0;
-            for (int r = 0; r < B; r++) any |= s_act[r];
-            s_any[0] = any;
-        }
-        __syncthreads();
-        if (!s_any[0]) break;
-        float4* qn = cur ? P.q1 : P.q0;
-        const float4* qo = cur ? P.q0 : P.q1;
-        const bool act = s_act[myr];
-        // phase A: p = r + beta p_old, t = g5Dw p, <p,Ap>
-        {
-            float f = 0.f;   // per-thread sum in FP32, one conversion per phase
-            if (act) {
-                const SpAxpy<float, SpF> Q{SpF{P.r32}, SpF{qo}, (float)s_beta[myr], !s_first[myr]};
-                FOR_MY_TILES(q) {
-                    const Pair<float> c = Q.ld(q.x);
-                    const Pair<float> tt = g5dw_at_c<float>(Q, c, Lf, q, m2f);
-                    st_f(qn, q.x, c);
-                    st_f(P.t32, q.x, tt);
-                    f += norm2(tt.a) + norm2(tt.b);
-                }
-            }
-            if (!breduce(gs, (double)f, P, smem, s_tmp)) { ok = false; goto done; }
-        }
-        for (int r = threadIdx.x; r < B; r += blockDim.x)
-            if (s_act[r]) s_alpha[r] = s_rr[r] / s_tmp[r];
-        __syncthreads();
-        // phase B: x += alpha p, r -= alpha g5Dw t
-        {
-            float f = 0.f;
-            if (act) {
-                const float alpha = (float)s_alpha[myr];
-                FOR_MY_TILES(q) {
-                    const Pair<float> pc = SpF{qn}.ld(q.x);
-                    const Pair<float> a = g5dw_at<float>(SpF{P.t32}, Lf, q, m2f);
-                    Pair<float> xv = SpF{P.x32}.ld(q.x), r = SpF{P.r32}.ld(q.x);
-                    xv.a = xv.a + alpha * pc.a;
-                    xv.b = xv.b + alpha * pc.b;
-                    r.a = r.a - alpha * a.a;
-                    r.b = r.b - alpha * a.b;
-                    st_f(P.x32, q.x, xv);
-                    st_f(P.r32, q.x, r);
-                    f += norm2(r.a) + norm2(r.b);
-                }
-            }
-            if (!breduce(gs, (double)f, P, smem, s_tmp)) { ok = false; goto done; }
-        }
-        // per-replica reliable-update decisions (identical in every block)
-        if (threadIdx.x == 0) {
-            int any = 0;
-            for (int r = 0; r < B; r++) {
-                s_upd[r] = 0;
-                if (!s_act[r]) continue;
-                const double rn = s_tmp[r];
-                s_maxrr[r] = fmax(s_maxrr[r], rn);
-                const bool cand = rn < s_tol[r] * s_s[r] * s_s[r];
-                if (rn < P.delta2 * s_maxrr[r] || cand || k == P.maxiter) {
-                    s_upd[r] = 1;
-                    s_nupd[r]++;
-                    any = 1;
-                } else {
-                    s_beta[r] = rn / s_rr[r];
-                    s_rr[r] = rn;
-                    s_rr64[r] = rn / (s_s[r] * s_s[r]);
-                }
-                s_first[r] = 0;
-            }
-            s_any[1] = any;
-        }
-        __syncthreads();
-        if (s_any[1]) {
-            const bool upd = s_upd[myr];
-            const double inv_s = 1.0 / s_s[myr];
-            if (upd) FOR_MY_TILES(q) {   // x += x32 / s
-                    const Pair<float> d = SpF{P.x32}.ld(q.x);
-                    Pair<double> xv = SpD{P.x, V}.ld(q.x);
-                    xv.a = xv.a + inv_s * to_d(d.a);
-                    xv.b = xv.b + inv_s * to_d(d.b);
-                    st_d(P.x, V, q.x, xv);
-                    st_f(P.x32, q.x, Pair<float>{make_float2(0, 0), make_float2(0, 0)});
-                }
-            if (!gs.sync()) { ok = false; goto done; }
-            if (upd) FOR_MY_TILES(q) st_d(P.t64, V, q.x, g5dw_at<double>(SpD{P.x, V}, L, q, m2));
-            if (!gs.sync()) { ok = false; goto done; }
-            double w = 0.0;
-            if (upd) FOR_MY_TILES(q) {   // r64 = b - A x
-                    const Pair<double> a = g5dw_at<double>(SpD{P.t64, V}, L, q, m2);
-                    Pair<double> r;
-                    r.a = __ldg(P.b + q.x) - a.a;
-                    r.b = __ldg(P.b + q.x + V) - a.b;
-                    st_d(P.r64, V, q.x, r);
-                    w += norm2(r.a) + norm2(r.b);
-                }
-            if (!breduce(gs, w, P, smem, s_tmp)) { ok = false; goto done; }
-            if (threadIdx.x == 0) {
-                int any = 0;
-                for (int r = 0; r < B; r++) {
-                    s_r4[r] = 0;
-                    if (!s_upd[r]) continue;
-                    const double rrt = s_tmp[r];
-                    s_rr64[r] = rrt;
-                    if (rrt < s_tol[r]) {
-                        s_act[r] = 0;
-                        s_conv[r] = 1;
-                        s_it[r] = k;
-                    } else if (k == P.maxiter) {
-                        s_act[r] = 0;
-                        s_it[r] = k;
-                    } else {
-                        s_r4[r] = 1;
-                        s_snew[r] = 1.0 / sqrt(rrt);
-                        any = 1;
-                    }
-                }
-                s_any[1] = any;
-            }
-            __syncthreads();
-            if (s_any[1]) {
-                double v = 0.0;
-                if (s_r4[myr]) {
-                    const double sn = s_snew[myr];
-                    FOR_MY_TILES(q) {   // r32 = s_new r64
-                        const Pair<float> r32{to_f(sn * P.r64[q.x]), to_f(sn * P.r64[q.x + V])};
-                        st_f(P.r32, q.x, r32);
-                        v += (double)(norm2(r32.a) + norm2(r32.b));
-                    }
-                }
-                if (!breduce(gs, v, P, smem, s_tmp)) { ok = false; goto done; }
-                for (int r = threadIdx.x; r < B; r += blockDim.x)
-                    if (s_r4[r]) {
-                        const double s = s_s[r], sn = s_snew[r];
-                        s_beta[r] = (s_rr64[r] * s * s / s_rr[r]) * (sn / s);
-                        s_s[r] = sn;
-                        s_rr[r] = s_tmp[r];
-                        s_maxrr[r] = s_tmp[r];
-                    }
-                __syncthreads();
+        if (!s_fl[FL_ACT]) break;
+        run_phase<PH_A, SH>(P, sv, cur, bc, segs, smem);
+        if (!rbarrier<SH>(gs, P, s_st, s_fl, s_rseg, RED_PAP, k)) return false;
+        run_phase<PH_B, SH>(P, sv, cur, bc, segs, smem);
+        if (!rbarrier<SH>(gs, P, s_st, s_fl, s_rseg, RED_RN, k)) return false;
+        if (s_fl[FL_UPD]) {
+            run_phase<PH_R1, SH>(P, sv, cur, bc, segs, smem);
+            if (!gs.sync()) return false;
+            run_phase<PH_R2, SH>(P, sv, cur, bc, segs, smem);
+            if (!gs.sync()) return false;
+            run_phase<PH_R3, SH>(P, sv, cur, bc, segs, smem);
+            if (!rbarrier<SH>(gs, P, s_st, s_fl, s_rseg, RED_TRUE, k)) return false;
+            if (s_fl[FL_R4]) {
+                run_phase<PH_R4, SH>(P, sv, cur, bc, segs, smem);
+                if (!rbarrier<SH>(gs, P, s_st, s_fl, s_rseg, RED_R4, k)) return false;
             }
         }
         cur ^= 1;
     }
-done:
+    return true;
+}
+
+template <bool SH>
+__global__ void __launch_bounds__(TILE, 4) k_r_cg_mixed(const RCGP P) {
+    __shared__ double smem[32];
+    __shared__ RepState s_st[SH ? kSharedReps : 1];
+    __shared__ int s_fl[FL_N];
+    __shared__ BlockCtx s_bc;
+    __shared__ SegInfo s_seg[kSegCache];
+    __shared__ int s_rseg[SH ? kSharedReps + 1 : 1];   // the replicas' segment ranges (SH)
+    if (threadIdx.x < FL_N) s_fl[threadIdx.x] = 0;
+    if (SH)
+        for (int r = threadIdx.x; r <= P.nrep; r += blockDim.x) s_rseg[r] = P.rep_seg[r];
+    block_ctx_init(P, s_bc, s_seg);
+    GridSync gs{&P.ctl->bar, &P.ctl->gen, &P.ctl->err};
+    int k = 0;
+    const bool ok = r_body<SH>(P, gs, k, smem, s_st, s_fl, s_rseg, s_bc, s_seg);
     if (blockIdx.x == 0) {
-        DevCtl* c = P.ctl;
-        for (int r = threadIdx.x; r < B; r += blockDim.x) {
-            P.out_iters[r] = s_conv[r] ? s_it[r] : (s_it[r] ? s_it[r] : P.maxiter);
-            P.out_conv[r] = ok && s_conv[r];
-            P.out_upd[r] = s_nupd[r];
-        }
-        __syncthreads();
+        if (SH && ok)   // every block holds the same records: block 0 stores them
+            for (int r = threadIdx.x; r < P.nrep; r += blockDim.x) P.st[r] = s_st[r];
         if (threadIdx.x == 0) {
-            const int err = ld_volatile_int(&c->err);
-            int all = ok;
-            long long tot = 0;
-            for (int r = 0; r < B; r++) {
-                all &= s_conv[r];
-                tot += P.out_iters[r];
-            }
+            DevCtl* c = P.ctl;
             c->last_iters = k;
-            c->iters_total += tot;
-            if (c->status == 0) {
-                if (err || !ok) c->status = QED2D_ERR_TIMEOUT;
-                else if (!all) c->status = QED2D_ERR_NOT_CONVERGED;
-            }
+            if (c->status == 0 && (ld_volatile_int(&c->err) || !ok)) c->status = QED2D_ERR_TIMEOUT;
         }
     }
 }
 
+// per-replica outputs of a solve: iterations, reliable updates; accumulated
+// iterations; status NOT_CONVERGED when a replica did not converge
+__global__ void k_r_finish(const RepState* __restrict__ st, int nrep, int maxiter, int* __restrict__ it_out,
+                           int* __restrict__ upd_out, long long* __restrict__ acc, DevCtl* ctl) {
+    if (ctl->status != 0) return;   // a solve that gave up leaves no per-replica results
+    int bad = 0;
+    for (int r = threadIdx.x; r < nrep; r += blockDim.x) {
+        const RepState s = st[r];
+        const int its = s.conv ? s.it : (s.it ? s.it : maxiter);
+        it_out[r] = its;
+        upd_out[r] = s.nupd;
+        acc[r] += its;
+        bad |= !s.conv;
+    }
+    bad = __syncthreads_or(bad);
+    if (threadIdx.x == 0 && bad) ctl->status = QED2D_ERR_NOT_CONVERGED;
+}
+
 }  // namespace qed2d
+
+#include "batch_cg_uniform.cuh"
 
 // ===========================================================================
 // host side
 using namespace qed2d;
 
 struct qed2d_batch {
-    BLat g;
+    int nrep = 0, ntiles = 0;
+    long long Vtot = 0;
+    std::vector<RepInfo> reps;
+    std::vector<double> beta, m2;
     int device = 0, num_sms = 148;
     cudaStream_t stream = nullptr;
-    std::vector<double> beta;
-    std::vector<double> m2;     // 2 + m0 per replica, set by each trajectory
+    int grid = 0, per_block = 0, nseg = 0, lg = 0;   // persistent CG geometry
+    RepInfo* d_reps = nullptr;
+    int4* d_tiles = nullptr;
+    int* d_seg0 = nullptr;
+    int* d_rep_seg = nullptr;
+    long long* d_dbase_c = nullptr;   // first double of each replica: complex fields [nrep+1]
+    long long* d_dbase_r = nullptr;   // the same for real fields
+    double* d_m2 = nullptr;
+    double* d_beta = nullptr;
+    uint64_t* d_seed = nullptr;
+    RepState* d_st = nullptr;       // [nrep] solver records
+    int* d_flags = nullptr;         // [FL_N]
+    double* d_red = nullptr;        // [nrep]
+    bool shared_state = false;      // records in shared memory (nrep <= kSharedReps)
+    bool uniform = false;           // equal sizes, nrep <= kUniformReps: k_u_cg_mixed
+    UGeom ug{};
+    int ugrid = 0, ubpr = 0, uper_block = 0;
+    double* d_upart = nullptr;      // [2][ubpr * nrep]
+    double* d_ured = nullptr;       // [2][nrep]
+    int* d_out = nullptr;           // [2][nrep]: iterations, reliable updates of the last solve
+    long long* d_iters = nullptr;   // [nrep] iterations accumulated over a trajectory
+    double* d_sums = nullptr;       // [2][nrep][5] start / end sums of a trajectory
+    double* d_tpart = nullptr;      // [ntiles][5]
+    double* d_part = nullptr;       // [nseg]
     DevCtl* ctl = nullptr;
     DevCtl* ctl_host = nullptr;
-    double* part = nullptr;
-    double* dscal = nullptr;    // [kMaxBatch*5 * 2] per-replica sums (start, end)
-    double* dpar = nullptr;     // [kMaxBatch * 2]: m2 (2+m0), beta
-    uint64_t* dseed = nullptr;  // [kMaxBatch]
-    int* dint = nullptr;        // [kMaxBatch * 3]: iterations, converged, reliable updates of the last solve
-    long long* diters = nullptr;   // [kMaxBatch] accumulated iterations
     std::map<std::string, std::pair<void*, size_t>> ws;
+
     void* buf(const std::string& name, size_t bytes) {
         auto it = ws.find(name);
         if (it != ws.end() && it->second.second >= bytes) return it->second.first;
@@ -516,31 +717,53 @@ struct qed2d_batch {
         ws[name] = {p, bytes};
         return p;
     }
-    double2* field(const char* n) { return (double2*)buf(n, sizeof(double2) * 2 * g.V); }
-    double* real2(const char* n) { return (double*)buf(n, sizeof(double) * 2 * g.V); }
-    float4* field32(const char* n) { return (float4*)buf(n, sizeof(float4) * g.V); }
+    double2* field(const char* n) { return (double2*)buf(n, sizeof(double2) * 2 * Vtot); }
+    double* real2(const char* n) { return (double*)buf(n, sizeof(double) * 2 * Vtot); }
+    float4* field32(const char* n) { return (float4*)buf(n, sizeof(float4) * Vtot); }
+    TileView tv() const { return TileView{d_reps, d_tiles}; }
 };
 
 namespace {
 
-int b_post(const char* name) {
+int r_post(const char* name) {
     count_launch();
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? QED2D_OK : cuda_status(e, name);
 }
 
-dim3 b_tiles(const qed2d_batch* h) { return dim3((unsigned)h->g.ntr, (unsigned)h->g.B); }
-
-// accumulate this solve's per-replica iterations
-__global__ void k_b_acc_iters(long long* acc, const int* it, int B) {
-    const int r = threadIdx.x;
-    if (r < B) acc[r] += it[r];
+int r_fill(qed2d_batch* h, double* out, bool complex_field, uint32_t stream, uint32_t counter, double scale) {
+    const long long npairs = complex_field ? 2 * h->Vtot : h->Vtot;   // pairs of doubles
+    k_r_random_normal<<<(unsigned)((npairs + 255) / 256), 256, 0, h->stream>>>(
+        out, complex_field ? h->d_dbase_c : h->d_dbase_r, h->nrep, npairs, h->d_seed, stream, counter, scale);
+    return r_post("k_r_random_normal");
 }
 
-int b_solve(qed2d_batch* h, const double2* U, const float4* U32, const double2* b, double2* x, double2* g5x,
+int r_sums(qed2d_batch* h, const double2* U, const double* mom, const double2* X, const double2* F, int slot) {
+    k_r_reduce_tiles<<<h->ntiles, TILE, 0, h->stream>>>(U, mom, X, F, h->tv(), h->d_tpart);
+    QTRY(r_post("k_r_reduce_tiles"));
+    k_r_reduce_final<<<(h->nrep + 7) / 8, 256, 0, h->stream>>>(h->d_tpart, h->d_reps, h->nrep,
+                                                                h->d_sums + (size_t)slot * h->nrep * 5);
+    return r_post("k_r_reduce_final");
+}
+
+int r_pack(qed2d_batch* h, double2* U, const double* mom, double eps, float4* U32) {
+    k_r_updt<<<h->ntiles, TILE, 0, h->stream>>>(U, mom, eps, U32, h->tv());
+    return r_post("k_r_updt");
+}
+
+int r_solve(qed2d_batch* h, const double2* U, const float4* U32, const double2* b, double2* x, double2* g5x,
             int maxiter, double eps) {
-    BCGP P{};
-    P.g = h->g;
+    RCGP P{};
+    P.nrep = h->nrep;
+    P.ntiles = h->ntiles;
+    P.per_block = h->per_block;
+    P.lg = h->lg;
+    P.nseg = h->nseg;
+    P.reps = h->d_reps;
+    P.tiles = h->d_tiles;
+    P.seg0 = h->d_seg0;
+    P.rep_seg = h->d_rep_seg;
+    P.m2 = h->d_m2;
     P.U = U;
     P.U32 = U32;
     P.b = b;
@@ -553,90 +776,211 @@ int b_solve(qed2d_batch* h, const double2* U, const float4* U32, const double2* 
     P.t32 = h->field32("b_t32");
     P.x32 = h->field32("b_x32");
     if (!P.r64 || !P.r32 || !P.q0 || !P.q1 || !P.t32 || !P.x32) return QED2D_ERR_NO_MEMORY;
-    for (int r = 0; r < h->g.B; r++) P.m2[r] = h->m2[r];
     P.eps = eps;
     P.delta2 = 0.05 * 0.05;
     P.maxiter = maxiter;
+    P.st = h->d_st;
+    P.flags = h->d_flags;
+    P.red = h->d_red;
+    P.part = h->d_part;
     P.ctl = h->ctl;
-    P.part = h->part;
-    P.out_iters = h->dint;
-    P.out_conv = h->dint + kMaxBatch;
-    P.out_upd = h->dint + 2 * kMaxBatch;
-    int per_sm = 0;
-    QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_b_cg_mixed, TILE, 0));
-    if (per_sm < 1) return QED2D_ERR_UNSUPPORTED;
-    long long maxg = (long long)per_sm * h->num_sms;
-    if (maxg > kMaxPartBlocks) maxg = kMaxPartBlocks;
-    long long bpr = maxg / h->g.B;
-    if (bpr < 1) return QED2D_ERR_UNSUPPORTED;
-    const long long per_block = (h->g.ntr + bpr - 1) / bpr;
-    bpr = (h->g.ntr + per_block - 1) / per_block;
-    P.bpr = (int)bpr;
-    P.per_block = (int)per_block;
     QCHECK(cudaMemsetAsync(&h->ctl->bar, 0, 2 * sizeof(unsigned long long) + sizeof(int), h->stream));
     void* args[] = {(void*)&P};
-    QCHECK(cudaLaunchCooperativeKernel((const void*)k_b_cg_mixed, dim3((unsigned)(bpr * h->g.B)), dim3(TILE), args, 0,
-                                       h->stream));
+    if (h->uniform) {
+        UCGP Q{};
+        Q.g = h->ug;
+        Q.U = U;
+        Q.U32 = U32;
+        Q.b = b;
+        Q.x = x;
+        Q.t64 = g5x;
+        Q.r64 = P.r64;
+        Q.r32 = P.r32;
+        Q.q0 = P.q0;
+        Q.q1 = P.q1;
+        Q.t32 = P.t32;
+        Q.x32 = P.x32;
+        for (int r = 0; r < h->nrep; r++) Q.m2[r] = h->m2[r];
+        Q.eps = eps;
+        Q.delta2 = P.delta2;
+        Q.maxiter = maxiter;
+        Q.bpr = h->ubpr;
+        Q.per_block = h->uper_block;
+        Q.ctl = h->ctl;
+        Q.part = h->d_upart;
+        Q.red = h->d_ured;
+        Q.st_out = h->d_st;
+        void* uargs[] = {(void*)&Q};
+        QCHECK(cudaLaunchCooperativeKernel((const void*)k_u_cg_mixed, dim3((unsigned)h->ugrid), dim3(TILE), uargs, 0,
+                                           h->stream));
+    } else {
+        const void* kern = h->shared_state ? (const void*)k_r_cg_mixed<true> : (const void*)k_r_cg_mixed<false>;
+        QCHECK(cudaLaunchCooperativeKernel(kern, dim3((unsigned)h->grid), dim3(TILE), args, 0, h->stream));
+    }
     count_launch();
-    k_b_acc_iters<<<1, kMaxBatch, 0, h->stream>>>(h->diters, h->dint, h->g.B);
-    return b_post("k_b_acc_iters");
+    k_r_finish<<<1, 256, 0, h->stream>>>(h->d_st, h->nrep, maxiter, h->d_out, h->d_out + h->nrep, h->d_iters, h->ctl);
+    return r_post("k_r_finish");
 }
 
-int b_reduce(qed2d_batch* h, const double2* U, const double* mom, const double2* X, const double2* F, int slot) {
-    long long nb = (h->g.Vr + RBB - 1) / RBB;
-    const long long cap = (long long)(kMaxPartVals * kMaxPartBlocks) / (5LL * h->g.B);
-    if (nb > 64) nb = 64;
-    if (nb > cap) nb = cap;
-    k_b_reduce<<<dim3((unsigned)nb, (unsigned)h->g.B), RBB, 0, h->stream>>>(U, mom, X, F, h->g, h->part,
-                                                                             h->dscal + slot * kMaxBatch * 5);
-    QTRY(b_post("k_b_reduce"));
-    k_b_reduce_final<<<1, 256, 0, h->stream>>>(h->part, (int)nb, h->g.B, h->dscal + slot * kMaxBatch * 5);
-    return b_post("k_b_reduce_final");
+int r_kick(qed2d_batch* h, double* mom, const double2* U, const float4* U32, double2* X, const double2* F, double2* G,
+           double eps, int maxiter, double tol) {
+    QTRY(r_solve(h, U, U32, F, X, G, maxiter, tol));
+    k_r_mom_kick<<<h->ntiles, TILE, 0, h->stream>>>(mom, U, h->tv(), h->d_beta, eps, X, G);
+    return r_post("k_r_mom_kick");
 }
 
-int b_fill(qed2d_batch* h, double* out, int dbl_per_elem, uint32_t stream, uint32_t counter, double scale) {
-    const long long pairs = h->g.Vr * dbl_per_elem;   // 2 Vr dbl_per_elem doubles per replica
-    k_b_random_normal<<<dim3((unsigned)((pairs + 255) / 256), (unsigned)h->g.B), 256, 0, h->stream>>>(
-        out, h->g, dbl_per_elem, h->dseed, stream, counter, scale);
-    return b_post("k_b_random_normal");
+template <class T>
+int upload(T** d, const std::vector<T>& v) {
+    QCHECK(cudaMalloc(d, sizeof(T) * std::max<size_t>(v.size(), 1)));
+    QCHECK(cudaMemcpy(*d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+    return QED2D_OK;
 }
 
-int b_kick(qed2d_batch* h, double* mom, const double2* U, const float4* U32, double2* X, const double2* F,
-           double2* G, double eps, int maxiter, double tol) {
-    QTRY(b_solve(h, U, U32, F, X, G, maxiter, tol));
-    k_b_mom_kick<<<b_tiles(h), TILE, 0, h->stream>>>(mom, U, h->g, h->dpar + kMaxBatch, eps, X, G);
-    return b_post("k_b_mom_kick");
+// replica table, tile table, persistent-grid geometry and (block, replica) segments
+int batch_setup(qed2d_batch* h, const int* L1, const int* L2, const double* beta) {
+    const int B = h->nrep;
+    std::vector<int4> tiles;
+    long long off = 0;
+    for (int r = 0; r < B; r++) {
+        RepInfo R{};
+        R.L1 = L1[r];
+        R.L2 = L2[r];
+        R.nt1 = (L1[r] + TX - 1) / TX;
+        const int nt2 = (L2[r] + TY - 1) / TY;
+        R.nt = R.nt1 * nt2;
+        R.V = (long long)L1[r] * L2[r];
+        R.off = off;
+        R.tile0 = (int)tiles.size();
+        for (int t2 = 0; t2 < nt2; t2++)
+            for (int t1 = 0; t1 < R.nt1; t1++) tiles.push_back(make_int4(r, t1, t2, 0));
+        off += R.V;
+        h->reps.push_back(R);
+    }
+    h->Vtot = off;
+    h->ntiles = (int)tiles.size();
+    h->beta.assign(beta, beta + B);
+    h->m2.assign(B, 2.0);
+    QCHECK(cudaGetDevice(&h->device));
+    QCHECK(cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device));
+    int per_sm = 0;
+    h->shared_state = B <= kSharedReps;
+    if (h->shared_state) QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_r_cg_mixed<true>, TILE, 0));
+    else QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_r_cg_mixed<false>, TILE, 0));
+    if (per_sm < 1) {
+        set_error("batch: the persistent solver does not fit on an SM");
+        return QED2D_ERR_UNSUPPORTED;
+    }
+    const long long maxg = std::min<long long>((long long)per_sm * h->num_sms, kMaxPartBlocks);
+    h->per_block = (int)((h->ntiles + maxg - 1) / maxg);
+    h->grid = (h->ntiles + h->per_block - 1) / h->per_block;
+    std::vector<int> seg0(h->grid), seg_rep;
+    for (int b = 0; b < h->grid; b++) {
+        seg0[b] = (int)seg_rep.size();
+        const int lo = b * h->per_block, hi = std::min(lo + h->per_block, h->ntiles);
+        for (int t = lo; t < hi; t++)
+            if (t == lo || tiles[t].x != tiles[t - 1].x) seg_rep.push_back(tiles[t].x);
+    }
+    h->nseg = (int)seg_rep.size();
+    std::vector<int> rep_seg(B + 1, 0);   // segments are ordered by replica
+    for (int s = 0; s < h->nseg; s++) rep_seg[seg_rep[s] + 1] = s + 1;
+    int maxsegs = 0;
+    for (int r = 0; r < B; r++) {
+        rep_seg[r + 1] = std::max(rep_seg[r + 1], rep_seg[r]);
+        maxsegs = std::max(maxsegs, rep_seg[r + 1] - rep_seg[r]);
+    }
+    // lanes per replica in the last block's sums: fewest rounds of loads
+    long long best = -1;
+    for (int lg = 0; lg <= 5; lg++) {
+        const long long G = 1LL << lg;
+        const long long cost = ((B * G + TILE - 1) / TILE) * ((maxsegs + G - 1) / G + 4 + lg);
+        if (best < 0 || cost < best) {
+            best = cost;
+            h->lg = lg;
+        }
+    }
+    // equal sizes and few replicas: the uniform kernel, whole blocks per replica
+    bool same = B <= kUniformReps;
+    for (int r = 1; r < B && same; r++) same = L1[r] == L1[0] && L2[r] == L2[0];
+    if (same) {
+        int per_smu = 0;
+        QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_smu, k_u_cg_mixed, TILE, 0));
+        const long long maxgu = std::min<long long>((long long)per_smu * h->num_sms, kMaxPartBlocks);
+        const RepInfo& R0 = h->reps[0];
+        if (per_smu >= 1 && maxgu / B >= 1) {
+            h->uniform = true;
+            h->ug = UGeom{R0.L1, R0.L2, B, R0.nt1, R0.V, (long long)R0.nt};
+            const long long bpr = maxgu / B;
+            h->uper_block = (int)((R0.nt + bpr - 1) / bpr);
+            h->ubpr = (R0.nt + h->uper_block - 1) / h->uper_block;
+            h->ugrid = h->ubpr * B;
+        }
+    }
+    std::vector<long long> dbc(B + 1), dbr(B + 1);
+    for (int r = 0; r <= B; r++) {
+        const long long o = r < B ? h->reps[r].off : h->Vtot;
+        dbc[r] = 4 * o;   // complex fields: 2 planes x 2 doubles per site
+        dbr[r] = 2 * o;   // real fields: 2 planes
+    }
+    QTRY(upload(&h->d_reps, h->reps));
+    QTRY(upload(&h->d_tiles, tiles));
+    QTRY(upload(&h->d_seg0, seg0));
+    QTRY(upload(&h->d_rep_seg, rep_seg));
+    QTRY(upload(&h->d_dbase_c, dbc));
+    QTRY(upload(&h->d_dbase_r, dbr));
+    QTRY(upload(&h->d_beta, h->beta));
+    QTRY(upload(&h->d_m2, h->m2));
+    QCHECK(cudaMalloc(&h->d_seed, sizeof(uint64_t) * B));
+    QCHECK(cudaMalloc(&h->d_st, sizeof(RepState) * B));
+    QCHECK(cudaMalloc(&h->d_flags, sizeof(int) * FL_N));
+    QCHECK(cudaMalloc(&h->d_red, sizeof(double) * B));
+    if (h->uniform) {
+        QCHECK(cudaMalloc(&h->d_upart, sizeof(double) * 2 * (size_t)h->ugrid));
+        QCHECK(cudaMalloc(&h->d_ured, sizeof(double) * 2 * B));
+    }
+    QCHECK(cudaMalloc(&h->d_out, sizeof(int) * 2 * B));
+    QCHECK(cudaMalloc(&h->d_iters, sizeof(long long) * B));
+    QCHECK(cudaMalloc(&h->d_sums, sizeof(double) * 2 * 5 * B));
+    QCHECK(cudaMalloc(&h->d_tpart, sizeof(double) * 5 * h->ntiles));
+    QCHECK(cudaMalloc(&h->d_part, sizeof(double) * h->nseg));
+    QCHECK(cudaMalloc(&h->ctl, sizeof(DevCtl)));
+    QCHECK(cudaMallocHost(&h->ctl_host, sizeof(DevCtl)));
+    QCHECK(cudaMemset(h->ctl, 0, sizeof(DevCtl)));
+    return QED2D_OK;
+}
+
+int set_masses(qed2d_batch* h, const double* am0) {
+    for (int r = 0; r < h->nrep; r++) h->m2[r] = 2.0 + am0[r];
+    QCHECK(cudaMemcpyAsync(h->d_m2, h->m2.data(), sizeof(double) * h->nrep, cudaMemcpyHostToDevice, h->stream));
+    return QED2D_OK;
 }
 
 }  // namespace
 
 extern "C" {
 
-int qed2d_batch_create(int nrep, int L1, int L2, const double* beta, qed2d_batch** out) {
+int qed2d_batch_create_ragged(int nrep, const int* L1, const int* L2, const double* beta, qed2d_batch** out) {
     if (!out) return QED2D_ERR_BAD_ARG;
     *out = nullptr;
-    if (nrep < 1 || nrep > kMaxBatch || L1 < 2 || L2 < 2 || !beta ||
-        (long long)nrep * L1 * L2 > (1LL << 30)) {
-        set_error("qed2d_batch_create: need 1 <= nrep <= 64, L1, L2 >= 2, nrep*L1*L2 <= 2^30 and a beta per replica");
+    if (nrep < 1 || nrep > kMaxReplicas || !L1 || !L2 || !beta) {
+        set_error("qed2d_batch_create_ragged: need 1 <= nrep <= 1024 and L1, L2, beta for every replica");
         return QED2D_ERR_BAD_ARG;
     }
+    long long V = 0;
+    for (int r = 0; r < nrep; r++) {
+        if (L1[r] < 2 || L2[r] < 2 || L1[r] > (1 << 20) || L2[r] > (1 << 20)) {
+            set_error("qed2d_batch_create_ragged: lattice extents must lie in [2, 2^20]");
+            return QED2D_ERR_BAD_ARG;
+        }
+        V += (long long)L1[r] * L2[r];
+        if (V > (1LL << 30)) {
+            set_error("qed2d_batch_create_ragged: more than 2^30 sites in the batch");
+            return QED2D_ERR_BAD_ARG;
+        }
+    }
     auto* h = new qed2d_batch();
-    h->g = make_blat(nrep, L1, L2);
-    h->beta.assign(beta, beta + nrep);
-    cudaError_t e = cudaGetDevice(&h->device);
-    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
-    if (e == cudaSuccess) e = cudaMalloc(&h->ctl, sizeof(DevCtl));
-    if (e == cudaSuccess) e = cudaMallocHost(&h->ctl_host, sizeof(DevCtl));
-    if (e == cudaSuccess) e = cudaMalloc(&h->part, sizeof(double) * kMaxPartVals * kMaxPartBlocks);
-    if (e == cudaSuccess) e = cudaMalloc(&h->dscal, sizeof(double) * kMaxBatch * 5 * 2);
-    if (e == cudaSuccess) e = cudaMalloc(&h->dpar, sizeof(double) * kMaxBatch * 2);
-    if (e == cudaSuccess) e = cudaMalloc(&h->dseed, sizeof(uint64_t) * kMaxBatch);
-    if (e == cudaSuccess) e = cudaMalloc(&h->dint, sizeof(int) * kMaxBatch * 3);
-    if (e == cudaSuccess) e = cudaMalloc(&h->diters, sizeof(long long) * kMaxBatch);
-    if (e == cudaSuccess) e = cudaMemset(h->ctl, 0, sizeof(DevCtl));
-    if (e == cudaSuccess) e = cudaMemcpy(h->dpar + kMaxBatch, beta, sizeof(double) * nrep, cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) {
-        const int st = cuda_status(e, "qed2d_batch_create");
+    h->nrep = nrep;
+    const int st = batch_setup(h, L1, L2, beta);
+    if (st != QED2D_OK) {
         qed2d_batch_destroy(h);
         return st;
     }
@@ -644,19 +988,28 @@ int qed2d_batch_create(int nrep, int L1, int L2, const double* beta, qed2d_batch
     return QED2D_OK;
 }
 
+int qed2d_batch_create(int nrep, int L1, int L2, const double* beta, qed2d_batch** out) {
+    if (!out) return QED2D_ERR_BAD_ARG;
+    *out = nullptr;
+    if (nrep < 1 || nrep > kMaxReplicas) {
+        set_error("qed2d_batch_create: need 1 <= nrep <= 1024");
+        return QED2D_ERR_BAD_ARG;
+    }
+    const std::vector<int> a(nrep, L1), b(nrep, L2);
+    return qed2d_batch_create_ragged(nrep, a.data(), b.data(), beta, out);
+}
+
 int qed2d_batch_destroy(qed2d_batch* h) {
     if (!h) return QED2D_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
     else cudaDeviceSynchronize();
     for (auto& kv : h->ws) cudaFree(kv.second.first);
-    cudaFree(h->ctl);
-    cudaFreeHost(h->ctl_host);
-    cudaFree(h->part);
-    cudaFree(h->dscal);
-    cudaFree(h->dpar);
-    cudaFree(h->dseed);
-    cudaFree(h->dint);
-    cudaFree(h->diters);
+    void* dev[] = {h->d_reps, h->d_tiles, h->d_seg0, h->d_rep_seg, h->d_dbase_c, h->d_dbase_r, h->d_m2,
+                   h->d_beta, h->d_seed,  h->d_st, h->d_flags, h->d_red, h->d_upart, h->d_ured,      h->d_out,     h->d_iters,   h->d_sums,
+                   h->d_tpart, h->d_part, h->ctl};
+    for (void* p : dev)
+        if (p) cudaFree(p);
+    if (h->ctl_host) cudaFreeHost(h->ctl_host);
     delete h;
     return QED2D_OK;
 }
@@ -667,6 +1020,13 @@ int qed2d_batch_set_stream(qed2d_batch* h, void* stream) {
     return QED2D_OK;
 }
 
+int qed2d_batch_layout(const qed2d_batch* h, int64_t* site_offsets) {
+    if (!h || !site_offsets) return QED2D_ERR_BAD_ARG;
+    for (int r = 0; r < h->nrep; r++) site_offsets[r] = h->reps[r].off;
+    site_offsets[h->nrep] = h->Vtot;
+    return QED2D_OK;
+}
+
 int qed2d_batch_cg(qed2d_batch* h, double* x, const double* U, const double* b, const double* am0, int maxiter,
                    double eps, int* iterations, int* updates) {
     if (!h || !x || !U || !b || !am0 || maxiter < 0 ||
@@ -674,8 +1034,7 @@ int qed2d_batch_cg(qed2d_batch* h, double* x, const double* U, const double* b, 
         set_error("qed2d_batch_cg: bad argument");
         return QED2D_ERR_BAD_ARG;
     }
-    const int B = h->g.B;
-    const size_t fb = sizeof(double2) * 2 * (size_t)h->g.V;
+    const size_t fb = sizeof(double2) * 2 * (size_t)h->Vtot;
     if ((const char*)x < (const char*)b + fb && (const char*)b < (const char*)x + fb) {
         set_error("qed2d_batch_cg: x aliases b");
         return QED2D_ERR_BAD_ARG;
@@ -684,24 +1043,18 @@ int qed2d_batch_cg(qed2d_batch* h, double* x, const double* U, const double* b, 
     float4* U32 = h->field32("b_U32");
     double2* G = h->field("b_G");
     if (!U32 || !G) return QED2D_ERR_NO_MEMORY;
-    h->m2.assign(B, 0.0);
-    for (int r = 0; r < B; r++) h->m2[r] = 2.0 + am0[r];
+    QTRY(set_masses(h, am0));
     QCHECK(cudaMemsetAsync(&h->ctl->status, 0, sizeof(int), s));
-    QCHECK(cudaMemsetAsync(h->diters, 0, sizeof(long long) * B, s));
-    Ctx tmp;
-    tmp.g.L1 = h->g.L1;
-    tmp.g.L2 = h->g.L2r * B;
-    tmp.g.V = h->g.V;
-    tmp.stream = s;
-    QTRY(launch_pack_links(tmp, U32, (const double2*)U));
-    QTRY(b_solve(h, (const double2*)U, U32, (const double2*)b, (double2*)x, G, maxiter, eps));
-    int hi[3 * kMaxBatch];
-    QCHECK(cudaMemcpyAsync(hi, h->dint, sizeof(hi), cudaMemcpyDeviceToHost, s));
+    QCHECK(cudaMemsetAsync(h->d_iters, 0, sizeof(long long) * h->nrep, s));
+    QTRY(r_pack(h, const_cast<double2*>((const double2*)U), nullptr, 0.0, U32));   // eps = 0: U is only read
+    QTRY(r_solve(h, (const double2*)U, U32, (const double2*)b, (double2*)x, G, maxiter, eps));
+    std::vector<int> out(2 * h->nrep);
+    QCHECK(cudaMemcpyAsync(out.data(), h->d_out, sizeof(int) * out.size(), cudaMemcpyDeviceToHost, s));
     QCHECK(cudaMemcpyAsync(h->ctl_host, h->ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, s));
     QCHECK(cudaStreamSynchronize(s));
-    for (int r = 0; r < B; r++) {
-        if (iterations) iterations[r] = hi[r];
-        if (updates) updates[r] = hi[2 * kMaxBatch + r];
+    for (int r = 0; r < h->nrep; r++) {
+        if (iterations) iterations[r] = out[r];
+        if (updates) updates[r] = out[h->nrep + r];
     }
     const int st = h->ctl_host->status;
     if (st != QED2D_OK) set_error(std::string("qed2d_batch_cg: ") + qed2d_status_string(st));
@@ -714,8 +1067,7 @@ int qed2d_batch_hmc_nf2(qed2d_batch* h, double* Ud, const double* am0, double ep
         set_error("qed2d_batch_hmc_nf2: bad argument");
         return QED2D_ERR_BAD_ARG;
     }
-    const int B = h->g.B;
-    const long long V = h->g.V, Vr = h->g.Vr;
+    const int B = h->nrep;
     double2* U = (double2*)Ud;
     double2* Ucp = h->field("b_Ucp");
     double* mom = h->real2("b_mom");
@@ -725,60 +1077,49 @@ int qed2d_batch_hmc_nf2(qed2d_batch* h, double* Ud, const double* am0, double ep
     float4* U32 = h->field32("b_U32");
     if (!Ucp || !mom || !X || !F || !G || !U32) return QED2D_ERR_NO_MEMORY;
     cudaStream_t s = h->stream;
-    // per-replica parameters
-    h->m2.assign(B, 0.0);
-    for (int r = 0; r < B; r++) h->m2[r] = 2.0 + am0[r];
-    QCHECK(cudaMemcpyAsync(h->dpar, h->m2.data(), sizeof(double) * B, cudaMemcpyHostToDevice, s));
-    QCHECK(cudaMemcpyAsync(h->dseed, seeds, sizeof(uint64_t) * B, cudaMemcpyHostToDevice, s));
-    QCHECK(cudaMemsetAsync(h->diters, 0, sizeof(long long) * B, s));
+    QTRY(set_masses(h, am0));
+    QCHECK(cudaMemcpyAsync(h->d_seed, seeds, sizeof(uint64_t) * B, cudaMemcpyHostToDevice, s));
+    QCHECK(cudaMemsetAsync(h->d_iters, 0, sizeof(long long) * B, s));
     QCHECK(cudaMemsetAsync(&h->ctl->status, 0, sizeof(int), s));
-    QCHECK(cudaMemcpyAsync(Ucp, U, sizeof(double2) * 2 * V, cudaMemcpyDeviceToDevice, s));
+    QCHECK(cudaMemcpyAsync(Ucp, U, sizeof(double2) * 2 * h->Vtot, cudaMemcpyDeviceToDevice, s));
     // draws (src/QED2dHMC.jl:69-70), H_ini, F = g5Dw X (:74-78)
-    QTRY(b_fill(h, mom, 1, QED2D_STREAM_MOMENTA, counter, 1.0));
-    QTRY(b_fill(h, (double*)X, 2, QED2D_STREAM_NOISE, counter, 1.0 / std::sqrt(2.0)));
-    QTRY(b_reduce(h, U, mom, X, nullptr, 0));
-    k_b_g5dw<<<b_tiles(h), TILE, 0, s>>>(F, U, X, h->g, h->dpar);
-    QTRY(b_post("k_b_g5dw"));
-    {
-        Ctx tmp;
-        tmp.g.L1 = h->g.L1;
-        tmp.g.L2 = h->g.L2r * B;
-        tmp.g.V = V;
-        tmp.stream = s;
-        QTRY(launch_pack_links(tmp, U32, U));
-        // leapfrog (src/QED2dHMC.jl:426-449)
-        QTRY(b_kick(h, mom, U, U32, X, F, G, 0.5 * eps, maxiter, tol));
-        for (int i = 0; i < ns - 1; i++) {
-            QTRY(launch_updt_fld(tmp, U, mom, eps, U32));
-            QTRY(b_kick(h, mom, U, U32, X, F, G, eps, maxiter, tol));
-        }
-        QTRY(launch_updt_fld(tmp, U, mom, eps, U32));
-        QTRY(b_kick(h, mom, U, U32, X, F, G, 0.5 * eps, maxiter, tol));
+    QTRY(r_fill(h, mom, false, QED2D_STREAM_MOMENTA, counter, 1.0));
+    QTRY(r_fill(h, (double*)X, true, QED2D_STREAM_NOISE, counter, 1.0 / std::sqrt(2.0)));
+    QTRY(r_sums(h, U, mom, X, nullptr, 0));
+    k_r_g5dw<<<h->ntiles, TILE, 0, s>>>(F, U, X, h->tv(), h->d_m2);
+    QTRY(r_post("k_r_g5dw"));
+    QTRY(r_pack(h, U, mom, 0.0, U32));
+    // leapfrog (src/QED2dHMC.jl:426-449)
+    QTRY(r_kick(h, mom, U, U32, X, F, G, 0.5 * eps, maxiter, tol));
+    for (int i = 0; i < ns - 1; i++) {
+        QTRY(r_pack(h, U, mom, eps, U32));
+        QTRY(r_kick(h, mom, U, U32, X, F, G, eps, maxiter, tol));
     }
+    QTRY(r_pack(h, U, mom, eps, U32));
+    QTRY(r_kick(h, mom, U, U32, X, F, G, 0.5 * eps, maxiter, tol));
     // H_fin with <X, F> (:82)
-    QTRY(b_reduce(h, U, mom, X, F, 1));
-    double sc[2][kMaxBatch * 5];
-    long long its[kMaxBatch];
-    QCHECK(cudaMemcpyAsync(sc, h->dscal, sizeof(sc), cudaMemcpyDeviceToHost, s));
-    QCHECK(cudaMemcpyAsync(its, h->diters, sizeof(long long) * B, cudaMemcpyDeviceToHost, s));
+    QTRY(r_sums(h, U, mom, X, F, 1));
+    std::vector<double> sc(2 * 5 * (size_t)B);
+    std::vector<long long> its(B);
+    QCHECK(cudaMemcpyAsync(sc.data(), h->d_sums, sizeof(double) * sc.size(), cudaMemcpyDeviceToHost, s));
+    QCHECK(cudaMemcpyAsync(its.data(), h->d_iters, sizeof(long long) * B, cudaMemcpyDeviceToHost, s));
     QCHECK(cudaMemcpyAsync(h->ctl_host, h->ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, s));
     QCHECK(cudaStreamSynchronize(s));
     const int st = h->ctl_host->status;
     for (int r = 0; r < B; r++) {
-        const double* a = &sc[0][r * 5];
-        const double* f = &sc[1][r * 5];
-        const double beta = h->beta[r];
-        const double hini = a[2] / 2.0 + beta * ((double)Vr - a[0]) + a[3];
-        const double hfin = f[2] / 2.0 + beta * ((double)Vr - f[0]) + f[4];
+        const RepInfo& R = h->reps[r];
+        const double* a = &sc[(size_t)r * 5];
+        const double* f = &sc[(size_t)(B + r) * 5];
+        const double hini = a[2] / 2.0 + h->beta[r] * ((double)R.V - a[0]) + a[3];
+        const double hfin = f[2] / 2.0 + h->beta[r] * ((double)R.V - f[0]) + f[4];
         const double qf = f[1] / (2.0 * M_PI);
-        double pacc = (qzero && std::fabs(qf) > 0.1) ? 0.0 : std::exp(-(hfin - hini));
+        const double pacc = (qzero && std::fabs(qf) > 0.1) ? 0.0 : std::exp(-(hfin - hini));
         int acc = 1;
         if (st != QED2D_OK) acc = 0;
         else if (pacc < 1.0) acc = pacc > qed2d_random_uniform(seeds[r], QED2D_STREAM_METROPOLIS, counter);
-        if (!acc)   // restore the replica's two planes
-            for (int k2 = 0; k2 < 2; k2++)
-                QCHECK(cudaMemcpyAsync(U + (k2 * B + r) * Vr, Ucp + (k2 * B + r) * Vr, sizeof(double2) * Vr,
-                                       cudaMemcpyDeviceToDevice, s));
+        if (!acc)   // restore the replica's links: one contiguous block
+            QCHECK(cudaMemcpyAsync(U + 2 * R.off, Ucp + 2 * R.off, sizeof(double2) * 2 * R.V, cudaMemcpyDeviceToDevice,
+                                   s));
         if (res) {
             res[r].accepted = acc;
             res[r].hini = hini;

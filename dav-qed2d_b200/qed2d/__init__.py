@@ -555,30 +555,69 @@ def HMC_(U, *args, integrator: Integrators = None, qzero=False, reversibility_te
 
 # ---------------------------------------------------------------------------
 # batched replicas (no single reference counterpart; include/qed2d.h)
-class Batch:
-    """nrep independent L1 x L2 lattices advanced together.  A batch field is a
-    CUDA tensor of shape (2, nrep, L2, L1): plane k of replica r is field[k, r],
-    itself in the reference layout.  Every replica follows HMC! Nf=2 with leapfrog
-    (src/QED2dHMC.jl:64-113) using the mixed solver; replica r draws exactly as a
-    single-lattice HMC_ with seed seeds[r]."""
+def _per_rep(v, n, name):
+    if isinstance(v, (list, tuple)):
+        if len(v) != n:
+            raise ValueError(f"{name}: expected {n} values, got {len(v)}")
+        return [float(x) for x in v]
+    return [float(v)] * n
 
-    def __init__(self, nrep, L1, L2, beta):
-        betas = [float(beta)] * nrep if not isinstance(beta, (list, tuple)) else [float(b) for b in beta]
-        self.nrep, self.L1, self.L2, self.beta = int(nrep), int(L1), int(L2), betas
+
+class Batch:
+    """Independent replica lattices advanced together: Batch(nrep, L1, L2, beta)
+    for nrep lattices of L1 x L2 sites, Batch.ragged([(L1, L2), ...], betas) for
+    lattices of uneven sizes.  A batch field is replica-major: replica r's field
+    is an ordinary reference-layout array at complex element 2*offsets[r].  For
+    an equal-size batch field() has shape (nrep, 2, L2, L1) and field[r] is
+    replica r; replica(t, r) gives that (2, L2_r, L1_r) view for every batch.
+    Every replica follows HMC! Nf=2 with leapfrog (src/QED2dHMC.jl:64-113) using
+    the mixed solver; replica r draws exactly as a single-lattice HMC_ with seed
+    seeds[r]."""
+
+    def __init__(self, nrep, L1, L2, beta, _sizes=None):
+        self.sizes = list(_sizes) if _sizes is not None else [(int(L1), int(L2))] * int(nrep)
+        self.nrep = len(self.sizes)
+        self.uniform = len(set(self.sizes)) == 1
+        self.L1, self.L2 = self.sizes[0]
+        self.beta = _per_rep(beta, self.nrep, "beta")
         h = C.c_void_p()
-        arr = (C.c_double * nrep)(*betas)
-        check(lib().qed2d_batch_create(self.nrep, self.L1, self.L2, arr, C.byref(h)), "batch_create")
+        arr = (C.c_double * self.nrep)(*self.beta)
+        if _sizes is None:
+            check(lib().qed2d_batch_create(self.nrep, self.L1, self.L2, arr, C.byref(h)), "batch_create")
+        else:
+            l1 = (C.c_int * self.nrep)(*[s[0] for s in self.sizes])
+            l2 = (C.c_int * self.nrep)(*[s[1] for s in self.sizes])
+            check(lib().qed2d_batch_create_ragged(self.nrep, l1, l2, arr, C.byref(h)), "batch_create_ragged")
         self.h = h.value
+        offs = (C.c_int64 * (self.nrep + 1))()
+        check(lib().qed2d_batch_layout(self.h, offs), "batch_layout")
+        self.offsets = list(offs)
+        self.sites = self.offsets[-1]
+
+    @classmethod
+    def ragged(cls, sizes, beta):
+        return cls(None, None, None, beta, _sizes=[(int(a), int(b)) for a, b in sizes])
 
     def field(self, dtype=torch.complex128):
-        return torch.zeros((2, self.nrep, self.L2, self.L1), dtype=dtype, device="cuda")
+        if self.uniform:
+            return torch.zeros((self.nrep, 2, self.L2, self.L1), dtype=dtype, device="cuda")
+        return torch.zeros(2 * self.sites, dtype=dtype, device="cuda")
+
+    def replica(self, t, r):
+        """(2, L2_r, L1_r) view of replica r of a batch field t."""
+        L1, L2 = self.sizes[r]
+        o = self.offsets[r]
+        return t.reshape(-1)[2 * o: 2 * (o + L1 * L2)].view(2, L2, L1)
+
+    def _check(self, t, name):
+        if t.numel() != 2 * self.sites or t.dtype != torch.complex128 or not t.is_contiguous() or not t.is_cuda:
+            raise ValueError(f"{name}: expected a contiguous CUDA complex128 batch field of {2 * self.sites} elements")
 
     def cg(self, x, U, b, am0, maxiter, eps):
         """Every replica's CG method 1 in one launch; returns (iterations, reliable updates) per replica."""
-        for t in (x, U, b):
-            if tuple(t.shape) != (2, self.nrep, self.L2, self.L1) or t.dtype != torch.complex128:
-                raise ValueError("expected complex128 tensors of shape (2, nrep, L2, L1)")
-        ams = [float(am0)] * self.nrep if not isinstance(am0, (list, tuple)) else [float(a) for a in am0]
+        for t, n in ((x, "x"), (U, "U"), (b, "b")):
+            self._check(t, n)
+        ams = _per_rep(am0, self.nrep, "am0")
         its, upd = (C.c_int * self.nrep)(), (C.c_int * self.nrep)()
         L = lib()
         check(L.qed2d_batch_set_stream(self.h, C.c_void_p(torch.cuda.current_stream().cuda_stream)))
@@ -590,9 +629,10 @@ class Batch:
         return list(its), list(upd)
 
     def hmc_nf2(self, U, am0, eps, ns, CGmaxiter, tol, seeds, counter, qzero=False):
-        if tuple(U.shape) != (2, self.nrep, self.L2, self.L1) or U.dtype != torch.complex128 or not U.is_contiguous():
-            raise ValueError("U: expected a contiguous complex128 tensor of shape (2, nrep, L2, L1)")
-        ams = [float(am0)] * self.nrep if not isinstance(am0, (list, tuple)) else [float(a) for a in am0]
+        self._check(U, "U")
+        ams = _per_rep(am0, self.nrep, "am0")
+        if len(seeds) != self.nrep:
+            raise ValueError(f"seeds: expected {self.nrep} values")
         res = (_lib.HmcResult * self.nrep)()
         L = lib()
         check(L.qed2d_batch_set_stream(self.h, C.c_void_p(torch.cuda.current_stream().cuda_stream)))

@@ -91,6 +91,8 @@ SIGNATURES = {
     "qed2d_hmc_nf2": (I, [P, P, D, D, I, I, I, D, I, U64, U32, PH]),
     "qed2d_hmc_rhmc": (I, [P, P, I, PD, D, I, I, D, PR, I, I, U64, U32, PH]),
     "qed2d_batch_create": (I, [I, I, I, PD, C.POINTER(C.c_void_p)]),
+    "qed2d_batch_create_ragged": (I, [I, PI, PI, PD, C.POINTER(C.c_void_p)]),
+    "qed2d_batch_layout": (I, [P, C.POINTER(C.c_int64)]),
     "qed2d_batch_destroy": (I, [P]),
     "qed2d_batch_set_stream": (I, [P, P]),
     "qed2d_batch_cg": (I, [P, P, P, P, PD, I, D, PI, PI]),

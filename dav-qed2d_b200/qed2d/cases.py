@@ -36,8 +36,8 @@ def main(argv=None):
         bt = qed2d.Batch(a.batch, L, L, 4.0)
         Ub, bb, xb = bt.field(), bt.field(), bt.field()
         for r in range(a.batch):
-            Ub[:, r] = U
-            bb[:, r] = torch.randn(2, L, L, dtype=torch.complex128, device="cuda", generator=g)
+            Ub[r] = U
+            bb[r] = torch.randn(2, L, L, dtype=torch.complex128, device="cuda", generator=g)
     for _ in range(a.repeat):
         ev0.record()
         if a.case == "g5dw":

@@ -241,13 +241,20 @@ int qed2d_hmc_rhmc(qed2d_ctx* ctx, double* U, int nf, const double* am0, double 
                    uint32_t counter, qed2d_hmc_result* res);
 
 /* ---- batched replicas (no single reference counterpart: the reference runs one
- * chain per process; this runs nrep independent chains of the same lattice size
- * together, each following HMC! Nf=2 with leapfrog, src/QED2dHMC.jl:64-113,426-481).
- * A batch field is the reference layout of an L1 x (nrep*L2) lattice: element
- * (i1, i2, replica r, plane k) at i1 + L1*(i2 + L2*(r + nrep*k)); direction 2
- * wraps inside each replica.  Solves use the mixed FP32/FP64 solver. ---- */
+ * chain per process; this runs nrep independent chains together, of equal or
+ * uneven lattice sizes, each following HMC! Nf=2 with leapfrog,
+ * src/QED2dHMC.jl:64-113,426-481).  A batch field is replica-major: replica r's
+ * field is an ordinary reference-layout array ([L1_r, L2_r, 2]) starting at
+ * complex element 2*off_r (real fields: real element 2*off_r), where off_r is
+ * the number of sites of replicas 0..r-1 (qed2d_batch_layout).  Solves use the
+ * mixed FP32/FP64 solver.  At most 1024 replicas and 2^30 sites per batch. ---- */
 typedef struct qed2d_batch qed2d_batch;
+/* nrep replicas of L1 x L2 sites; beta[nrep] */
 int qed2d_batch_create(int nrep, int L1, int L2, const double* beta, qed2d_batch** out);
+/* nrep replicas of L1[r] x L2[r] sites; beta[nrep] */
+int qed2d_batch_create_ragged(int nrep, const int* L1, const int* L2, const double* beta, qed2d_batch** out);
+/* site_offsets[nrep+1]: off_r of every replica, then the total number of sites */
+int qed2d_batch_layout(const qed2d_batch* batch, int64_t* site_offsets);
 int qed2d_batch_destroy(qed2d_batch* batch);
 int qed2d_batch_set_stream(qed2d_batch* batch, void* cuda_stream);
 /* every replica's CG method 1 (src/QED2dSolver.jl:3-46) in one launch:

@@ -25,7 +25,7 @@ def test_batch_matches_single_and_oracle(L1, L2):
     b = qed2d.Batch(nrep, L1, L2, betas)
     Ub = b.field()
     for r in range(nrep):
-        Ub[:, r] = to_dev(U0[r])
+        Ub[r] = to_dev(U0[r])
     infos = b.hmc_nf2(Ub, am0s, 0.1, 5, 10000, 1e-24, seeds, counter)
     qed2d.set_precision("mixed")
     for r in range(nrep):
@@ -35,7 +35,7 @@ def test_batch_matches_single_and_oracle(L1, L2):
         single = qed2d.HMC_(Ud, am0s[r], 0.1, 5, [], 10000, 1e-24, prm, None, counter=counter)
         assert abs(single.dH - infos[r].dH) < 1e-8
         assert single.accepted == infos[r].accepted
-        assert rel(to_host(Ub[:, r]), to_host(Ud)) < 1e-9
+        assert rel(to_host(Ub[r]), to_host(Ud)) < 1e-9
     qed2d.set_precision("f64")
     # replica 1 against the oracle replaying its draws
     r = 1
@@ -46,7 +46,7 @@ def test_batch_matches_single_and_oracle(L1, L2):
                                         Oracle.uniform(seeds[r], 3, counter))
     assert st == 0 and acc == infos[r].accepted
     assert abs(infos[r].dH - (hf - hi)) < 1e-8
-    assert rel(to_host(Ub[:, r]), Uo) < 1e-9
+    assert rel(to_host(Ub[r]), Uo) < 1e-9
 
 
 def test_batch_rejects_bad_shape():
@@ -54,7 +54,7 @@ def test_batch_rejects_bad_shape():
     b = qed2d.Batch(2, 16, 16, 4.0)
     import torch
     with pytest.raises(ValueError):
-        b.hmc_nf2(torch.zeros((2, 3, 16, 16), dtype=torch.complex128, device="cuda"), 0.3, 0.1, 2, 100, 1e-20,
+        b.hmc_nf2(torch.zeros((3, 2, 16, 16), dtype=torch.complex128, device="cuda"), 0.3, 0.1, 2, 100, 1e-20,
                   [1, 2], 0)
 
 
@@ -68,15 +68,114 @@ def test_batch_cg_matches_single_cg():
     b = qed2d.Batch(nrep, L1, L2, 4.0)
     U, src, x = b.field(), b.field(), b.field()
     for r in range(nrep):
-        U[:, r] = to_dev(hot_links(L1, L2, 200 + r))
-        src[:, r] = to_dev(cgauss(L1, L2, 300 + r, 2))
+        U[r] = to_dev(hot_links(L1, L2, 200 + r))
+        src[r] = to_dev(cgauss(L1, L2, 300 + r, 2))
     its, upd = b.cg(x, U, src, am0s, 20000, 1e-24)
     qed2d.set_precision("mixed")
     prm = qed2d.LattParm((L1, L2), 4.0)
     for r in range(nrep):
         xs = qed2d.cfield(L1, L2)
-        it = qed2d.CG(xs, U[:, r].contiguous(), src[:, r].contiguous(), am0s[r], 20000, 1e-24,
+        it = qed2d.CG(xs, U[r].contiguous(), src[r].contiguous(), am0s[r], 20000, 1e-24,
                       qed2d.gamm5Dw_sqr_msq, prm, None)
-        assert rel(to_host(x[:, r]), to_host(xs)) < 1e-9
+        assert rel(to_host(x[r]), to_host(xs)) < 1e-9
         assert abs(its[r] - it) <= max(3, it // 20) and upd[r] >= 1
+    qed2d.set_precision("f64")
+
+
+RAGGED = [(32, 24), (16, 16), (40, 36), (64, 8), (24, 40), (33, 17)]
+
+
+def test_ragged_batch_matches_single_and_oracle():
+    """Replicas of uneven sizes (partial 32x8 tiles included) in one batch: each
+    reproduces the single-lattice trajectory with its own beta, mass and seed."""
+    import qed2d
+    n = len(RAGGED)
+    betas = [4.0, 3.0, 5.0, 2.5, 4.5, 3.5]
+    am0s = [0.3, 0.25, 0.4, 0.2, 0.35, 0.3]
+    seeds = [21, 22, 23, 24, 25, 26]
+    counter = 3
+    b = qed2d.Batch.ragged(RAGGED, betas)
+    assert b.offsets[-1] == sum(l1 * l2 for l1, l2 in RAGGED)
+    Ub = b.field()
+    U0 = [hot_links(l1, l2, 500 + r) for r, (l1, l2) in enumerate(RAGGED)]
+    for r in range(n):
+        b.replica(Ub, r).copy_(to_dev(U0[r]))
+    infos = b.hmc_nf2(Ub, am0s, 0.1, 5, 10000, 1e-24, seeds, counter)
+    qed2d.set_precision("mixed")
+    for r, (l1, l2) in enumerate(RAGGED):
+        prm = qed2d.LattParm((l1, l2), betas[r])
+        Ud = to_dev(U0[r])
+        qed2d.seed(seeds[r])
+        single = qed2d.HMC_(Ud, am0s[r], 0.1, 5, [], 10000, 1e-24, prm, None, counter=counter)
+        assert abs(single.dH - infos[r].dH) < 1e-8, r
+        assert single.accepted == infos[r].accepted, r
+        assert rel(to_host(b.replica(Ub, r)), to_host(Ud)) < 1e-9, r
+    qed2d.set_precision("f64")
+    r = 5   # the odd-sized replica against the oracle replaying its draws
+    l1, l2 = RAGGED[r]
+    o = Oracle(l1, l2, betas[r])
+    mom0 = Oracle.normal(2 * l1 * l2, seeds[r], 1, counter).reshape(2, l2, l1)
+    noise = cgauss(l1, l2, seeds[r], 16, counter)
+    st, Uo, acc, hi, hf, _ = o.hmc_nf2(U0[r], am0s[r], 0.1, 5, 10000, 1e-24, mom0, noise,
+                                        Oracle.uniform(seeds[r], 3, counter))
+    assert st == 0 and acc == infos[r].accepted
+    assert abs(infos[r].dH - (hf - hi)) < 1e-8
+    assert rel(to_host(b.replica(Ub, r)), Uo) < 1e-9
+
+
+def test_ragged_batch_cg_matches_single_and_is_deterministic():
+    import qed2d
+    n = len(RAGGED)
+    am0s = [0.2, 0.3, 0.4, 0.5, 0.25, 0.35]
+    b = qed2d.Batch.ragged(RAGGED, [4.0] * n)
+    U, src, x, x2 = b.field(), b.field(), b.field(), b.field()
+    for r, (l1, l2) in enumerate(RAGGED):
+        b.replica(U, r).copy_(to_dev(hot_links(l1, l2, 700 + r)))
+        b.replica(src, r).copy_(to_dev(cgauss(l1, l2, 800 + r, 2)))
+    its, upd = b.cg(x, U, src, am0s, 20000, 1e-24)
+    its2, _ = b.cg(x2, U, src, am0s, 20000, 1e-24)
+    assert its == its2 and bool((x == x2).all())   # fixed-order reductions: bit-identical
+    qed2d.set_precision("mixed")
+    for r, (l1, l2) in enumerate(RAGGED):
+        prm = qed2d.LattParm((l1, l2), 4.0)
+        xs = qed2d.cfield(l1, l2)
+        it = qed2d.CG(xs, b.replica(U, r).contiguous(), b.replica(src, r).contiguous(), am0s[r], 20000, 1e-24,
+                      qed2d.gamm5Dw_sqr_msq, prm, None)
+        assert rel(to_host(b.replica(x, r)), to_host(xs)) < 1e-9, r
+        assert abs(its[r] - it) <= max(3, it // 20) and upd[r] >= 1, r
+    qed2d.set_precision("f64")
+
+
+def test_ragged_rejects_bad_sizes():
+    import qed2d
+    with pytest.raises(qed2d.Qed2dError):
+        qed2d.Batch.ragged([(16, 16), (1, 16)], [4.0, 4.0])
+    with pytest.raises(ValueError):
+        qed2d.Batch.ragged([(16, 16), (16, 8)], [4.0])
+
+
+def test_many_replicas_global_state_cg():
+    """More than 64 replicas keep the solver records in global memory: solutions
+    still equal the single-lattice solves and repeat bit for bit."""
+    import qed2d
+    rng = np.random.default_rng(77)
+    n = 80
+    sizes = [(int(a), int(b)) for a, b in zip(rng.choice([8, 16, 24, 40], n), rng.choice([4, 8, 12, 16], n))]
+    am0s = rng.uniform(0.1, 0.5, n).tolist()
+    b = qed2d.Batch.ragged(sizes, [4.0] * n)
+    U, src, x, x2 = b.field(), b.field(), b.field(), b.field()
+    for r, (l1, l2) in enumerate(sizes):
+        b.replica(U, r).copy_(to_dev(hot_links(l1, l2, 900 + r)))
+        b.replica(src, r).copy_(to_dev(cgauss(l1, l2, 1000 + r, 2)))
+    its, _ = b.cg(x, U, src, am0s, 20000, 1e-24)
+    its2, _ = b.cg(x2, U, src, am0s, 20000, 1e-24)
+    assert its == its2 and bool((x == x2).all())
+    qed2d.set_precision("mixed")
+    for r in (0, 1, 41, n - 1):
+        l1, l2 = sizes[r]
+        prm = qed2d.LattParm((l1, l2), 4.0)
+        xs = qed2d.cfield(l1, l2)
+        qed2d.CG(xs, b.replica(U, r).contiguous(), b.replica(src, r).contiguous(), am0s[r], 20000, 1e-24,
+                 qed2d.gamm5Dw_sqr_msq, prm, None)
+        assert rel(to_host(b.replica(x, r)), to_host(xs)) < 1e-9, r
     qed2d.set_precision("f64")

@@ -100,3 +100,37 @@ def test_nf2_64_mixed_vs_f64_and_oracle(q):
         assert abs(i.dH - (hf - hi)) < 1e-7, prec
         assert i.accepted == acc, prec
         assert rel(Uh, Uo) < 1e-8, prec
+
+
+def test_ensemble_512_ragged_replicas(q):
+    """512 Nf=2 replicas with sizes drawn from {32, 48, 64, 96, 128, 256}^2, beta in
+    [2, 6], m0 in [0.05, 0.3], hot starts, leapfrog ns=10 eps=0.1: one batched
+    trajectory, then one replica of each size (and the last one) against the
+    single-lattice mixed path.  Delta H is a difference of two O(V) sums, so its
+    tolerance scales with |H|."""
+    import torch
+    rng = np.random.default_rng(2024)
+    n = 512
+    sizes = [(int(s), int(s)) for s in rng.choice([32, 48, 64, 96, 128, 256], n)]
+    betas = rng.uniform(2.0, 6.0, n).tolist()
+    am0s = rng.uniform(0.05, 0.3, n).tolist()
+    seeds = [9000 + r for r in range(n)]
+    counter = 1
+    b = q.Batch.ragged(sizes, betas)
+    g = torch.Generator(device="cuda").manual_seed(2024)
+    U = torch.polar(torch.ones(2 * b.sites, dtype=torch.float64, device="cuda"),
+                    (torch.rand(2 * b.sites, dtype=torch.float64, device="cuda", generator=g) * 2 - 1) * np.pi)
+    U0 = U.clone()
+    infos = b.hmc_nf2(U, am0s, 0.1, 10, 20000, 1e-24, seeds, counter)
+    assert all(np.isfinite(i.dH) for i in infos)
+    picks = sorted({sizes.index(s) for s in set(sizes)} | {n - 1})
+    q.set_precision("mixed")
+    for r in picks:
+        prm = q.LattParm(sizes[r], betas[r])
+        Ud = b.replica(U0, r).clone()
+        q.seed(seeds[r])
+        single = q.HMC_(Ud, am0s[r], 0.1, 10, [], 20000, 1e-24, prm, None, counter=counter)
+        assert abs(single.dH - infos[r].dH) < 1e-9 * abs(single.hini) + 1e-8, r
+        assert single.accepted == infos[r].accepted, r
+        assert rel(to_host(b.replica(U, r)), to_host(Ud)) < 1e-9, r
+    q.set_precision("f64")
