@@ -40,12 +40,18 @@ SEED = 1234
 WORKLOAD = (f"Nf=2 HMC trajectory, {L}x{L}, beta={BETA}, m0={AM0}, leapfrog ns={NS} eps={EPS}, "
             f"CG to |r|/|b|<1e-12 (eps=1e-24)")
 THERM_TRAJ = 10
-# algorithmic bytes per site (see DESIGN.md "Kernels and their rooflines")
+# algorithmic bytes per site of the solver phases (FP32 packed spinors and links)
 B_MIXED_ITER = 192.0     # FP32 fused iteration: phase A 80 B + phase B 112 B
 B_MIXED_UPDATE = 400.0   # one FP64 reliable update (4 phases)
 B_MIXED_SETUP = 112.0    # |b|^2, x=0, r32 = b/|b|, x32 = 0
 B_F64_ITER = 384.0       # FP64 fused iteration: phase A 160 B + phase B 224 B
 B_DSLASH_F64 = 96.0      # g5Dw apply, FP64: spinor in 32 + links 32 + out 32
+B_DSLASH_C64 = 48.0      # g5Dw apply on complex64 fields: spinor in 16 + links 16 + out 16
+# DRAM bytes (read + write) per site-iteration of k_u_cg_mixed at 4 x 512^2, from an
+# ncu capture of one 100-iteration launch (8.717 GB over 1,048,576 sites x 100);
+# traffic grows in proportion to the iterations at fixed size
+U_DRAM_PER_SITE_ITER = 83.1
+ENS_NS, ENS_EPS = 10, 0.1   # replica ensemble: leapfrog ns=10, eps=0.1
 
 
 def load_peaks():
@@ -268,6 +274,42 @@ def run_ours(args):
     e2e = {"value": world * B * args.steps / e2e_t, "unit": "traj/s",
            "h2d_bytes_per_step": U.numel() * 16, "d2h_bytes_per_step": U.numel() * 16 + C.sizeof(res)}
 
+    # --- replica ensemble: 512 Nf=2 lattices of uneven sizes; under torchrun
+    # each rank advances its cost-balanced share (no exchange), timed as the
+    # slowest rank
+    ensemble = None
+    if not args.skip_ensemble:
+        from qed2d.cases import ensemble_config, hot_batch_field
+        from qed2d.replicas import gather_by_replica, rank_share, slowest
+        sizes, betas, am0s = ensemble_config(512, 2024)
+        mine = rank_share(sizes, rank, world)
+        eb = qed2d.Batch.ragged([sizes[i] for i in mine], [betas[i] for i in mine])
+        Ue = hot_batch_field(eb, 2024 + rank)
+        em, es = [am0s[i] for i in mine], [9000 + i for i in mine]
+        eb.hmc_nf2(Ue, em, ENS_EPS, ENS_NS, MAXITER, TOL, es, 0)   # warm-up
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n_traj = 2
+        e0.record()
+        einfos = [eb.hmc_nf2(Ue, em, ENS_EPS, ENS_NS, MAXITER, TOL, es, 1 + t) for t in range(n_traj)]
+        e1.record()
+        torch.cuda.synchronize()
+        t_e = slowest(e0.elapsed_time(e1) / 1e3, device=dev if dist else None)
+        per_rep = gather_by_replica(mine, [(sum(st[j].cg_iterations for st in einfos),
+                                            sum(st[j].accepted for st in einfos)) for j in range(len(mine))],
+                                    len(sizes))
+        ensemble = {"replicas": len(sizes), "sites": sum(a * b for a, b in sizes),
+                    "sizes": "32..256 squared, drawn from seed 2024", "beta": "U[2,6]", "m0": "U[0.05,0.3]",
+                    "ns": ENS_NS, "eps": ENS_EPS, "start": "hot", "ranks": world,
+                    "value": len(sizes) * n_traj / t_e, "unit": "traj/s", "ms_per_batched_traj": 1e3 * t_e / n_traj,
+                    "cg_iterations_per_traj_mean": sum(p[0] for p in per_rep) / (n_traj * len(sizes)),
+                    "accepted": sum(p[1] for p in per_rep), "of": n_traj * len(sizes),
+                    "timed": f"{n_traj} batched trajectories after 1 warm-up"}
+        del eb, Ue
+        torch.cuda.empty_cache()
+
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -292,12 +334,13 @@ def run_ours(args):
     V = L * L
     bytes_k = V * sum(B_MIXED_SETUP + i * B_MIXED_ITER + u * B_MIXED_UPDATE for i, u in zip(its, upd))
     achieved = bytes_k / t_k / 1e9
-    traffic = None
-    roofline = {"kernel": "k_b_cg_mixed", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+    traffic = V * sum(its) * U_DRAM_PER_SITE_ITER
+    roofline = {"kernel": "k_u_cg_mixed", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                 "note": f"one launch = one solve of all {B} replicas: per replica iterations {min(its)}-{max(its)} "
                         f"x {B_MIXED_ITER:.0f} B/site + reliable updates {min(upd)}-{max(upd)} x "
-                        f"{B_MIXED_UPDATE:.0f} B/site; {B} x {L}^2 working set exceeds L2"}
+                        f"{B_MIXED_UPDATE:.0f} B/site; {B} x {L}^2 working set partly L2-resident; traffic = ncu DRAM bytes per site-iteration at this size "
+                        f"x the solve's site-iterations"}
 
     # --- single-chain baselines on the same field and draws as replica 0's first
     # timed step: mixed (no batching), fused FP64, and the plain FP64 GPU path
@@ -338,6 +381,20 @@ def run_ours(args):
         t_ap = a0.elapsed_time(a1) / 1e3 / n_ap
         Vb = Lbig * Lbig
         f64_gbs = B_DSLASH_F64 * Vb / t_ap / 1e9
+        # the same apply on complex64 spinors and links
+        U64, si64 = Ub.to(torch.complex64), si.to(torch.complex64)
+        so64 = torch.empty_like(si64)
+        for _ in range(3):
+            qed2d.gamm5Dw(so64, U64, si64, AM0, pb)
+        a0.record()
+        for _ in range(n_ap):
+            qed2d.gamm5Dw(so64, U64, si64, AM0, pb)
+        a1.record()
+        torch.cuda.synchronize()
+        t_ap32 = a0.elapsed_time(a1) / 1e3 / n_ap
+        c64_gbs = B_DSLASH_C64 * Vb / t_ap32 / 1e9
+        apply_err = float(((so64.to(torch.complex128) - so).abs().max() / so.abs().max()).item())
+        del U64, si64, so64
         qed2d.set_precision("mixed")
         xb = torch.zeros_like(si)
         cg_runs = []
@@ -351,11 +408,24 @@ def run_ours(args):
             torch.cuda.synchronize()
             it, _, up = qed2d.last_solve(pb)
             cg_runs.append((a0.elapsed_time(a1) / 1e3, it, up))
+        # FP32-inner vs FP64 solution at the reference's stop rule
+        sols = {}
+        for prec in ("mixed", "f64"):
+            qed2d.set_precision(prec)
+            xs_ = torch.zeros_like(si)
+            qed2d.CG(xs_, Ub, si, AM0, MAXITER, TOL, qed2d.gamm5Dw_sqr_msq, pb, None)
+            sols[prec] = (xs_, qed2d.last_solve(pb))
+        sol_err = float(((sols["mixed"][0] - sols["f64"][0]).abs().max() / sols["f64"][0].abs().max()).item())
+        sol_its = {k: v[1][0] for k, v in sols.items()}
+        del sols
         qed2d.set_precision("f64")
         t_cg, it_cg, upd_cg = cg_runs[-1]
         cg_gbs = Vb * (B_MIXED_SETUP + it_cg * B_MIXED_ITER + upd_cg * B_MIXED_UPDATE) / t_cg / 1e9
         dslash = {"lattice": f"{Lbig}x{Lbig}", "g5dw_f64_GBs": f64_gbs, "g5dw_f64_frac": f64_gbs / peak,
-                  "g5dw_f64_us": t_ap * 1e6, "cg_mixed_GBs": cg_gbs, "cg_mixed_frac": cg_gbs / peak,
+                  "g5dw_f64_us": t_ap * 1e6, "g5dw_c64_GBs": c64_gbs, "g5dw_c64_frac": c64_gbs / peak,
+                  "g5dw_c64_us": t_ap32 * 1e6, "g5dw_c64_vs_f64_rel_err": apply_err,
+                  "cg_solution_mixed_vs_f64_rel_err": sol_err, "cg_solution_iterations": sol_its,
+                  "cg_mixed_GBs": cg_gbs, "cg_mixed_frac": cg_gbs / peak,
                   "cg_mixed_iters": it_cg, "cg_mixed_updates": upd_cg, "peak_GBs": peak, "peak_kind": peak_kind}
         del Ub, si, so, xb
         torch.cuda.empty_cache()
@@ -396,6 +466,7 @@ def run_ours(args):
             "batched_vs_plain": value / world / (1.0 / base["plain"][0]),
             "batched_vs_f64_fused": value / world / (1.0 / base["f64"][0])},
         "dslash_hbm": dslash,
+        "ensemble": ensemble,
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -410,6 +481,7 @@ def main():
     ap.add_argument("--batch", type=int, default=4, help="replica chains per GPU advanced together")
     ap.add_argument("--skip-sweep", action="store_true", help="skip the 8192^2 Dslash bandwidth sweep")
     ap.add_argument("--skip-cpu", action="store_true", help="skip the oracle CPU baseline")
+    ap.add_argument("--skip-ensemble", action="store_true", help="skip the 512-replica ensemble measurement")
     ap.add_argument("--skip-baselines", action="store_true",
                     help="skip the plain-FP64 and fused-FP64 GPU trajectories")
     args = ap.parse_args()

@@ -128,7 +128,8 @@ __global__ void k_r_random_normal(double* __restrict__ out, const long long* __r
     out[d + 1] = scale * z1;
 }
 
-// per-tile sums (Re P, arg P, mom^2, |X|^2, Re<X,F>) -> part[tile*5 + k]
+// per-tile compensated sums (Re P, arg P, mom^2, |X|^2, Re<X,F>) ->
+// part[tile*10 + 2k] (hi), part[tile*10 + 2k + 1] (lo)
 __global__ void __launch_bounds__(TILE) k_r_reduce_tiles(const double2* __restrict__ U, const double* __restrict__ mom,
                                                          const double2* __restrict__ X, const double2* __restrict__ F,
                                                          TileView tv, double* __restrict__ part) {
@@ -137,23 +138,26 @@ __global__ void __launch_bounds__(TILE) k_r_reduce_tiles(const double2* __restri
     const Lat g = lat_of(R);
     const Site q = site_at(g, T.y, T.z, threadIdx.x);
     const long long o = 2 * R.off;
-    double v[5] = {0, 0, 0, 0, 0};
+    DSum v[5] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}};
     if (q.ok) {
         const double2* u = U + o;
         const double2 p = plaquette_of(__ldg(u + q.x), __ldg(u + g.V + q.xp1), __ldg(u + q.xp2), __ldg(u + g.V + q.x));
-        v[0] = p.x;
-        v[1] = atan2(p.y, p.x);
-        if (mom) v[2] = mom[o + q.x] * mom[o + q.x] + mom[o + q.x + g.V] * mom[o + q.x + g.V];
+        v[0].hi = p.x;
+        v[1].hi = atan2(p.y, p.x);
+        if (mom) v[2].hi = mom[o + q.x] * mom[o + q.x] + mom[o + q.x + g.V] * mom[o + q.x + g.V];
         if (X) {
             const double2 a = X[o + q.x], b = X[o + q.x + g.V];
-            v[3] = norm2(a) + norm2(b);
-            if (F) v[4] = cjmul(a, F[o + q.x]).x + cjmul(b, F[o + q.x + g.V]).x;
+            v[3].hi = norm2(a) + norm2(b);
+            if (F) v[4].hi = cjmul(a, F[o + q.x]).x + cjmul(b, F[o + q.x + g.V]).x;
         }
     }
-    __shared__ double smem[32 * 5];
-    block_sum<5>(v, smem);
+    __shared__ double smem[64 * 5];
+    block_dsum<5>(v, smem);
     if (threadIdx.x == 0)
-        for (int k = 0; k < 5; k++) part[(size_t)blockIdx.x * 5 + k] = v[k];
+        for (int k = 0; k < 5; k++) {
+            part[(size_t)blockIdx.x * 10 + 2 * k] = v[k].hi;
+            part[(size_t)blockIdx.x * 10 + 2 * k + 1] = v[k].lo;
+        }
 }
 
 // per-replica sums of the per-tile partials (one warp per replica, fixed order)
@@ -162,15 +166,21 @@ __global__ void k_r_reduce_final(const double* __restrict__ part, const RepInfo*
     const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
     if (r >= nrep) return;   // whole warps leave together
     const RepInfo R = reps[r];
-    double s[5] = {0, 0, 0, 0, 0};
+    DSum s[5] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}};
     for (int t = lane; t < R.nt; t += 32)
 #pragma unroll
-        for (int k = 0; k < 5; k++) s[k] += part[(size_t)(R.tile0 + t) * 5 + k];
+        for (int k = 0; k < 5; k++) {
+            const double* pp = part + (size_t)(R.tile0 + t) * 10 + 2 * k;
+            dsum_merge(s[k], DSum{pp[0], pp[1]});
+        }
 #pragma unroll
     for (int k = 0; k < 5; k++) {
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s[k] += __shfl_xor_sync(0xffffffffu, s[k], o);
-        if (lane == 0) out[(size_t)r * 5 + k] = s[k];
+        for (int o = 16; o > 0; o >>= 1) {
+            const DSum t{__shfl_xor_sync(0xffffffffu, s[k].hi, o), __shfl_xor_sync(0xffffffffu, s[k].lo, o)};
+            dsum_merge(s[k], t);
+        }
+        if (lane == 0) out[(size_t)r * 5 + k] = s[k].hi + s[k].lo;
     }
 }
 
@@ -695,7 +705,7 @@ struct qed2d_batch {
     int* d_out = nullptr;           // [2][nrep]: iterations, reliable updates of the last solve
     long long* d_iters = nullptr;   // [nrep] iterations accumulated over a trajectory
     double* d_sums = nullptr;       // [2][nrep][5] start / end sums of a trajectory
-    double* d_tpart = nullptr;      // [ntiles][5]
+    double* d_tpart = nullptr;      // [ntiles][5][hi, lo]
     double* d_part = nullptr;       // [nseg]
     DevCtl* ctl = nullptr;
     DevCtl* ctl_host = nullptr;
@@ -940,7 +950,7 @@ int batch_setup(qed2d_batch* h, const int* L1, const int* L2, const double* beta
     QCHECK(cudaMalloc(&h->d_out, sizeof(int) * 2 * B));
     QCHECK(cudaMalloc(&h->d_iters, sizeof(long long) * B));
     QCHECK(cudaMalloc(&h->d_sums, sizeof(double) * 2 * 5 * B));
-    QCHECK(cudaMalloc(&h->d_tpart, sizeof(double) * 5 * h->ntiles));
+    QCHECK(cudaMalloc(&h->d_tpart, sizeof(double) * 10 * h->ntiles));
     QCHECK(cudaMalloc(&h->d_part, sizeof(double) * h->nseg));
     QCHECK(cudaMalloc(&h->ctl, sizeof(DevCtl)));
     QCHECK(cudaMallocHost(&h->ctl_host, sizeof(DevCtl)));

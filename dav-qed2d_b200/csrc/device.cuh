@@ -208,6 +208,63 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double* smem /* >= 32
     }
 }
 
+// Compensated (double-double) sums for the energies that Metropolis compares:
+// TwoSum (Knuth; Moller) yields the exact rounding error of each addition, and
+// the errors are summed separately (Ogita, Rump & Oishi's Sum2), so a sum of
+// 10^8 site terms is as accurate as one in twice the working precision.
+struct DSum {
+    double hi, lo;
+};
+__device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
+    s = a + b;
+    const double bp = s - a;
+    e = (a - (s - bp)) + (b - bp);
+}
+__device__ __forceinline__ void dsum_add(DSum& d, double x) {
+    double s, e;
+    two_sum(d.hi, x, s, e);
+    d.hi = s;
+    d.lo += e;
+}
+__device__ __forceinline__ void dsum_merge(DSum& d, const DSum& o) {
+    double s, e;
+    two_sum(d.hi, o.hi, s, e);
+    d.hi = s;
+    d.lo += e + o.lo;
+}
+// block reduction of NV compensated sums; the result is valid in thread 0
+template <int NV>
+__device__ __forceinline__ void block_dsum(DSum (&v)[NV], double* smem /* >= 64*NV */) {
+#pragma unroll
+    for (int k = 0; k < NV; k++)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const DSum t{__shfl_xor_sync(0xffffffffu, v[k].hi, o), __shfl_xor_sync(0xffffffffu, v[k].lo, o)};
+            dsum_merge(v[k], t);
+        }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            smem[(2 * k) * 32 + warp] = v[k].hi;
+            smem[(2 * k + 1) * 32 + warp] = v[k].lo;
+        }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            DSum s{lane < nw ? smem[(2 * k) * 32 + lane] : 0.0, lane < nw ? smem[(2 * k + 1) * 32 + lane] : 0.0};
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const DSum t{__shfl_xor_sync(0xffffffffu, s.hi, o), __shfl_xor_sync(0xffffffffu, s.lo, o)};
+                dsum_merge(s, t);
+            }
+            v[k] = s;
+        }
+    }
+}
+
 // Sum part[0..n) in a fixed order, identically in every block (warp 0 does it;
 // result broadcast through shared memory).  Deterministic across launches.
 template <int NV>

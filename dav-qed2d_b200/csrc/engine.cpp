@@ -451,6 +451,17 @@ int qed2d_gamm5dw(qed2d_ctx* ctx, double* so, const double* U, const double* si,
     return launch_g5dw(c, C2(so), C2(U), C2(si), am0, nullptr, make_double2(0, 0), false);
 }
 
+int qed2d_gamm5dw_c64(qed2d_ctx* ctx, float* so, const float* U, const float* si, double am0) {
+    QCTX(ctx);
+    QPTR(so);
+    QPTR(U);
+    QPTR(si);
+    const size_t nb = sizeof(float2) * 2 * (size_t)c.g.V;
+    if (overlap(so, nb, si, nb)) return bad_arg("gamm5Dw (complex64): output aliases an input");
+    return launch_g5dw_c64(c, reinterpret_cast<float2*>(so), reinterpret_cast<const float2*>(U),
+                           reinterpret_cast<const float2*>(si), am0);
+}
+
 int qed2d_gamm5(qed2d_ctx* ctx, double* so, const double* si) {
     QCTX(ctx);
     QPTR(so);

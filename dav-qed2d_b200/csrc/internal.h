@@ -78,6 +78,7 @@ int64_t launches();
 
 // kernel launchers (kernels.cu) --------------------------------------------
 // All complex fields are double2 planes in the reference layout.
+int launch_g5dw_c64(Ctx& c, float2* so, const float2* U, const float2* si, double am0);
 int launch_g5dw(Ctx& c, double2* so, const double2* U, const double2* si, double am0, const double2* addv,
                 double2 addc, bool g5_out);
 int launch_g5(Ctx& c, double2* so, const double2* si);

@@ -33,6 +33,17 @@ __global__ void __launch_bounds__(TILE) k_g5dw(double2* __restrict__ so, const d
     st_d(so, g.V, q.x, o);
 }
 
+// gamm5Dw on complex64 fields in the reference layout: the FP32 arithmetic of
+// the mixed solver's inner iterations on complex64 spinors and links
+__global__ void __launch_bounds__(TILE) k_g5dw_c64(float2* __restrict__ so, const float2* __restrict__ U,
+                                                   const float2* __restrict__ si, float m2, Lat g) {
+    const Site q = site_of_tile(g, blockIdx.x, threadIdx.x);
+    if (!q.ok) return;
+    const Pair<float> o = g5dw_at<float>(SpF2{si, g.V}, LkF2{U, g.V}, q, m2);
+    so[q.x] = o.a;
+    so[q.x + g.V] = o.b;
+}
+
 // gamm5 (src/QED2dDirac.jl:130-146)
 __global__ void k_g5(double2* __restrict__ so, const double2* __restrict__ si, long long V) {
     const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -177,18 +188,23 @@ __global__ void k_zaxpby(double2* y, double2 a, const double2* x, double2 b, con
 }
 
 // ---------------------------------------------------------------------------
-// single-launch deterministic reductions: per-block tree sums to part[], the
-// last block to finish sums part[] in a fixed order into ctl->scal[slot..]
+// single-launch deterministic reductions: per-block compensated sums to part[]
+// (hi, lo pairs), the last block to finish merges part[] in a fixed order into
+// ctl->scal[slot..] (hi + lo)
 constexpr int RB = 256;
 
 template <int NV>
-__device__ __forceinline__ void finish_reduce(double (&v)[NV], double* part, DevCtl* ctl, int slot) {
-    __shared__ double smem[32 * NV];
+__device__ __forceinline__ void finish_reduce(DSum (&v)[NV], double* part, DevCtl* ctl, int slot) {
+    static_assert(2 * NV <= kMaxPartVals, "partials hold (hi, lo) pairs");
+    __shared__ double smem[64 * NV];
     __shared__ bool last;
-    block_sum<NV>(v, smem);
+    block_dsum<NV>(v, smem);
     if (threadIdx.x == 0) {
 #pragma unroll
-        for (int k = 0; k < NV; k++) part[(size_t)k * kMaxPartBlocks + blockIdx.x] = v[k];
+        for (int k = 0; k < NV; k++) {
+            part[(size_t)(2 * k) * kMaxPartBlocks + blockIdx.x] = v[k].hi;
+            part[(size_t)(2 * k + 1) * kMaxPartBlocks + blockIdx.x] = v[k].lo;
+        }
         __threadfence();
         last = atomicAdd(&ctl->ticket, 1u) == gridDim.x - 1;
     }
@@ -198,45 +214,52 @@ __device__ __forceinline__ void finish_reduce(double (&v)[NV], double* part, Dev
     if (threadIdx.x < 32) {
 #pragma unroll
         for (int k = 0; k < NV; k++) {
-            double s = 0.0;
-            for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) s += __ldcg(part + (size_t)k * kMaxPartBlocks + i);
+            DSum s{0.0, 0.0};
+            for (int i = threadIdx.x; i < (int)gridDim.x; i += 32)
+                dsum_merge(s, DSum{__ldcg(part + (size_t)(2 * k) * kMaxPartBlocks + i),
+                                   __ldcg(part + (size_t)(2 * k + 1) * kMaxPartBlocks + i)});
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (threadIdx.x == 0) ctl->scal[slot + k] = s;
+            for (int o = 16; o > 0; o >>= 1) {
+                const DSum t{__shfl_xor_sync(0xffffffffu, s.hi, o), __shfl_xor_sync(0xffffffffu, s.lo, o)};
+                dsum_merge(s, t);
+            }
+            if (threadIdx.x == 0) ctl->scal[slot + k] = s.hi + s.lo;
         }
         if (threadIdx.x == 0) ctl->ticket = 0;
     }
 }
 
+// |x|^2 (kind 0) or <x, y> (kind 1), compensated
 __global__ void __launch_bounds__(RB) k_reduce_vec(int kind, const double2* __restrict__ x,
                                                    const double2* __restrict__ y, long long n, double* part,
                                                    DevCtl* ctl, int slot) {
-    double v[2] = {0.0, 0.0};
+    DSum v[2] = {{0.0, 0.0}, {0.0, 0.0}};
     for (long long i = blockIdx.x * (long long)RB + threadIdx.x; i < n; i += (long long)gridDim.x * RB) {
         const double2 a = x[i];
         if (kind == 0) {
-            v[0] += norm2(a);
+            dsum_add(v[0], norm2(a));
         } else {
             const double2 d = cjmul(a, y[i]);
-            v[0] += d.x;
-            v[1] += d.y;
+            dsum_add(v[0], d.x);
+            dsum_add(v[1], d.y);
         }
     }
     finish_reduce<2>(v, part, ctl, slot);
 }
 
-// (sum Re P, sum arg P, sum mom^2) -- Action/Plaquette/Qtop/Hamiltonian (src/QED2dHMC.jl:198-237)
+// (sum Re P, sum arg P, sum mom^2), compensated -- Action/Plaquette/Qtop/Hamiltonian
+// (src/QED2dHMC.jl:198-237)
 __global__ void __launch_bounds__(RB) k_reduce_gauge(const double2* __restrict__ U, const double* __restrict__ mom,
                                                      Lat g, double* part, DevCtl* ctl, int slot) {
-    double v[3] = {0.0, 0.0, 0.0};
+    DSum v[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
     for (long long x = blockIdx.x * (long long)RB + threadIdx.x; x < g.V; x += (long long)gridDim.x * RB) {
         const int i2 = (int)(x / g.L1), i1 = (int)(x - (long long)i2 * g.L1);
         const long long xp1 = (i1 + 1 == g.L1) ? x - (g.L1 - 1) : x + 1;
         const long long xp2 = (i2 + 1 == g.L2) ? (long long)i1 : x + g.L1;
         const double2 p = plaquette_of(__ldg(U + x), __ldg(U + g.V + xp1), __ldg(U + xp2), __ldg(U + g.V + x));
-        v[0] += p.x;
-        v[1] += atan2(p.y, p.x);
-        if (mom) v[2] += mom[x] * mom[x] + mom[x + g.V] * mom[x + g.V];
+        dsum_add(v[0], p.x);
+        dsum_add(v[1], atan2(p.y, p.x));
+        if (mom) dsum_add(v[2], mom[x] * mom[x] + mom[x + g.V] * mom[x + g.V]);
     }
     finish_reduce<3>(v, part, ctl, slot);
 }
@@ -267,6 +290,11 @@ static unsigned reduce_grid(long long n) {
     if (b > 4 * 148) b = 4 * 148;
     if (b < 1) b = 1;
     return (unsigned)b;
+}
+
+int launch_g5dw_c64(Ctx& c, float2* so, const float2* U, const float2* si, double am0) {
+    k_g5dw_c64<<<tiles_grid(c.g), TILE, 0, c.stream>>>(so, U, si, (float)(2.0 + am0), c.g);
+    return post_launch("k_g5dw_c64");
 }
 
 int launch_g5dw(Ctx& c, double2* so, const double2* U, const double2* si, double am0, const double2* addv,

@@ -140,6 +140,12 @@ struct SpAxpy {
     }
 };
 
+struct SpF2 {   // complex64 planes (reference layout in single precision): p[x + k V]
+    const float2* p;
+    long long V;
+    __device__ __forceinline__ Pair<float> ld(long long x) const { return {__ldg(p + x), __ldg(p + x + V)}; }
+};
+
 // link accessors
 struct LkD {
     const double2* U;
@@ -157,6 +163,13 @@ struct LkF {
         const float4 q = __ldg(U + x);
         return make_float2(q.z, q.w);
     }
+};
+
+struct LkF2 {   // complex64 link planes
+    const float2* U;
+    long long V;
+    __device__ __forceinline__ float2 u1(long long x) const { return __ldg(U + x); }
+    __device__ __forceinline__ float2 u2(long long x) const { return __ldg(U + V + x); }
 };
 
 // gamma5 Dw applied at one site

@@ -209,7 +209,13 @@ def updt_fld_(U, mom, eps):
 # ---------------------------------------------------------------------------
 # Dirac operator (src/QED2dDirac.jl)
 def gamm5Dw(so, U, si, am0, prm: LattParm, kprm=None):
-    """gamm5Dw (src/QED2dDirac.jl:2-33)."""
+    """gamm5Dw (src/QED2dDirac.jl:2-33).  complex64 fields (so, U, si all
+    complex64) run the FP32 apply; complex128 the FP64 one."""
+    if isinstance(so, torch.Tensor) and so.dtype == torch.complex64:
+        c64 = torch.complex64
+        check(lib().qed2d_gamm5dw_c64(_c(prm), _ptr(so, prm, c64, name="so"), _ptr(U, prm, c64, name="U"),
+                                      _ptr(si, prm, c64, name="si"), float(am0)), "gamm5Dw (complex64)")
+        return
     check(lib().qed2d_gamm5dw(_c(prm), _cp(so, prm), _cp(U, prm), _cp(si, prm), float(am0)), "gamm5Dw")
 
 

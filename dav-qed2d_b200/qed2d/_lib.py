@@ -55,6 +55,7 @@ SIGNATURES = {
     "qed2d_krnl_force": (I, [P, P, P, P]),
     "qed2d_updt_fld": (I, [P, P, P, D]),
     "qed2d_gamm5dw": (I, [P, P, P, P, D]),
+    "qed2d_gamm5dw_c64": (I, [P, P, P, P, D]),
     "qed2d_gamm5": (I, [P, P, P]),
     "qed2d_dw": (I, [P, P, P, P, D]),
     "qed2d_gamm5dw_sqr": (I, [P, P, P, P, D]),

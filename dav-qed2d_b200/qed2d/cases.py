@@ -4,8 +4,10 @@
 
 cases: g5dw (FP64 gamm5Dw apply), cg_mixed / cg_f64 (one persistent CG launch
 capped at --maxiter iterations), force (gamm5Dw + tr_dQwdU), updt (link update),
-bcg (one batched mixed CG launch over --batch replicas).  Seeded hot-start links and Gaussian sources; prints the
-per-launch time of the last repeat.
+bcg (one batched mixed CG launch over --batch replicas of L x L), ens (one
+batched mixed CG over the 512-replica ensemble of uneven sizes).  Seeded
+hot-start links and Gaussian sources; prints the per-launch time of the last
+repeat.
 """
 import argparse
 import sys
@@ -15,10 +17,30 @@ import torch
 
 import qed2d
 
+ENSEMBLE_SIZES = (32, 48, 64, 96, 128, 256)
+
+
+def ensemble_config(n=512, seed=2024):
+    """The replica ensemble: n Nf=2 lattices with sizes drawn from the seed over
+    {32, 48, 64, 96, 128, 256}^2, beta ~ U[2, 6], m0 ~ U[0.05, 0.3]; returns
+    (sizes, betas, masses)."""
+    rng = np.random.default_rng(seed)
+    sizes = [(int(s), int(s)) for s in rng.choice(ENSEMBLE_SIZES, n)]
+    return sizes, rng.uniform(2.0, 6.0, n).tolist(), rng.uniform(0.05, 0.3, n).tolist()
+
+
+def hot_batch_field(batch, seed):
+    """A hot start (link angles uniform in [-pi, pi)) for every replica of a batch."""
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    n = 2 * batch.sites
+    th = (torch.rand(n, dtype=torch.float64, device="cuda", generator=g) * 2 - 1) * np.pi
+    U = torch.polar(torch.ones(n, dtype=torch.float64, device="cuda"), th)
+    return U.view(batch.field().shape) if batch.uniform else U
+
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["g5dw", "cg_mixed", "cg_f64", "force", "updt", "bcg"])
+    ap.add_argument("case", choices=["g5dw", "cg_mixed", "cg_f64", "force", "updt", "bcg", "ens"])
     ap.add_argument("--batch", type=int, default=4)
     ap.add_argument("--L", type=int, default=2048)
     ap.add_argument("--maxiter", type=int, default=100)
@@ -38,6 +60,12 @@ def main(argv=None):
         for r in range(a.batch):
             Ub[r] = U
             bb[r] = torch.randn(2, L, L, dtype=torch.complex128, device="cuda", generator=g)
+    if a.case == "ens":
+        sizes, betas, am0s = ensemble_config(512, 2024)
+        bt = qed2d.Batch.ragged(sizes, betas)
+        Ub = hot_batch_field(bt, 2024)
+        bb = torch.randn(2 * bt.sites, dtype=torch.complex128, device="cuda", generator=g)
+        xb = torch.zeros_like(bb)
     for _ in range(a.repeat):
         ev0.record()
         if a.case == "g5dw":
@@ -53,9 +81,9 @@ def main(argv=None):
             qed2d.gamm5Dw(g5, U, si, 0.1, prm)
             f = torch.zeros(2, L, L, dtype=torch.float64, device="cuda")
             qed2d.tr_dQwdU(f, U, si, g5, prm)
-        elif a.case == "bcg":
+        elif a.case in ("bcg", "ens"):
             try:
-                it = bt.cg(xb, Ub, bb, 0.1, a.maxiter, 1e-24)
+                it = bt.cg(xb, Ub, bb, 0.1 if a.case == "bcg" else am0s, a.maxiter, 1e-24)
             except qed2d.Qed2dError:
                 it = "capped"
         elif a.case == "updt":
@@ -63,7 +91,7 @@ def main(argv=None):
             qed2d.updt_fld_(U, mom, 0.01)
         ev1.record()
         torch.cuda.synchronize()
-    it = qed2d.last_solve(prm) if a.case.startswith("cg") else (it if a.case == "bcg" else None)
+    it = qed2d.last_solve(prm) if a.case.startswith("cg") else (it if a.case in ("bcg", "ens") else None)
     print(f"{a.case} L={L}: {ev0.elapsed_time(ev1):.3f} ms  solve={it}")
     return 0
 

@@ -122,6 +122,9 @@ int qed2d_updt_fld(qed2d_ctx* ctx, double* U, const double* mom, double eps);
 /* ---- Dirac operator: src/QED2dDirac.jl ---- */
 /* gamm5Dw -- src/QED2dDirac.jl:2-33 */
 int qed2d_gamm5dw(qed2d_ctx* ctx, double* so, const double* U, const double* si, double am0);
+/* gamm5Dw on complex64 fields in the same layout (FP32 arithmetic): the
+ * single-precision apply of the mixed solver, for complex64 callers */
+int qed2d_gamm5dw_c64(qed2d_ctx* ctx, float* so, const float* U, const float* si, double am0);
 /* gamm5 -- src/QED2dDirac.jl:130-146 */
 int qed2d_gamm5(qed2d_ctx* ctx, double* so, const double* si);
 /* Dw -- src/QED2dDirac.jl:157-169 */

@@ -108,18 +108,13 @@ def test_ensemble_512_ragged_replicas(q):
     trajectory, then one replica of each size (and the last one) against the
     single-lattice mixed path.  Delta H is a difference of two O(V) sums, so its
     tolerance scales with |H|."""
-    import torch
-    rng = np.random.default_rng(2024)
+    from qed2d.cases import ensemble_config, hot_batch_field
     n = 512
-    sizes = [(int(s), int(s)) for s in rng.choice([32, 48, 64, 96, 128, 256], n)]
-    betas = rng.uniform(2.0, 6.0, n).tolist()
-    am0s = rng.uniform(0.05, 0.3, n).tolist()
+    sizes, betas, am0s = ensemble_config(n, 2024)
     seeds = [9000 + r for r in range(n)]
     counter = 1
     b = q.Batch.ragged(sizes, betas)
-    g = torch.Generator(device="cuda").manual_seed(2024)
-    U = torch.polar(torch.ones(2 * b.sites, dtype=torch.float64, device="cuda"),
-                    (torch.rand(2 * b.sites, dtype=torch.float64, device="cuda", generator=g) * 2 - 1) * np.pi)
+    U = hot_batch_field(b, 2024)
     U0 = U.clone()
     infos = b.hmc_nf2(U, am0s, 0.1, 10, 20000, 1e-24, seeds, counter)
     assert all(np.isfinite(i.dH) for i in infos)

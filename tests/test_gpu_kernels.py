@@ -137,3 +137,20 @@ def test_topological_charge_exact_on_large_hot_field(q):
     prm = q.LattParm((L, L), 11.25)
     U = hot_links(L, L, 11)
     assert q.Qtop_rounded(to_dev(U), prm) == int(np.rint(Oracle(L, L, 11.25).qtop(U)))
+
+
+@pytest.mark.parametrize("L1,L2", [(64, 48), (333, 77)])
+def test_g5dw_complex64_vs_f64(q, L1, L2):
+    """The FP32 apply on complex64 fields against the FP64 apply of the same
+    (rounded) inputs: relative error at FP32 rounding, below 1e-6."""
+    import torch
+    prm = q.LattParm((L1, L2), 4.0)
+    U = to_dev(hot_links(L1, L2, 41)).to(torch.complex64)
+    si = to_dev(cgauss(L1, L2, 42, 2)).to(torch.complex64)
+    so = torch.empty_like(si)
+    q.gamm5Dw(so, U, si, 0.1, prm)
+    ref = q.cfield(L1, L2)
+    q.gamm5Dw(ref, U.to(torch.complex128), si.to(torch.complex128), 0.1, prm)
+    assert rel(to_host(so).astype(np.complex128), to_host(ref)) < 1e-6
+    with pytest.raises(ValueError):   # mixed precisions are rejected
+        q.gamm5Dw(so, U.to(torch.complex128), si, 0.1, prm)

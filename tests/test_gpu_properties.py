@@ -166,3 +166,25 @@ def test_zolotarev_bounds(q):
         r = q.get_rhmc_params(n, r_a, r_b)
         W = q.reweighting_factor(U, am0, 100000, 1e-25, prm, None, r)
         assert np.exp(-2 * V * r.delta) < W < np.exp(2 * V * r.delta)
+
+
+def test_energy_sums_are_compensated(q):
+    """The sums behind Action/Plaquette/Hamiltonian (and so Delta H) are
+    compensated: at 2048^2 they equal the correctly rounded sum of the site terms
+    (math.fsum) to within one ulp, where a plain FP64 sum drifts by many."""
+    import math
+    import torch
+    L = 2048
+    V = L * L   # a power of two: Plaquette * V is the raw sum
+    rng = np.random.default_rng(5)
+    U = np.exp(1j * 0.3 * rng.uniform(-1, 1, (2, L, L)))
+    U1, U2 = U[0], U[1]
+    P = (U1 * np.roll(U2, -1, axis=1)) * np.conj(np.roll(U1, -1, axis=0) * U2)
+    exact = math.fsum(P.real.ravel().tolist())
+    Ud = to_dev(U)
+    got = q.Plaquette(Ud, q.LattParm((L, L), 4.0)) * V
+    assert abs(got - exact) <= np.spacing(exact), (got - exact) / np.spacing(exact)
+    mom = rng.normal(size=(2, L, L))
+    exact_m = math.fsum((mom[0] ** 2 + mom[1] ** 2).ravel().tolist()) / 2
+    H = q.Hamiltonian(torch.from_numpy(mom).cuda(), Ud, q.LattParm((L, L), 0.0))
+    assert abs(H - exact_m) <= np.spacing(exact_m), (H - exact_m) / np.spacing(exact_m)
