@@ -13,13 +13,17 @@
 // and the single-lattice element order, so replica r reproduces a
 // single-lattice run with that seed.
 //
-// Work decomposition: a table lists every 32x8 tile of every replica, replica
-// after replica; a persistent block owns a contiguous range of the table and
-// walks it without division.  The tiles of one replica inside one block form a
-// "segment"; each segment writes one partial sum (fixed order inside), so
-// per-replica sums are deterministic.  The block arriving last at a barrier
-// sums each replica's segments, runs that replica's CG scalar recurrences
-// (state in global memory) and releases the others.
+// Work decomposition of the persistent solver: every replica's 32x8 tiles are
+// cut into chunks, the chunks dealt round-robin over the replicas, and each
+// block owns a contiguous range of that order, so one replica's work (its FP64
+// reliable updates run while the others wait) is spread over many blocks.  A
+// run of one replica's tiles inside a block is a "segment" with one partial
+// sum (fixed order inside), so per-replica sums are deterministic.  The block
+// arriving last at a barrier sums each replica's partials and either publishes
+// the sums (at most 64 replicas: every block keeps all replicas' CG records in
+// shared memory and updates them itself) or updates the records in global
+// memory.  Standalone kernels (forces, link updates, sums) run one block per
+// tile of a replica-major tile table.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -226,13 +230,20 @@ enum { FL_ACT, FL_UPD, FL_R4, FL_N };   // any replica active / updating / resca
 enum { RED_BB, RED_RR0, RED_PAP, RED_RN, RED_TRUE, RED_R4 };
 enum { PH_SETUP, PH_START, PH_A, PH_B, PH_R1, PH_R2, PH_R3, PH_R4 };
 
+// One segment of the solver's work: n tiles of replica r starting at tile
+// (t1, t2), walked row by row; its partial sum goes to part[slot].  Slots are
+// numbered replica by replica, so replica r's partials are the contiguous
+// range rep_seg[r] .. rep_seg[r+1]-1.
+struct SegDesc {
+    int r, t1, t2, n, slot, pad0, pad1, pad2;
+};
+
 struct RCGP {
-    int nrep, ntiles, per_block, lg;   // lg: log2 of the lanes summing one replica's segments
-    int nseg;
+    int nrep, lg;         // lg: log2 of the lanes summing one replica's partials
     const RepInfo* reps;
-    const int4* tiles;
-    const int* seg0;      // [grid] first segment of each block
-    const int* rep_seg;   // [nrep+1] segments of replica r: rep_seg[r] .. rep_seg[r+1]-1
+    const SegDesc* segs;  // segments, block after block
+    const int* seg0;      // [grid+1] segments of block b: seg0[b] .. seg0[b+1]-1
+    const int* rep_seg;   // [nrep+1] partial slots of replica r
     const double* m2;     // 2 + m0 per replica
     const double2* U;
     const float4* U32;
@@ -364,47 +375,57 @@ __device__ __forceinline__ acc_t<PH> tile_work(const RCGP& P, const RepVals& v, 
 // A block's place in the tile table (set once per launch, kept in shared
 // memory) and the records of its first kSegCache replicas, so that a phase
 // starts without global loads.
-constexpr int kSegCache = 16;
+constexpr int kSegCache = 64;
 struct BlockCtx {
-    int r0, t1, t2, seg, lo, hi, nsb;   // first replica and tile, first segment, tile range, segments
+    int seg, nsb;   // first segment, segments of this block
 };
 struct SegInfo {
+    SegDesc d;
     RepInfo R;
     double m2;
+};
+// per-block shared scratch of a phase: the segments' scalars and per-warp partials
+struct PhaseScratch {
+    RepVals vals[kSegCache];
+    double wsum[kSegCache][TILE / 32];
 };
 
 __device__ __forceinline__ void block_ctx_init(const RCGP& P, BlockCtx& bc, SegInfo* seg) {
     if (threadIdx.x == 0) {
-        const int lo = blockIdx.x * P.per_block;
-        const int4 T0 = P.tiles[lo];
         const int s0 = P.seg0[blockIdx.x];
-        const int s1 = blockIdx.x + 1 < gridDim.x ? P.seg0[blockIdx.x + 1] : P.nseg;
-        bc = BlockCtx{T0.x, T0.y, T0.z, s0, lo, min(lo + P.per_block, P.ntiles), s1 - s0};
+        bc = BlockCtx{s0, P.seg0[blockIdx.x + 1] - s0};
     }
     __syncthreads();
     for (int i = threadIdx.x; i < min(bc.nsb, kSegCache); i += blockDim.x) {
-        seg[i].R = P.reps[bc.r0 + i];
-        seg[i].m2 = P.m2[bc.r0 + i];
+        const SegDesc d = P.segs[bc.seg + i];
+        seg[i].d = d;
+        seg[i].R = P.reps[d.r];
+        seg[i].m2 = P.m2[d.r];
     }
     __syncthreads();
 }
 
-// One phase over the block's tile range: the tiles of each replica form one
-// segment with one partial sum (phases R1 and R2 sum nothing).
+// One phase over the block's segments (phases R1 and R2 sum nothing).  The
+// scalars of the block's first kSegCache segments are fetched together at the
+// start (one round trip), and a segment's partial is a warp sum per warp,
+// summed over the warps in a fixed order at the end of the phase; further
+// segments fetch their scalars and reduce one by one.
 template <int PH, bool SH>
 __device__ __forceinline__ void run_phase(const RCGP& P, const StateView<SH>& sv, int cur, const BlockCtx& bcs,
-                                          const SegInfo* segs, double* smem) {
+                                          const SegInfo* segs, PhaseScratch& ps, double* smem) {
     constexpr bool kSum = PH != PH_R1 && PH != PH_R2;
-    int t1 = bcs.t1, t2 = bcs.t2, tt = bcs.lo;
-    for (int i = 0;; i++) {
-        const int r = bcs.r0 + i;
-        const RepInfo R = i < kSegCache ? segs[i].R : P.reps[r];
-        const double m2 = i < kSegCache ? segs[i].m2 : __ldg(P.m2 + r);
-        const int n = min(bcs.hi - tt, R.nt - (t2 * R.nt1 + t1));
-        const RepVals v = rep_vals<PH, SH>(sv, r, m2);
+    const int nsb = bcs.nsb, ncache = min(nsb, kSegCache);
+    if (threadIdx.x < ncache) ps.vals[threadIdx.x] = rep_vals<PH, SH>(sv, segs[threadIdx.x].d.r, segs[threadIdx.x].m2);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int i = 0; i < nsb; i++) {
+        const bool cached = i < kSegCache;
+        const SegDesc d = cached ? segs[i].d : P.segs[bcs.seg + i];
+        const RepInfo R = cached ? segs[i].R : P.reps[d.r];
+        const RepVals v = cached ? ps.vals[i] : rep_vals<PH, SH>(sv, d.r, __ldg(P.m2 + d.r));
         acc_t<PH> acc = 0;
         if (v.work)
-            for (int j = 0; j < n; j++) {
+            for (int j = 0, t1 = d.t1, t2 = d.t2; j < d.n; j++) {
                 acc += tile_work<PH>(P, v, R, t1, t2, cur);
                 if (++t1 == R.nt1) {
                     t1 = 0;
@@ -412,14 +433,27 @@ __device__ __forceinline__ void run_phase(const RCGP& P, const StateView<SH>& sv
                 }
             }
         if constexpr (kSum) {
-            double red[1] = {(double)acc};
-            block_sum<1>(red, smem);
-            if (threadIdx.x == 0) P.part[bcs.seg + i] = red[0];
+            if (cached) {
+                double w = (double)acc;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+                if (lane == 0) ps.wsum[i][warp] = w;
+            } else {
+                double red[1] = {(double)acc};
+                block_sum<1>(red, smem);
+                if (threadIdx.x == 0) P.part[d.slot] = red[0];
+            }
         }
-        tt += n;
-        if (tt >= bcs.hi) break;
-        t1 = 0;
-        t2 = 0;
+    }
+    if constexpr (kSum) {
+        __syncthreads();
+        if (threadIdx.x < ncache) {
+            double s = 0.0;
+#pragma unroll
+            for (int w = 0; w < TILE / 32; w++) s += ps.wsum[threadIdx.x][w];
+            P.part[segs[threadIdx.x].d.slot] = s;
+            __threadfence();
+        }
     }
 }
 
@@ -594,28 +628,28 @@ __device__ __forceinline__ bool rbarrier(GridSync& gs, const RCGP& P, RepState* 
 // the solve; false when a barrier gave up
 template <bool SH>
 __device__ __forceinline__ bool r_body(const RCGP& P, GridSync& gs, int& k, double* smem, RepState* s_st, int* s_fl,
-                                       const int* s_rseg, const BlockCtx& bc, const SegInfo* segs) {
+                                       const int* s_rseg, const BlockCtx& bc, const SegInfo* segs, PhaseScratch& ps) {
     const StateView<SH> sv{s_st, P.st};
     int cur = 0;
-    run_phase<PH_SETUP, SH>(P, sv, cur, bc, segs, smem);
+    run_phase<PH_SETUP, SH>(P, sv, cur, bc, segs, ps, smem);
     if (!rbarrier<SH>(gs, P, s_st, s_fl, s_rseg, RED_BB, 0)) return false;
-    run_phase<PH_START, SH>(P, sv, cur, bc, segs, smem);
+    run_phase<PH_START, SH>(P, sv, cur, bc, segs, ps, smem);
     if (!rbarrier<SH>(gs, P, s_st, s_fl, s_rseg, RED_RR0, 0)) return false;
     for (k = 1; k <= P.maxiter; k++) {
         if (!s_fl[FL_ACT]) break;
-        run_phase<PH_A, SH>(P, sv, cur, bc, segs, smem);
+        run_phase<PH_A, SH>(P, sv, cur, bc, segs, ps, smem);
         if (!rbarrier<SH>(gs, P, s_st, s_fl, s_rseg, RED_PAP, k)) return false;
-        run_phase<PH_B, SH>(P, sv, cur, bc, segs, smem);
+        run_phase<PH_B, SH>(P, sv, cur, bc, segs, ps, smem);
         if (!rbarrier<SH>(gs, P, s_st, s_fl, s_rseg, RED_RN, k)) return false;
         if (s_fl[FL_UPD]) {
-            run_phase<PH_R1, SH>(P, sv, cur, bc, segs, smem);
+            run_phase<PH_R1, SH>(P, sv, cur, bc, segs, ps, smem);
             if (!gs.sync()) return false;
-            run_phase<PH_R2, SH>(P, sv, cur, bc, segs, smem);
+            run_phase<PH_R2, SH>(P, sv, cur, bc, segs, ps, smem);
             if (!gs.sync()) return false;
-            run_phase<PH_R3, SH>(P, sv, cur, bc, segs, smem);
+            run_phase<PH_R3, SH>(P, sv, cur, bc, segs, ps, smem);
             if (!rbarrier<SH>(gs, P, s_st, s_fl, s_rseg, RED_TRUE, k)) return false;
             if (s_fl[FL_R4]) {
-                run_phase<PH_R4, SH>(P, sv, cur, bc, segs, smem);
+                run_phase<PH_R4, SH>(P, sv, cur, bc, segs, ps, smem);
                 if (!rbarrier<SH>(gs, P, s_st, s_fl, s_rseg, RED_R4, k)) return false;
             }
         }
@@ -631,6 +665,7 @@ __global__ void __launch_bounds__(TILE, 4) k_r_cg_mixed(const RCGP P) {
     __shared__ int s_fl[FL_N];
     __shared__ BlockCtx s_bc;
     __shared__ SegInfo s_seg[kSegCache];
+    __shared__ PhaseScratch s_ps;
     __shared__ int s_rseg[SH ? kSharedReps + 1 : 1];   // the replicas' segment ranges (SH)
     if (threadIdx.x < FL_N) s_fl[threadIdx.x] = 0;
     if (SH)
@@ -638,7 +673,7 @@ __global__ void __launch_bounds__(TILE, 4) k_r_cg_mixed(const RCGP P) {
     block_ctx_init(P, s_bc, s_seg);
     GridSync gs{&P.ctl->bar, &P.ctl->gen, &P.ctl->err};
     int k = 0;
-    const bool ok = r_body<SH>(P, gs, k, smem, s_st, s_fl, s_rseg, s_bc, s_seg);
+    const bool ok = r_body<SH>(P, gs, k, smem, s_st, s_fl, s_rseg, s_bc, s_seg, s_ps);
     if (blockIdx.x == 0) {
         if (SH && ok)   // every block holds the same records: block 0 stores them
             for (int r = threadIdx.x; r < P.nrep; r += blockDim.x) P.st[r] = s_st[r];
@@ -687,6 +722,7 @@ struct qed2d_batch {
     RepInfo* d_reps = nullptr;
     int4* d_tiles = nullptr;
     int* d_seg0 = nullptr;
+    SegDesc* d_segs = nullptr;
     int* d_rep_seg = nullptr;
     long long* d_dbase_c = nullptr;   // first double of each replica: complex fields [nrep+1]
     long long* d_dbase_r = nullptr;   // the same for real fields
@@ -765,12 +801,9 @@ int r_solve(qed2d_batch* h, const double2* U, const float4* U32, const double2* 
             int maxiter, double eps) {
     RCGP P{};
     P.nrep = h->nrep;
-    P.ntiles = h->ntiles;
-    P.per_block = h->per_block;
     P.lg = h->lg;
-    P.nseg = h->nseg;
     P.reps = h->d_reps;
-    P.tiles = h->d_tiles;
+    P.segs = h->d_segs;
     P.seg0 = h->d_seg0;
     P.rep_seg = h->d_rep_seg;
     P.m2 = h->d_m2;
@@ -881,22 +914,48 @@ int batch_setup(qed2d_batch* h, const int* L1, const int* L2, const double* beta
         return QED2D_ERR_UNSUPPORTED;
     }
     const long long maxg = std::min<long long>((long long)per_sm * h->num_sms, kMaxPartBlocks);
+    // Work order of the persistent solver: every replica's tiles cut into chunks
+    // of `chunk` tiles, the chunks dealt round-robin over the replicas, so the
+    // work of any one replica is spread over many blocks (a replica's FP64
+    // reliable updates run while the others wait); blocks take contiguous
+    // ranges of this order, and each run of consecutive tiles of one replica
+    // inside a block is a segment with its own partial sum.
+    const int chunk = std::max(8, (h->ntiles + 4095) / 4096);
+    std::vector<int2> order;   // (replica, tile index inside the replica)
+    order.reserve(h->ntiles);
+    int maxch = 0;
+    for (int r = 0; r < B; r++) maxch = std::max(maxch, (h->reps[r].nt + chunk - 1) / chunk);
+    for (int k = 0; k < maxch; k++)
+        for (int r = 0; r < B; r++)
+            for (int lt = k * chunk; lt < std::min((k + 1) * chunk, h->reps[r].nt); lt++) order.push_back(make_int2(r, lt));
     h->per_block = (int)((h->ntiles + maxg - 1) / maxg);
     h->grid = (h->ntiles + h->per_block - 1) / h->per_block;
-    std::vector<int> seg0(h->grid), seg_rep;
+    std::vector<int> seg0(h->grid + 1);
+    std::vector<SegDesc> segs;
+    std::vector<std::vector<int>> rep_segs(B);   // segments of each replica, in block order
     for (int b = 0; b < h->grid; b++) {
-        seg0[b] = (int)seg_rep.size();
+        seg0[b] = (int)segs.size();
         const int lo = b * h->per_block, hi = std::min(lo + h->per_block, h->ntiles);
-        for (int t = lo; t < hi; t++)
-            if (t == lo || tiles[t].x != tiles[t - 1].x) seg_rep.push_back(tiles[t].x);
+        for (int t = lo; t < hi; t++) {
+            const int2 o = order[t];
+            if (t > lo && o.x == order[t - 1].x && o.y == order[t - 1].y + 1) {
+                segs.back().n++;
+                continue;
+            }
+            const RepInfo& R = h->reps[o.x];
+            rep_segs[o.x].push_back((int)segs.size());
+            segs.push_back(SegDesc{o.x, o.y % R.nt1, o.y / R.nt1, 1, 0, 0, 0, 0});
+        }
     }
-    h->nseg = (int)seg_rep.size();
-    std::vector<int> rep_seg(B + 1, 0);   // segments are ordered by replica
-    for (int s = 0; s < h->nseg; s++) rep_seg[seg_rep[s] + 1] = s + 1;
+    seg0[h->grid] = (int)segs.size();
+    h->nseg = (int)segs.size();
+    std::vector<int> rep_seg(B + 1, 0);   // partial slots: replica by replica
     int maxsegs = 0;
-    for (int r = 0; r < B; r++) {
-        rep_seg[r + 1] = std::max(rep_seg[r + 1], rep_seg[r]);
-        maxsegs = std::max(maxsegs, rep_seg[r + 1] - rep_seg[r]);
+    for (int r = 0, slot = 0; r < B; r++) {
+        rep_seg[r] = slot;
+        for (int i : rep_segs[r]) segs[i].slot = slot++;
+        rep_seg[r + 1] = slot;
+        maxsegs = std::max(maxsegs, (int)rep_segs[r].size());
     }
     // lanes per replica in the last block's sums: fewest rounds of loads
     long long best = -1;
@@ -934,6 +993,7 @@ int batch_setup(qed2d_batch* h, const int* L1, const int* L2, const double* beta
     QTRY(upload(&h->d_reps, h->reps));
     QTRY(upload(&h->d_tiles, tiles));
     QTRY(upload(&h->d_seg0, seg0));
+    QTRY(upload(&h->d_segs, segs));
     QTRY(upload(&h->d_rep_seg, rep_seg));
     QTRY(upload(&h->d_dbase_c, dbc));
     QTRY(upload(&h->d_dbase_r, dbr));
@@ -1014,7 +1074,7 @@ int qed2d_batch_destroy(qed2d_batch* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     else cudaDeviceSynchronize();
     for (auto& kv : h->ws) cudaFree(kv.second.first);
-    void* dev[] = {h->d_reps, h->d_tiles, h->d_seg0, h->d_rep_seg, h->d_dbase_c, h->d_dbase_r, h->d_m2,
+    void* dev[] = {h->d_reps, h->d_tiles, h->d_seg0, h->d_segs, h->d_rep_seg, h->d_dbase_c, h->d_dbase_r, h->d_m2,
                    h->d_beta, h->d_seed,  h->d_st, h->d_flags, h->d_red, h->d_upart, h->d_ured,      h->d_out,     h->d_iters,   h->d_sums,
                    h->d_tpart, h->d_part, h->ctl};
     for (void* p : dev)
