@@ -734,6 +734,7 @@ struct qed2d_batch {
     double* d_red = nullptr;        // [nrep]
     bool shared_state = false;      // records in shared memory (nrep <= kSharedReps)
     bool uniform = false;           // equal sizes, nrep <= kUniformReps: k_u_cg_mixed
+    int usched = -1;                // its reduction schedule (-1: not tuned yet)
     UGeom ug{};
     int ugrid = 0, ubpr = 0, uper_block = 0;
     double* d_upart = nullptr;      // [2][ubpr * nrep]
@@ -797,6 +798,48 @@ int r_pack(qed2d_batch* h, double2* U, const double* mom, double eps, float4* U3
     return r_post("k_r_updt");
 }
 
+// First solve of an equal-size batch: time both reduction schedules of
+// k_u_cg_mixed (same bits) on the caller's operator and sources, capped at 24
+// iterations, into scratch outputs, and keep the faster; the device control
+// block is saved and restored around it.  QED2D_TUNE=0: every block sums.
+template <class Launch>
+int tune_uniform(qed2d_batch* h, const UCGP& Q, int maxiter, Launch launch) {
+    if (!tuning_enabled()) {
+        h->usched = 1;
+        return QED2D_OK;
+    }
+    DevCtl saved;
+    QCHECK(cudaMemcpyAsync(&saved, h->ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, h->stream));
+    QCHECK(cudaStreamSynchronize(h->stream));
+    UCGP T = Q;
+    T.x = h->field("tune_x");
+    T.t64 = h->field("tune_g5x");
+    T.maxiter = std::min(maxiter, 24);
+    if (!T.x || !T.t64) return QED2D_ERR_NO_MEMORY;
+    cudaEvent_t e0, e1;
+    QCHECK(cudaEventCreate(&e0));
+    QCHECK(cudaEventCreate(&e1));
+    float tbest[2] = {1e30f, 1e30f};
+    int st = QED2D_OK;
+    for (int rep = 0; rep < 3 && st == QED2D_OK; rep++)
+        for (int rs = 0; rs < 2 && st == QED2D_OK; rs++) {
+            cudaEventRecord(e0, h->stream);
+            st = launch(rs, T);
+            cudaEventRecord(e1, h->stream);
+            if (cudaEventSynchronize(e1) != cudaSuccess) st = cuda_status(cudaGetLastError(), "schedule tuning");
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep > 0) tbest[rs] = std::min(tbest[rs], ms);   // the first round warms up
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    QCHECK(cudaMemcpyAsync(h->ctl, &saved, sizeof(DevCtl), cudaMemcpyHostToDevice, h->stream));
+    QCHECK(cudaStreamSynchronize(h->stream));
+    if (st != QED2D_OK) return st;
+    h->usched = tbest[1] <= tbest[0] ? 1 : 0;
+    return QED2D_OK;
+}
+
 int r_solve(qed2d_batch* h, const double2* U, const float4* U32, const double2* b, double2* x, double2* g5x,
             int maxiter, double eps) {
     RCGP P{};
@@ -853,9 +896,19 @@ int r_solve(qed2d_batch* h, const double2* U, const float4* U32, const double2* 
         Q.part = h->d_upart;
         Q.red = h->d_ured;
         Q.st_out = h->d_st;
-        void* uargs[] = {(void*)&Q};
-        QCHECK(cudaLaunchCooperativeKernel((const void*)k_u_cg_mixed, dim3((unsigned)h->ugrid), dim3(TILE), uargs, 0,
-                                           h->stream));
+        auto launch = [&](int rs, const UCGP& q) -> int {
+            QCHECK(cudaMemsetAsync(&h->ctl->bar, 0, 2 * sizeof(unsigned long long) + sizeof(int), h->stream));
+            void* uargs[] = {(void*)&q};
+            QCHECK(cudaLaunchCooperativeKernel(rs ? (const void*)k_u_cg_mixed<1> : (const void*)k_u_cg_mixed<0>,
+                                               dim3((unsigned)h->ugrid), dim3(TILE), uargs, 0, h->stream));
+            count_launch();
+            return QED2D_OK;
+        };
+        if (h->usched < 0) QTRY(tune_uniform(h, Q, maxiter, launch));
+        QTRY(launch(h->usched, Q));
+        k_r_finish<<<1, 256, 0, h->stream>>>(h->d_st, h->nrep, maxiter, h->d_out, h->d_out + h->nrep, h->d_iters,
+                                              h->ctl);
+        return r_post("k_r_finish");
     } else {
         const void* kern = h->shared_state ? (const void*)k_r_cg_mixed<true> : (const void*)k_r_cg_mixed<false>;
         QCHECK(cudaLaunchCooperativeKernel(kern, dim3((unsigned)h->grid), dim3(TILE), args, 0, h->stream));
@@ -972,7 +1025,10 @@ int batch_setup(qed2d_batch* h, const int* L1, const int* L2, const double* beta
     for (int r = 1; r < B && same; r++) same = L1[r] == L1[0] && L2[r] == L2[0];
     if (same) {
         int per_smu = 0;
-        QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_smu, k_u_cg_mixed, TILE, 0));
+        int per_smu1 = 0;
+        QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_smu, k_u_cg_mixed<0>, TILE, 0));
+        QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_smu1, k_u_cg_mixed<1>, TILE, 0));
+        per_smu = std::min(per_smu, per_smu1);
         const long long maxgu = std::min<long long>((long long)per_smu * h->num_sms, kMaxPartBlocks);
         const RepInfo& R0 = h->reps[0];
         if (per_smu >= 1 && maxgu / B >= 1) {
@@ -1087,6 +1143,21 @@ int qed2d_batch_destroy(qed2d_batch* h) {
 int qed2d_batch_set_stream(qed2d_batch* h, void* stream) {
     if (!h) return QED2D_ERR_BAD_ARG;
     h->stream = (cudaStream_t)stream;
+    return QED2D_OK;
+}
+
+int qed2d_batch_set_schedule(qed2d_batch* h, int schedule) {
+    if (!h || schedule < -1 || schedule > 1) {
+        set_error("qed2d_batch_set_schedule: schedule must be -1, 0 or 1");
+        return QED2D_ERR_BAD_ARG;
+    }
+    h->usched = schedule;
+    return QED2D_OK;
+}
+
+int qed2d_batch_get_schedule(const qed2d_batch* h, int* schedule) {
+    if (!h || !schedule) return QED2D_ERR_BAD_ARG;
+    *schedule = h->uniform ? h->usched : 2;
     return QED2D_OK;
 }
 

@@ -3,10 +3,10 @@
 //
 // Block b serves replica b / bpr only, and a contiguous range of that
 // replica's tiles, so every block's geometry, masses and pointers are kernel
-// constants and a phase starts without any loads.  The block arriving last at
-// a barrier sums each replica's partials in a fixed order (deterministic) and
-// publishes one sum per replica; every block then runs the per-replica CG
-// scalar recurrences itself in shared memory.  Replicas that have converged
+// constants and a phase starts without any loads.  Each replica's partials are
+// summed in a fixed order (deterministic) under one of two schedules (ureduce),
+// and every block runs the per-replica CG scalar recurrences itself in shared
+// memory.  Replicas that have converged
 // stop working but keep joining the barriers until all are done.  The
 // recurrences are those of the ragged kernel (rep_step) and of the
 // single-lattice mixed solver.
@@ -41,7 +41,7 @@ struct UCGP {
     int maxiter, bpr, per_block;
     DevCtl* ctl;
     double* part;       // [2][bpr * B] block partials (alternating)
-    double* red;        // [2][B] per-replica sums (alternating)
+    double* red;        // [2][B] published per-replica sums (RS = 0)
     RepState* st_out;   // [B] final records
 };
 
@@ -60,12 +60,18 @@ __device__ __forceinline__ Site usite_at(const UGeom& g, int r, int t1, int t2, 
     return s;
 }
 
-// Barrier with one sum per replica: the last block sums the replicas' partials
-// (one warp per replica) into red[]; then every block runs the recurrences of
-// every replica for reduction `kind` on its shared records and flags.
+// Barrier with one sum per replica (one warp per replica over its blocks'
+// partials, fixed order).  Two schedules give the same bits: RS = 0, the last
+// block to arrive sums and publishes red[] before releasing and every block
+// reads red[]; RS = 1, the last block releases at once and every block sums
+// the partials itself.  Then every block runs every replica's recurrences for
+// reduction `kind` on its shared records and flags.  A failed or timed-out
+// wait is passed on through shared memory.
+template <int RS>
 __device__ __forceinline__ bool ureduce(GridSync& gs, double v, const UCGP& P, double* smem, RepState* s_st,
                                         int* s_fl, int kind, int k) {
-    __shared__ int s_last, s_bits;
+    __shared__ int s_last, s_bits, s_ok;
+    __shared__ double s_red[kUniformReps];
     const int buf = gs.nred++ & 1;
     double* part = P.part + (size_t)buf * P.bpr * P.g.B;
     double* red = P.red + (size_t)buf * P.g.B;
@@ -76,26 +82,48 @@ __device__ __forceinline__ bool ureduce(GridSync& gs, double v, const UCGP& P, d
         s_bits = 0;
     }
     const bool last = gs.arrive(&s_last);
-    if (last) {
-        __threadfence();
-        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    auto sum_partials = [&](double* out) {
         for (int r = warp; r < P.g.B; r += nw) {
             double s = 0.0;
             for (int i = lane; i < P.bpr; i += 32) s += __ldcg(part + (size_t)r * P.bpr + i);
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == 0) red[r] = s;
+            if (lane == 0) out[r] = s;
+        }
+    };
+    if constexpr (RS == 0) {
+        if (last) {
+            __threadfence();
+            sum_partials(red);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                gs.release();
+                s_ok = 1;
+            }
+        } else if (threadIdx.x == 0) {
+            s_ok = gs.wait();
         }
         __syncthreads();
-        if (threadIdx.x == 0) gs.release();
-    } else if (threadIdx.x == 0) {
-        gs.wait();
+        if (threadIdx.x < P.g.B) s_red[threadIdx.x] = __ldcg(red + threadIdx.x);
+    } else {
+        if (threadIdx.x == 0) {
+            if (last) {
+                gs.release();
+                s_ok = 1;
+            } else {
+                s_ok = gs.wait();
+            }
+        }
+        __syncthreads();
+        if (last) __threadfence();
+        sum_partials(s_red);
     }
     __syncthreads();
     int fl[FL_N] = {0, 0, 0};
     if (threadIdx.x < P.g.B) {
         RepState st = s_st[threadIdx.x];
-        rep_step(st, kind, __ldcg(red + threadIdx.x), k, P.eps, P.delta2, P.maxiter, fl);
+        rep_step(st, kind, s_red[threadIdx.x], k, P.eps, P.delta2, P.maxiter, fl);
         s_st[threadIdx.x] = st;
     }
     const int bits = __reduce_or_sync(0xffffffffu, fl[FL_ACT] | fl[FL_UPD] << 1 | fl[FL_R4] << 2);
@@ -108,7 +136,7 @@ __device__ __forceinline__ bool ureduce(GridSync& gs, double v, const UCGP& P, d
         s_fl[FL_R4] |= (s_bits >> 2) & 1;
     }
     __syncthreads();
-    return ld_volatile_int(gs.err) == 0;
+    return s_ok != 0;
 }
 
 // this block's contiguous range of its replica's tiles, walked without division
@@ -117,6 +145,7 @@ __device__ __forceinline__ bool ureduce(GridSync& gs, double v, const UCGP& P, d
          ++tt_, (++t1_ == TR.nt1 ? (t1_ = 0, ++t2_) : 0))                                       \
         if (const Site q = usite_at(P.g, myr, t1_, t2_, threadIdx.x); q.ok)
 
+template <int RS>
 __device__ __forceinline__ bool u_body(const UCGP& P, GridSync& gs, int& k, double* smem, RepState* s_st,
                                        int* s_fl) {
     const int myr = blockIdx.x / P.bpr, lb = blockIdx.x - myr * P.bpr;
@@ -141,7 +170,7 @@ __device__ __forceinline__ bool u_body(const UCGP& P, GridSync& gs, int& k, doub
             v += norm2(bv.a) + norm2(bv.b);
             st_d(xx, V, q.x, z);
         }
-        if (!ureduce(gs, v, P, smem, s_st, s_fl, RED_BB, 0)) return false;
+        if (!ureduce<RS>(gs, v, P, smem, s_st, s_fl, RED_BB, 0)) return false;
     }
     {   // r32 = s b, x32 = 0 (a zero source keeps x = 0 and g5Dw x = 0)
         double v = 0.0;
@@ -156,7 +185,7 @@ __device__ __forceinline__ bool u_body(const UCGP& P, GridSync& gs, int& k, doub
                 st_d(t64, V, q.x, z);
             }
         }
-        if (!ureduce(gs, v, P, smem, s_st, s_fl, RED_RR0, 0)) return false;
+        if (!ureduce<RS>(gs, v, P, smem, s_st, s_fl, RED_RR0, 0)) return false;
     }
     for (k = 1; k <= P.maxiter; k++) {
         if (!s_fl[FL_ACT]) break;
@@ -175,7 +204,7 @@ __device__ __forceinline__ bool u_body(const UCGP& P, GridSync& gs, int& k, doub
                     f += norm2(tt.a) + norm2(tt.b);
                 }
             }
-            if (!ureduce(gs, (double)f, P, smem, s_st, s_fl, RED_PAP, k)) return false;
+            if (!ureduce<RS>(gs, (double)f, P, smem, s_st, s_fl, RED_PAP, k)) return false;
         }
         {   // x += alpha p, r -= alpha g5Dw t
             float f = 0.f;
@@ -195,7 +224,7 @@ __device__ __forceinline__ bool u_body(const UCGP& P, GridSync& gs, int& k, doub
                     f += norm2(r.a) + norm2(r.b);
                 }
             }
-            if (!ureduce(gs, (double)f, P, smem, s_st, s_fl, RED_RN, k)) return false;
+            if (!ureduce<RS>(gs, (double)f, P, smem, s_st, s_fl, RED_RN, k)) return false;
         }
         if (s_fl[FL_UPD]) {   // FP64 reliable update of the replicas that asked for one
             const RepState st = s_st[myr];
@@ -220,7 +249,7 @@ __device__ __forceinline__ bool u_body(const UCGP& P, GridSync& gs, int& k, doub
                     st_d(r64, V, q.x, r);
                     w += norm2(r.a) + norm2(r.b);
                 }
-            if (!ureduce(gs, w, P, smem, s_st, s_fl, RED_TRUE, k)) return false;
+            if (!ureduce<RS>(gs, w, P, smem, s_st, s_fl, RED_TRUE, k)) return false;
             if (s_fl[FL_R4]) {
                 double v = 0.0;
                 const RepState st4 = s_st[myr];
@@ -229,7 +258,7 @@ __device__ __forceinline__ bool u_body(const UCGP& P, GridSync& gs, int& k, doub
                         st_f(P.r32, q.x, r32);
                         v += (double)(norm2(r32.a) + norm2(r32.b));
                     }
-                if (!ureduce(gs, v, P, smem, s_st, s_fl, RED_R4, k)) return false;
+                if (!ureduce<RS>(gs, v, P, smem, s_st, s_fl, RED_R4, k)) return false;
             }
         }
         cur ^= 1;
@@ -238,6 +267,7 @@ __device__ __forceinline__ bool u_body(const UCGP& P, GridSync& gs, int& k, doub
 }
 #undef FOR_MY_UTILES
 
+template <int RS>
 __global__ void __launch_bounds__(TILE, 4) k_u_cg_mixed(const UCGP P) {
     __shared__ double smem[32];
     __shared__ RepState s_st[kUniformReps];
@@ -246,7 +276,7 @@ __global__ void __launch_bounds__(TILE, 4) k_u_cg_mixed(const UCGP P) {
     __syncthreads();
     GridSync gs{&P.ctl->bar, &P.ctl->gen, &P.ctl->err};
     int k = 0;
-    const bool ok = u_body(P, gs, k, smem, s_st, s_fl);
+    const bool ok = u_body<RS>(P, gs, k, smem, s_st, s_fl);
     if (blockIdx.x == 0) {
         if (ok)   // every block holds the same records: block 0 stores them
             for (int r = threadIdx.x; r < P.g.B; r += blockDim.x) P.st_out[r] = s_st[r];

@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstddef>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -68,44 +69,78 @@ __device__ __forceinline__ void write_partials(double* part, const double* v, in
 }
 
 // Grid-wide sum of NV values (NV <= 4), deterministic: every block writes its
-// partials; the last block to arrive sums them in a fixed order (thread t takes
-// partials t, t+blockDim, ..., then a fixed-shape tree), publishes the sums in
-// ctl->red and releases the barrier; every block then reads the sums.  Partials
-// and sums alternate between two buffers: reduction n+2 overwrites buffer n's
-// only after every block has passed barrier n+1, i.e. has read the result of n.
-template <int NV>
+// partials and arrives at a bounded grid barrier; the partials are summed in a
+// fixed order (thread t takes partials t, t+blockDim, ..., then a fixed-shape
+// tree).  Two schedules give the same bits:
+//   RS = 0: the last block to arrive sums them, publishes the sums in red[]
+//           and releases; every block then reads red[] (one more round trip);
+//   RS = 1: the last block releases at once and every block sums all partials
+//           itself (no second round trip, more L2 reads).
+// Which one is faster depends on the lattice size; the context tunes it.
+// Partials and sums alternate between two buffers: reduction n+2 overwrites
+// buffer n's only after every block has passed barrier n+1, i.e. has read the
+// results of n.  (The error flag is read once per barrier: a status kept in
+// shared memory instead made these kernels spill, 7% slower at 2048^2.)
+template <int NV, int RS>
 __device__ __forceinline__ bool reduce_sync(GridSync& gs, double (&v)[NV], double* part_base, double* red_base,
                                             double* smem) {
     static_assert(NV <= kMaxPartVals / 2, "too many values for the double-buffered partials");
     __shared__ int s_last;
     const int buf = gs.nred++ & 1;
     double* part = part_base + (size_t)buf * (kMaxPartVals / 2) * kMaxPartBlocks;
-    double* red = red_base + buf * 4;
     block_sum<NV>(v, smem);
     write_partials(part, v, NV);
     const bool last = gs.arrive(&s_last);
-    if (last) {
-        __threadfence();
-        double w[NV];
+    if constexpr (RS == 0) {
+        double* red = red_base + buf * 4;
+        if (last) {
+            __threadfence();
+            double w[NV];
+#pragma unroll
+            for (int k = 0; k < NV; k++) {
+                double s = 0.0;
+                for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x)
+                    s += __ldcg(part + (size_t)k * kMaxPartBlocks + i);
+                w[k] = s;
+            }
+            block_sum<NV>(w, smem);
+            if (threadIdx.x == 0) {
+#pragma unroll
+                for (int k = 0; k < NV; k++) red[k] = w[k];
+                gs.release();
+            }
+        } else if (threadIdx.x == 0) {
+            gs.wait();
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < NV; k++) v[k] = __ldcg(red + k);
+        return ld_volatile_int(gs.err) == 0;
+    } else {
+        if (threadIdx.x == 0) {
+            if (last) gs.release();
+            else gs.wait();
+        }
+        __syncthreads();
+        const bool ok = ld_volatile_int(gs.err) == 0;   // issued together with the partial loads
+        if (last) __threadfence();
 #pragma unroll
         for (int k = 0; k < NV; k++) {
             double s = 0.0;
-            for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) s += __ldcg(part + (size_t)k * kMaxPartBlocks + i);
-            w[k] = s;
+            for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x)
+                s += __ldcg(part + (size_t)k * kMaxPartBlocks + i);
+            v[k] = s;
         }
-        block_sum<NV>(w, smem);
-        if (threadIdx.x == 0) {
+        block_sum<NV>(v, smem);
+        __shared__ double s_v[4];
+        if (threadIdx.x == 0)
 #pragma unroll
-            for (int k = 0; k < NV; k++) red[k] = w[k];
-            gs.release();
-        }
-    } else if (threadIdx.x == 0) {
-        gs.wait();
+            for (int k = 0; k < NV; k++) s_v[k] = v[k];
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < NV; k++) v[k] = s_v[k];
+        return ok;
     }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < NV; k++) v[k] = __ldcg(red + k);
-    return ld_volatile_int(gs.err) == 0;
 }
 
 __device__ __forceinline__ void finish_solve(const CGP& P, int iters, bool conv, double rr, double bb,
@@ -129,6 +164,7 @@ __device__ __forceinline__ void finish_solve(const CGP& P, int iters, bool conv,
 
 // ---------------------------------------------------------------------------
 // FP64 persistent CG
+template <int RS>
 __global__ void __launch_bounds__(TILE, 3) k_cg_f64(const CGP P) {
     __shared__ double smem[32 * 2];
     GridSync gs{&P.ctl->bar, &P.ctl->gen, &P.ctl->err};
@@ -153,7 +189,7 @@ __global__ void __launch_bounds__(TILE, 3) k_cg_f64(const CGP P) {
                 st_d(P.t, V, q.x, g5dw_at<double>(SpD{P.x, V}, L, q, m2));
             }
         }
-        if (!reduce_sync<1>(gs, v, P.part, P.ctl->red, smem)) goto done;
+        if (!reduce_sync<1, RS>(gs, v, P.part, P.ctl->red, smem)) goto done;
         bb = v[0];
     }
     if (bb == 0.0) {   // zero source: zero solution
@@ -175,7 +211,7 @@ __global__ void __launch_bounds__(TILE, 3) k_cg_f64(const CGP P) {
                 st_d(P.r, V, q.x, r);
                 v[0] += norm2(r.a) + norm2(r.b);
             }
-            if (!reduce_sync<1>(gs, v, P.part, P.ctl->red, smem)) goto done;
+            if (!reduce_sync<1, RS>(gs, v, P.part, P.ctl->red, smem)) goto done;
             rr = v[0];
             if (rr < tol) { conv = true; goto epilogue; }
         } else {
@@ -194,7 +230,7 @@ __global__ void __launch_bounds__(TILE, 3) k_cg_f64(const CGP P) {
                 st_d(P.t, V, q.x, tt);
                 v[0] += norm2(tt.a) + norm2(tt.b) + mu2 * (norm2(c.a) + norm2(c.b));
             }
-            if (!reduce_sync<1>(gs, v, P.part, P.ctl->red, smem)) goto done;
+            if (!reduce_sync<1, RS>(gs, v, P.part, P.ctl->red, smem)) goto done;
             const double alpha = rr / v[0];
             v[0] = 0.0;
             FOR_TILES(q) {
@@ -209,7 +245,7 @@ __global__ void __launch_bounds__(TILE, 3) k_cg_f64(const CGP P) {
                 st_d(P.r, V, q.x, r);
                 v[0] += norm2(r.a) + norm2(r.b);
             }
-            if (!reduce_sync<1>(gs, v, P.part, P.ctl->red, smem)) goto done;
+            if (!reduce_sync<1, RS>(gs, v, P.part, P.ctl->red, smem)) goto done;
             const double rn = v[0];
             if (rn < tol) { rr = rn; conv = true; break; }
             beta = rn / rr;
@@ -225,6 +261,7 @@ done:
 
 // ---------------------------------------------------------------------------
 // mixed FP32/FP64 reliable-update CG
+template <int RS>
 __global__ void __launch_bounds__(TILE, 4) k_cg_mixed(const CGP P) {
     __shared__ double smem[32 * 2];
     GridSync gs{&P.ctl->bar, &P.ctl->gen, &P.ctl->err};
@@ -247,7 +284,7 @@ __global__ void __launch_bounds__(TILE, 4) k_cg_mixed(const CGP P) {
             if (!P.guess) st_d(P.x, V, q.x, Pair<double>{make_double2(0, 0), make_double2(0, 0)});
             else st_d(t64, V, q.x, g5dw_at<double>(SpD{P.x, V}, L, q, m2));
         }
-        if (!reduce_sync<1>(gs, v, P.part, P.ctl->red, smem)) goto done;
+        if (!reduce_sync<1, RS>(gs, v, P.part, P.ctl->red, smem)) goto done;
         bb = v[0];
     }
     if (bb == 0.0) {
@@ -271,7 +308,7 @@ __global__ void __launch_bounds__(TILE, 4) k_cg_mixed(const CGP P) {
                 st_d(P.r, V, q.x, r);
                 v[0] += norm2(r.a) + norm2(r.b);
             }
-            if (!reduce_sync<1>(gs, v, P.part, P.ctl->red, smem)) goto done;
+            if (!reduce_sync<1, RS>(gs, v, P.part, P.ctl->red, smem)) goto done;
             rr64 = v[0];
             if (rr64 < tol) { conv = true; goto done; }
         } else {
@@ -289,7 +326,7 @@ __global__ void __launch_bounds__(TILE, 4) k_cg_mixed(const CGP P) {
                 st_f(P.x32, q.x, Pair<float>{make_float2(0, 0), make_float2(0, 0)});
                 v[0] += (double)norm2(r32.a) + (double)norm2(r32.b);
             }
-            if (!reduce_sync<1>(gs, v, P.part, P.ctl->red, smem)) goto done;
+            if (!reduce_sync<1, RS>(gs, v, P.part, P.ctl->red, smem)) goto done;
             rr = v[0];
         }
         double maxrr = rr, beta = 0.0;
@@ -309,7 +346,7 @@ __global__ void __launch_bounds__(TILE, 4) k_cg_mixed(const CGP P) {
                 fc += norm2(c.a) + norm2(c.b);
             }
             double v[1] = {(double)ft + mu2 * (double)fc};
-            if (!reduce_sync<1>(gs, v, P.part, P.ctl->red, smem)) goto done;
+            if (!reduce_sync<1, RS>(gs, v, P.part, P.ctl->red, smem)) goto done;
             const float alpha = (float)(rr / v[0]);
             float fr = 0.f;
             FOR_TILES(q) {
@@ -325,7 +362,7 @@ __global__ void __launch_bounds__(TILE, 4) k_cg_mixed(const CGP P) {
                 fr += norm2(r.a) + norm2(r.b);
             }
             v[0] = (double)fr;
-            if (!reduce_sync<1>(gs, v, P.part, P.ctl->red, smem)) goto done;
+            if (!reduce_sync<1, RS>(gs, v, P.part, P.ctl->red, smem)) goto done;
             const double rn = v[0];
             maxrr = fmax(maxrr, rn);
             const bool cand = rn < tol * s * s;
@@ -354,7 +391,7 @@ __global__ void __launch_bounds__(TILE, 4) k_cg_mixed(const CGP P) {
                     st_d(P.r, V, q.x, r);
                     w[0] += norm2(r.a) + norm2(r.b);
                 }
-                if (!reduce_sync<1>(gs, w, P.part, P.ctl->red, smem)) goto done;
+                if (!reduce_sync<1, RS>(gs, w, P.part, P.ctl->red, smem)) goto done;
                 const double rrt = w[0];
                 rr64 = rrt;
                 if (rrt < tol) { conv = true; break; }
@@ -366,7 +403,7 @@ __global__ void __launch_bounds__(TILE, 4) k_cg_mixed(const CGP P) {
                     st_f(P.r32, q.x, r32);
                     w[0] += (double)(norm2(r32.a) + norm2(r32.b));
                 }
-                if (!reduce_sync<1>(gs, w, P.part, P.ctl->red, smem)) goto done;
+                if (!reduce_sync<1, RS>(gs, w, P.part, P.ctl->red, smem)) goto done;
                 beta = (rrt * s * s / rr) * (s_new / s);
                 s = s_new;
                 rr = w[0];
@@ -418,6 +455,7 @@ struct MSP {
 };
 
 __global__ void __launch_bounds__(TILE, 3) k_cg_multishift(const MSP P) {
+    constexpr int RS = 1;   // latency-bound at the RHMC sizes: every block sums
     __shared__ double smem[32 * 2];
     __shared__ double z[kMaxShifts], zp[kMaxShifts], ai[kMaxShifts], bi[kMaxShifts];
     __shared__ int upd[kMaxShifts], act[kMaxShifts];
@@ -441,7 +479,7 @@ __global__ void __launch_bounds__(TILE, 3) k_cg_multishift(const MSP P) {
             st_d(P.r, V, q.x, bv);
             for (int i = 0; i < P.n; i++) st_d(P.x[i], V, q.x, Pair<double>{make_double2(0, 0), make_double2(0, 0)});
         }
-        if (!reduce_sync<1>(gs, v, P.part, P.ctl->red, smem)) goto done;
+        if (!reduce_sync<1, RS>(gs, v, P.part, P.ctl->red, smem)) goto done;
         bb = v[0];
     }
     if (bb == 0.0) { conv = true; goto done; }
@@ -480,7 +518,7 @@ __global__ void __launch_bounds__(TILE, 3) k_cg_multishift(const MSP P) {
                     }
                 }
             }
-            if (!reduce_sync<1>(gs, v, P.part, P.ctl->red, smem)) goto done;
+            if (!reduce_sync<1, RS>(gs, v, P.part, P.ctl->red, smem)) goto done;
             const double alpha = rr / v[0];
             v[0] = 0.0;
             FOR_TILES(q) {
@@ -495,7 +533,7 @@ __global__ void __launch_bounds__(TILE, 3) k_cg_multishift(const MSP P) {
                 st_d(P.r, V, q.x, r);
                 v[0] += norm2(r.a) + norm2(r.b);
             }
-            if (!reduce_sync<1>(gs, v, P.part, P.ctl->red, smem)) goto done;
+            if (!reduce_sync<1, RS>(gs, v, P.part, P.ctl->red, smem)) goto done;
             const double rn = v[0];
             const double beta_new = rn / rr;
             // shift scalars (identical in every block)
@@ -593,6 +631,74 @@ static int launch_coop(Ctx& c, K kernel, Par P) {
 
 static int solve_plain(Ctx& c, const SolveArgs& a);
 
+// Schedule tuning.  The two reduction schedules of reduce_sync give the same
+// bits, so the choice changes only the time.  The first solve of each
+// precision on a context times both on the caller's operator and source,
+// capped at kTuneIters iterations, into scratch outputs, and keeps the faster;
+// the device control block is saved before and restored after, so counters and
+// status are those of the caller's solves alone.  With QED2D_TUNE=0 in the
+// environment the choice is the size rule measured on B200 instead: every
+// block sums (RS = 1) up to 2^20 sites, the last block publishes beyond.
+constexpr int kTuneIters = 24;
+
+bool tuning_enabled() {
+    const char* e = std::getenv("QED2D_TUNE");
+    return !(e && e[0] == '0');
+}
+
+template <class Launch>
+static int time_schedules(Ctx& c, Launch launch, int* best) {
+    cudaEvent_t e0, e1;
+    QCHECK(cudaEventCreate(&e0));
+    QCHECK(cudaEventCreate(&e1));
+    float tbest[2] = {1e30f, 1e30f};
+    int st = QED2D_OK;
+    for (int rep = 0; rep < 3 && st == QED2D_OK; rep++)
+        for (int rs = 0; rs < 2 && st == QED2D_OK; rs++) {
+            cudaEventRecord(e0, c.stream);
+            st = launch(rs);
+            cudaEventRecord(e1, c.stream);
+            if (cudaEventSynchronize(e1) != cudaSuccess) st = cuda_status(cudaGetLastError(), "schedule tuning");
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep > 0) tbest[rs] = std::min(tbest[rs], ms);   // the first round warms up
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *best = tbest[1] <= tbest[0] ? 1 : 0;
+    return st;
+}
+
+static int tune_cg(Ctx& c, const CGP& P, int slot) {
+    if (!tuning_enabled()) {
+        c.sched[slot] = c.g.V <= (1LL << 20) ? 1 : 0;
+        return QED2D_OK;
+    }
+    DevCtl saved;
+    QCHECK(cudaMemcpyAsync(&saved, c.ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, c.stream));
+    QCHECK(cudaStreamSynchronize(c.stream));
+    CGP T = P;
+    T.x = c.spinor("tune_x");
+    if (T.g5x) T.g5x = c.spinor("tune_g5x");
+    if (!T.x || (P.g5x && !T.g5x)) return QED2D_ERR_NO_MEMORY;
+    T.maxiter = std::min(P.maxiter, kTuneIters);
+    const size_t fb = sizeof(double2) * 2 * (size_t)c.g.V;
+    int best = 1;
+    const int st = time_schedules(
+        c,
+        [&](int rs) -> int {
+            if (P.guess) QCHECK(cudaMemcpyAsync(T.x, P.x, fb, cudaMemcpyDeviceToDevice, c.stream));
+            if (slot == 0) return launch_coop(c, rs ? k_cg_f64<1> : k_cg_f64<0>, T);
+            return launch_coop(c, rs ? k_cg_mixed<1> : k_cg_mixed<0>, T);
+        },
+        &best);
+    QCHECK(cudaMemcpyAsync(c.ctl, &saved, sizeof(DevCtl), cudaMemcpyHostToDevice, c.stream));
+    QCHECK(cudaStreamSynchronize(c.stream));
+    if (st != QED2D_OK) return st;
+    c.sched[slot] = best;
+    return QED2D_OK;
+}
+
 int cg_solve(Ctx& c, const SolveArgs& a, int precision) {
     if (precision == QED2D_PREC_PLAIN) return solve_plain(c, a);
     CGP P{};
@@ -614,7 +720,8 @@ int cg_solve(Ctx& c, const SolveArgs& a, int precision) {
     if (precision == QED2D_PREC_F64) {
         P.p0 = c.spinor("cg_p0");
         P.p1 = c.spinor("cg_p1");
-        return launch_coop(c, k_cg_f64, P);
+        if (c.sched[0] < 0) QTRY(tune_cg(c, P, 0));
+        return launch_coop(c, c.sched[0] ? k_cg_f64<1> : k_cg_f64<0>, P);
     }
     P.r32 = c.spinor32("cg_r32");
     P.q0 = c.spinor32("cg_q0");
@@ -628,7 +735,8 @@ int cg_solve(Ctx& c, const SolveArgs& a, int precision) {
         QTRY(launch_pack_links(c, u32, a.U));
         P.U32 = u32;
     }
-    return launch_coop(c, k_cg_mixed, P);
+    if (c.sched[1] < 0) QTRY(tune_cg(c, P, 1));
+    return launch_coop(c, c.sched[1] ? k_cg_mixed<1> : k_cg_mixed<0>, P);
 }
 
 int multishift_solve(Ctx& c, const double2* U, const double2* b, double2* const* x, const double* mu2, int n,
@@ -880,7 +988,7 @@ extern "C" int qed2d_cg_noalloc(int L1, int L2, double* so, const double* U, con
     int dev = 0, sms = 0, per_sm = 0;
     QCHECK(cudaGetDevice(&dev));
     QCHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_f64, TILE, 0));
+    QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_f64<0>, TILE, 0));
     if (per_sm < 1) return QED2D_ERR_UNSUPPORTED;
     long long grid = (long long)per_sm * sms;
     if (grid > kMaxPartBlocks) grid = kMaxPartBlocks;
@@ -891,7 +999,7 @@ extern "C" int qed2d_cg_noalloc(int L1, int L2, double* so, const double* U, con
 
     QCHECK(cudaMemsetAsync(ctl, 0, sizeof(DevCtl), s));
     void* args[] = {(void*)&P};
-    QCHECK(cudaLaunchCooperativeKernel((const void*)k_cg_f64, dim3((unsigned)grid), dim3(TILE), args, 0, s));
+    QCHECK(cudaLaunchCooperativeKernel((const void*)k_cg_f64<0>, dim3((unsigned)grid), dim3(TILE), args, 0, s));
     count_launch();
     DevCtl h;
     QCHECK(cudaMemcpyAsync(&h, ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, s));

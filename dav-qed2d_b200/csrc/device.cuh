@@ -158,28 +158,41 @@ struct GridSync {
         __threadfence();
         st_release_u64(gen, target);
     }
-    // Wait for the release (thread 0 of the other blocks), bounded.
-    __device__ __forceinline__ void wait() {
+    // Wait for the release (thread 0 of the other blocks), bounded.  Returns
+    // false when the wait ended on the error flag or timed out.
+    __device__ __forceinline__ bool wait() {
         unsigned long long polls = 0;
+        bool ok = true;
         while (ld_acquire_u64(gen) < target) {
-            if (ld_volatile_int(err) != 0) break;
+            if (ld_volatile_int(err) != 0) {
+                ok = false;
+                break;
+            }
             if (++polls > (1ULL << 26)) {
                 atomicExch(err, 2 /* QED2D_ERR_TIMEOUT */);
+                ok = false;
                 break;
             }
             __nanosleep(32);
         }
         __threadfence();
+        return ok;
     }
+    // Plain grid barrier; false in a block whose wait failed (the error is
+    // passed on through shared memory, so no block reads the flag again).
     __device__ __forceinline__ bool sync() {
-        __shared__ int s_last;
+        __shared__ int s_last, s_ok;
         const bool last = arrive(&s_last);
         if (threadIdx.x == 0) {
-            if (last) release();
-            else wait();
+            if (last) {
+                release();
+                s_ok = 1;
+            } else {
+                s_ok = wait();
+            }
         }
         __syncthreads();
-        return ld_volatile_int(err) == 0;
+        return s_ok != 0;
     }
 };
 

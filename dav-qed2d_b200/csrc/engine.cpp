@@ -403,6 +403,21 @@ int qed2d_ctx_get_dims(const qed2d_ctx* ctx, int* L1, int* L2) {
     return QED2D_OK;
 }
 
+int qed2d_ctx_set_schedule(qed2d_ctx* ctx, int precision, int schedule) {
+    QCTX(ctx);
+    if (precision != QED2D_PREC_F64 && precision != QED2D_PREC_MIXED) return bad_arg("schedule: F64 or MIXED only");
+    if (schedule < -1 || schedule > 1) return bad_arg("schedule must be -1, 0 or 1");
+    c.sched[precision == QED2D_PREC_F64 ? 0 : 1] = schedule;
+    return QED2D_OK;
+}
+
+int qed2d_ctx_get_schedule(const qed2d_ctx* ctx, int precision, int* schedule) {
+    if (!ctx || !schedule) return bad_arg("context or schedule is NULL");
+    if (precision != QED2D_PREC_F64 && precision != QED2D_PREC_MIXED) return bad_arg("schedule: F64 or MIXED only");
+    *schedule = ctx->c.sched[precision == QED2D_PREC_F64 ? 0 : 1];
+    return QED2D_OK;
+}
+
 int qed2d_last_solve(const qed2d_ctx* ctx, int64_t* iterations, double* rel, int64_t* reliable_updates) {
     if (!ctx) return bad_arg("context is NULL");
     if (iterations) *iterations = ctx->c.last_iters;

@@ -38,7 +38,7 @@ __all__ = [
     "gamm5Dw", "gamm5Dw_sqr", "gamm5Dw_sqr_msq", "tr_dQwdU", "gamm5Dw_sqr_musq", "gamm5Dw_sqr_sqr_musq",
     "gamm5Dw_sqr_sqr", "gamm5", "Dw", "CG", "save_gauge", "load_gauge", "get_rhmc_params", "power_method",
     "reweighting_factor", "R", "MultiCG", "generate_pseudofermion_", "plwv", "LuscherZ",
-    "seed", "set_precision", "Qed2dError", "cfield", "rfield", "context",
+    "seed", "set_precision", "set_schedule", "get_schedule", "Qed2dError", "cfield", "rfield", "context",
 ]
 
 
@@ -289,6 +289,23 @@ def CG(so, U, si, am0, *args, so_as_guess=False):
         check(st, "CG")
         return it.value
     raise TypeError("CG: unsupported argument list")
+
+
+_PRECS = {"f64": _lib.PREC_F64, "mixed": _lib.PREC_MIXED}
+
+
+def set_schedule(prm: LattParm, schedule: int, precision="mixed") -> None:
+    """Fix the persistent solver's reduction schedule on this lattice's context:
+    0 (last block publishes the sums) or 1 (every block sums), or -1 to tune
+    again on the next solve.  Both schedules give the same bits."""
+    check(lib().qed2d_ctx_set_schedule(_c(prm), _PRECS[precision], int(schedule)), "set_schedule")
+
+
+def get_schedule(prm: LattParm, precision="mixed") -> int:
+    """The solver's reduction schedule on this lattice (-1 until the first solve tunes it)."""
+    v = C.c_int(0)
+    check(lib().qed2d_ctx_get_schedule(_c(prm), _PRECS[precision], C.byref(v)), "get_schedule")
+    return v.value
 
 
 def last_solve(prm: LattParm):
@@ -603,6 +620,18 @@ class Batch:
     @classmethod
     def ragged(cls, sizes, beta):
         return cls(None, None, None, beta, _sizes=[(int(a), int(b)) for a, b in sizes])
+
+    @property
+    def schedule(self) -> int:
+        """Reduction schedule of the batched solver: -1 untuned, 0/1 (equal-size
+        batches of at most 64 replicas), 2 (ragged solver)."""
+        v = C.c_int(0)
+        check(lib().qed2d_batch_get_schedule(self.h, C.byref(v)), "batch_get_schedule")
+        return v.value
+
+    @schedule.setter
+    def schedule(self, s: int) -> None:
+        check(lib().qed2d_batch_set_schedule(self.h, int(s)), "batch_set_schedule")
 
     def field(self, dtype=torch.complex128):
         if self.uniform:

@@ -46,6 +46,8 @@ SIGNATURES = {
     "qed2d_ctx_set_stream": (I, [P, P]),
     "qed2d_ctx_set_precision": (I, [P, I]),
     "qed2d_ctx_get_dims": (I, [P, PI, PI]),
+    "qed2d_ctx_set_schedule": (I, [P, I, I]),
+    "qed2d_ctx_get_schedule": (I, [P, I, PI]),
     "qed2d_last_solve": (I, [P, PI64, PD, PI64]),
     "qed2d_status_string": (C.c_char_p, [I]),
     "qed2d_last_error": (C.c_char_p, []),
@@ -94,6 +96,8 @@ SIGNATURES = {
     "qed2d_batch_create": (I, [I, I, I, PD, C.POINTER(C.c_void_p)]),
     "qed2d_batch_create_ragged": (I, [I, PI, PI, PD, C.POINTER(C.c_void_p)]),
     "qed2d_batch_layout": (I, [P, C.POINTER(C.c_int64)]),
+    "qed2d_batch_set_schedule": (I, [P, I]),
+    "qed2d_batch_get_schedule": (I, [P, PI]),
     "qed2d_batch_destroy": (I, [P]),
     "qed2d_batch_set_stream": (I, [P, P]),
     "qed2d_batch_cg": (I, [P, P, P, P, PD, I, D, PI, PI]),

@@ -100,6 +100,14 @@ int qed2d_ctx_set_beta(qed2d_ctx* ctx, double beta);
 int qed2d_ctx_set_stream(qed2d_ctx* ctx, void* cuda_stream);
 int qed2d_ctx_set_precision(qed2d_ctx* ctx, int precision);
 int qed2d_ctx_get_dims(const qed2d_ctx* ctx, int* L1, int* L2);
+/* Reduction schedule of the persistent F64 / MIXED solvers: 0 = the last block
+ * to reach a grid barrier sums the partials and publishes them, 1 = every block
+ * sums them itself.  Both give the same bits; the first solve of each precision
+ * on a context times both and keeps the faster (a host synchronisation; set
+ * QED2D_TUNE=0 in the environment for a fixed size rule instead).  set: 0 or 1
+ * to fix it, -1 to tune again on the next solve; get: -1 while untuned. */
+int qed2d_ctx_set_schedule(qed2d_ctx* ctx, int precision, int schedule);
+int qed2d_ctx_get_schedule(const qed2d_ctx* ctx, int precision, int* schedule);
 /* iterations, final |r|^2/|b|^2 and (QED2D_PREC_MIXED) FP64 reliable updates of
  * the most recent solve on this context; any pointer may be NULL */
 int qed2d_last_solve(const qed2d_ctx* ctx, int64_t* iterations, double* rel_residual_sq,
@@ -260,6 +268,10 @@ int qed2d_batch_create_ragged(int nrep, const int* L1, const int* L2, const doub
 int qed2d_batch_layout(const qed2d_batch* batch, int64_t* site_offsets);
 int qed2d_batch_destroy(qed2d_batch* batch);
 int qed2d_batch_set_stream(qed2d_batch* batch, void* cuda_stream);
+/* the batched solver's reduction schedule, as qed2d_ctx_set_schedule (equal-size
+ * batches of at most 64 replicas; get reports 2 for the ragged solver) */
+int qed2d_batch_set_schedule(qed2d_batch* batch, int schedule);
+int qed2d_batch_get_schedule(const qed2d_batch* batch, int* schedule);
 /* every replica's CG method 1 (src/QED2dSolver.jl:3-46) in one launch:
  * x_r = ((g5Dw)^2)^-1 b_r with mass am0[r]; iterations[nrep] and updates[nrep]
  * (FP64 reliable updates) may be NULL */

@@ -179,3 +179,27 @@ def test_many_replicas_global_state_cg():
                  qed2d.gamm5Dw_sqr_msq, prm, None)
         assert rel(to_host(b.replica(x, r)), to_host(xs)) < 1e-9, r
     qed2d.set_precision("f64")
+
+
+def test_batch_reduction_schedules_give_identical_bits():
+    """Equal-size batches: both reduction schedules of the batched solver give
+    bitwise identical solutions; the first solve tunes the schedule."""
+    import qed2d
+    nrep, L1, L2 = 3, 64, 48
+    b = qed2d.Batch(nrep, L1, L2, 4.0)
+    assert b.schedule == -1
+    U, src = b.field(), b.field()
+    for r in range(nrep):
+        U[r] = to_dev(hot_links(L1, L2, 40 + r))
+        src[r] = to_dev(cgauss(L1, L2, 50 + r, 2))
+    x = b.field()
+    b.cg(x, U, src, [0.2, 0.3, 0.25], 20000, 1e-24)
+    assert b.schedule in (0, 1)
+    res = []
+    for sched in (0, 1):
+        b.schedule = sched
+        x = b.field()
+        its, _ = b.cg(x, U, src, [0.2, 0.3, 0.25], 20000, 1e-24)
+        res.append((its, to_host(x)))
+    assert res[0][0] == res[1][0] and np.array_equal(res[0][1], res[1][1])
+    assert qed2d.Batch.ragged([(16, 16), (32, 8)], [4.0, 4.0]).schedule == 2

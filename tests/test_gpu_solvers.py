@@ -211,3 +211,32 @@ def test_persistent_solver_deterministic(q, prec, L1, L2):
         assert it == ref_it
         assert torch.equal(x, ref)
     q.set_precision("f64")
+
+
+@pytest.mark.parametrize("L", [64, 256])
+@pytest.mark.parametrize("prec", ["f64", "mixed"])
+def test_reduction_schedules_give_identical_bits(L, prec):
+    """The two grid-reduction schedules of the persistent solvers (last block
+    publishes / every block sums) perform the same additions in the same order:
+    solutions and iteration counts are bitwise identical, so the tuner's choice
+    never changes a result.  The first solve tunes the schedule (0 or 1)."""
+    import qed2d
+    prm = qed2d.LattParm((L, L), 4.0)
+    U, src = to_dev(hot_links(L, L, 5)), to_dev(cgauss(L, L, 6, 2))
+    qed2d.set_precision(prec)
+    try:
+        qed2d.set_schedule(prm, -1, prec)
+        x = qed2d.cfield(L, L)
+        qed2d.CG(x, U, src, 0.2, 20000, 1e-24, qed2d.gamm5Dw_sqr_msq, prm, None)
+        assert qed2d.get_schedule(prm, prec) in (0, 1)
+        out = []
+        for sched in (0, 1):
+            qed2d.set_schedule(prm, sched, prec)
+            x = qed2d.cfield(L, L)
+            it = qed2d.CG(x, U, src, 0.2, 20000, 1e-24, qed2d.gamm5Dw_sqr_msq, prm, None)
+            out.append((it, to_host(x)))
+        assert out[0][0] == out[1][0]
+        assert np.array_equal(out[0][1], out[1][1])
+    finally:
+        qed2d.set_schedule(prm, -1, prec)
+        qed2d.set_precision("f64")
