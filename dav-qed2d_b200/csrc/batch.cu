@@ -239,7 +239,7 @@ struct SegDesc {
 };
 
 struct RCGP {
-    int nrep, lg;         // lg: log2 of the lanes summing one replica's partials
+    int nrep;
     const RepInfo* reps;
     const SegDesc* segs;  // segments, block after block
     const int* seg0;      // [grid+1] segments of block b: seg0[b] .. seg0[b+1]-1
@@ -256,7 +256,9 @@ struct RCGP {
     int maxiter;
     RepState* st;   // [nrep] (final state in both modes)
     int* flags;     // [FL_N] (global-state mode)
-    double* red;    // [nrep] per-replica sums (shared-state mode)
+    int* flag_acc;  // OR of the flags raised by the replicas finished at a barrier (global-state mode)
+    int* cnt;       // [nrep] segments of each replica reduced so far at the current barrier
+    double* red;    // [2][nrep] per-replica sums (shared-state mode, alternating)
     double* part;   // one partial per segment
     DevCtl* ctl;
 };
@@ -383,6 +385,7 @@ struct SegInfo {
     SegDesc d;
     RepInfo R;
     double m2;
+    int rs0, rs1;   // the replica's partial slots
 };
 // per-block shared scratch of a phase: the segments' scalars and per-warp partials
 struct PhaseScratch {
@@ -401,6 +404,8 @@ __device__ __forceinline__ void block_ctx_init(const RCGP& P, BlockCtx& bc, SegI
         seg[i].d = d;
         seg[i].R = P.reps[d.r];
         seg[i].m2 = P.m2[d.r];
+        seg[i].rs0 = P.rep_seg[d.r];
+        seg[i].rs1 = P.rep_seg[d.r + 1];
     }
     __syncthreads();
 }
@@ -441,7 +446,10 @@ __device__ __forceinline__ void run_phase(const RCGP& P, const StateView<SH>& sv
             } else {
                 double red[1] = {(double)acc};
                 block_sum<1>(red, smem);
-                if (threadIdx.x == 0) P.part[d.slot] = red[0];
+                if (threadIdx.x == 0) {
+                    P.part[d.slot] = red[0];
+                    __threadfence();
+                }
             }
         }
     }
@@ -539,68 +547,119 @@ __device__ __forceinline__ void clear_flags(int kind, int* fl) {
     if (kind == RED_TRUE) fl[FL_R4] = 0;
 }
 
-// The last block's part of a barrier: per-replica sums of the segments (2^lg
-// lanes per replica, fixed order); SH publishes them, otherwise the records and
-// flags are updated here.
+// Per-replica completion at a barrier, before the block arrives: each segment
+// of this block counts itself into its replica's counter; the block whose
+// segment completes a replica finishes it -- one warp sums the replica's
+// partials (lanes over the slots in a fixed order, then a fixed shuffle tree,
+// so the result does not depend on which block finishes) and either publishes
+// the sum (SH) or runs the replica's recurrences on its global record and ORs
+// the flags it raises into flag_acc.  The per-replica work is thus spread over
+// the blocks instead of serialised in the block that arrives last.
 template <bool SH>
-__device__ __forceinline__ void last_block_sums(const RCGP& P, const int* rseg, int* s_fl, int* s_bits, int kind,
-                                                int k) {
-    const int G = 1 << P.lg, span = P.nrep << P.lg;
-    int fl[FL_N] = {0, 0, 0};
-    for (int base = 0; base < span; base += blockDim.x) {   // same trip count in every thread
-        const int idx = base + threadIdx.x, r = idx >> P.lg, j = idx & (G - 1);
-        RepState st{};
-        if (!SH && idx < span && j == 0) st = ld_state(P.st + r);   // issued before the sums
-        double s = 0.0;
-        if (idx < span)
-            for (int i = rseg[r] + j, e = rseg[r + 1]; i < e; i += G) s += __ldcg(P.part + i);
-        for (int o = G >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (idx < span && j == 0) {
-            if (SH) {
-                P.red[r] = s;
-            } else {
-                rep_step(st, kind, s, k, P.eps, P.delta2, P.maxiter, fl);
-                st_state(P.st + r, st);
-            }
+__device__ __forceinline__ void finish_replica(const RCGP& P, int r, int rs0, int rs1, int kind, int k,
+                                               double* red) {
+    const int lane = threadIdx.x & 31;
+    __threadfence();
+    double s = 0.0;
+    for (int i = rs0 + lane; i < rs1; i += 32) s += __ldcg(P.part + i);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) {
+        if (SH) {
+            red[r] = s;
+        } else {
+            RepState st = ld_state(P.st + r);
+            int fl[FL_N] = {0, 0, 0};
+            rep_step(st, kind, s, k, P.eps, P.delta2, P.maxiter, fl);
+            st_state(P.st + r, st);
+            const int bits = fl[FL_ACT] | fl[FL_UPD] << 1 | fl[FL_R4] << 2;
+            if (bits) atomicOr(P.flag_acc, bits);
         }
-    }
-    if (!SH) {
-        const int bits = __reduce_or_sync(0xffffffffu, fl[FL_ACT] | fl[FL_UPD] << 1 | fl[FL_R4] << 2);
-        if ((threadIdx.x & 31) == 0 && bits) atomicOr(s_bits, bits);
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int g[FL_N] = {s_fl[FL_ACT], s_fl[FL_UPD], s_fl[FL_R4]};
-            clear_flags(kind, g);
-            g[FL_ACT] |= *s_bits & 1;
-            g[FL_UPD] |= (*s_bits >> 1) & 1;
-            g[FL_R4] |= (*s_bits >> 2) & 1;
-            for (int i = 0; i < FL_N; i++) {
-                s_fl[i] = g[i];
-                P.flags[i] = g[i];
-            }
-        }
+        __threadfence();
     }
 }
 
-// Grid barrier with per-replica sums (2^lg lanes per replica, fixed order).
-// SH: the last block publishes the sums and every block updates its shared
-// records; otherwise the last block updates the global records and flags.
-// s_fl (shared) holds the flags afterwards in every block.
 template <bool SH>
-__device__ __forceinline__ bool rbarrier(GridSync& gs, const RCGP& P, RepState* s_st, int* s_fl, const int* s_rseg,
-                                         int kind, int k) {
+__device__ __forceinline__ void complete_replicas(const RCGP& P, const BlockCtx& bcs, const SegInfo* segs, int kind,
+                                                  int k, double* red) {
+    __shared__ int s_ntask, s_task[kSegCache][3];
+    if (threadIdx.x == 0) s_ntask = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < bcs.nsb; i += blockDim.x) {
+        int r, rs0, rs1;
+        if (i < kSegCache) {
+            r = segs[i].d.r;
+            rs0 = segs[i].rs0;
+            rs1 = segs[i].rs1;
+        } else {
+            r = P.segs[bcs.seg + i].r;
+            rs0 = __ldg(P.rep_seg + r);
+            rs1 = __ldg(P.rep_seg + r + 1);
+        }
+        if (atomicAdd(P.cnt + r, 1) == rs1 - rs0 - 1) {   // this block completes replica r
+            P.cnt[r] = 0;
+            const int t = atomicAdd(&s_ntask, 1);
+            if (t < kSegCache) {
+                s_task[t][0] = r;
+                s_task[t][1] = rs0;
+                s_task[t][2] = rs1;
+            } else {   // more completions than task slots: this thread finishes it alone
+                __threadfence();
+                double s = 0.0;
+                for (int j = rs0; j < rs1; j++) s += __ldcg(P.part + j);
+                if (SH) {
+                    red[r] = s;
+                } else {
+                    RepState st = ld_state(P.st + r);
+                    int fl[FL_N] = {0, 0, 0};
+                    rep_step(st, kind, s, k, P.eps, P.delta2, P.maxiter, fl);
+                    st_state(P.st + r, st);
+                    const int bits = fl[FL_ACT] | fl[FL_UPD] << 1 | fl[FL_R4] << 2;
+                    if (bits) atomicOr(P.flag_acc, bits);
+                }
+                __threadfence();
+            }
+        }
+    }
+    __syncthreads();
+    const int nt = min(s_ntask, kSegCache), warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int t = warp; t < nt; t += nw) finish_replica<SH>(P, s_task[t][0], s_task[t][1], s_task[t][2], kind, k, red);
+}
+
+// Grid barrier after a reduction: the replicas are completed by the blocks
+// (complete_replicas), the last block to arrive merges the flags (global
+// records) and releases; with shared records every block then runs every
+// replica's recurrences on the published sums.  s_fl (shared) holds the flags
+// afterwards in every block.
+template <bool SH>
+__device__ __forceinline__ bool rbarrier(GridSync& gs, const RCGP& P, RepState* s_st, int* s_fl, const BlockCtx& bcs,
+                                         const SegInfo* segs, int kind, int k) {
     __shared__ int s_last, s_bits;
+    double* red = P.red + (size_t)(gs.nred++ & 1) * P.nrep;   // alternate: a slow block may still read the last
+    complete_replicas<SH>(P, bcs, segs, kind, k, red);
     if (threadIdx.x == 0) s_bits = 0;   // arrive() begins with __syncthreads
     const bool last = gs.arrive(&s_last);
-    if (last) {
-        __threadfence();
-        last_block_sums<SH>(P, SH ? s_rseg : P.rep_seg, s_fl, &s_bits, kind, k);
-        __syncthreads();
-        if (threadIdx.x == 0) gs.release();
-    } else if (threadIdx.x == 0) {
-        gs.wait();
-        if (!SH)
-            for (int i = 0; i < FL_N; i++) s_fl[i] = __ldcg(P.flags + i);
+    if (threadIdx.x == 0) {
+        if (last) {
+            if (!SH) {
+                __threadfence();
+                const int bits = atomicExch(P.flag_acc, 0);
+                int g[FL_N] = {s_fl[FL_ACT], s_fl[FL_UPD], s_fl[FL_R4]};
+                clear_flags(kind, g);
+                g[FL_ACT] |= bits & 1;
+                g[FL_UPD] |= (bits >> 1) & 1;
+                g[FL_R4] |= (bits >> 2) & 1;
+                for (int i = 0; i < FL_N; i++) {
+                    s_fl[i] = g[i];
+                    P.flags[i] = g[i];
+                }
+            }
+            gs.release();
+        } else {
+            gs.wait();
+            if (!SH)
+                for (int i = 0; i < FL_N; i++) s_fl[i] = __ldcg(P.flags + i);
+        }
     }
     __syncthreads();
     if (SH) {   // every block: the recurrences of every replica on the published sums
@@ -608,7 +667,7 @@ __device__ __forceinline__ bool rbarrier(GridSync& gs, const RCGP& P, RepState* 
         if (threadIdx.x < P.nrep) {   // nrep <= kSharedReps <= blockDim.x
             const int r = threadIdx.x;
             RepState st = s_st[r];
-            rep_step(st, kind, __ldcg(P.red + r), k, P.eps, P.delta2, P.maxiter, fl);
+            rep_step(st, kind, __ldcg(red + r), k, P.eps, P.delta2, P.maxiter, fl);
             s_st[r] = st;
         }
         const int bits = __reduce_or_sync(0xffffffffu, fl[FL_ACT] | fl[FL_UPD] << 1 | fl[FL_R4] << 2);
@@ -628,29 +687,29 @@ __device__ __forceinline__ bool rbarrier(GridSync& gs, const RCGP& P, RepState* 
 // the solve; false when a barrier gave up
 template <bool SH>
 __device__ __forceinline__ bool r_body(const RCGP& P, GridSync& gs, int& k, double* smem, RepState* s_st, int* s_fl,
-                                       const int* s_rseg, const BlockCtx& bc, const SegInfo* segs, PhaseScratch& ps) {
+                                       const BlockCtx& bc, const SegInfo* segs, PhaseScratch& ps) {
     const StateView<SH> sv{s_st, P.st};
     int cur = 0;
     run_phase<PH_SETUP, SH>(P, sv, cur, bc, segs, ps, smem);
-    if (!rbarrier<SH>(gs, P, s_st, s_fl, s_rseg, RED_BB, 0)) return false;
+    if (!rbarrier<SH>(gs, P, s_st, s_fl, bc, segs, RED_BB, 0)) return false;
     run_phase<PH_START, SH>(P, sv, cur, bc, segs, ps, smem);
-    if (!rbarrier<SH>(gs, P, s_st, s_fl, s_rseg, RED_RR0, 0)) return false;
+    if (!rbarrier<SH>(gs, P, s_st, s_fl, bc, segs, RED_RR0, 0)) return false;
     for (k = 1; k <= P.maxiter; k++) {
         if (!s_fl[FL_ACT]) break;
         run_phase<PH_A, SH>(P, sv, cur, bc, segs, ps, smem);
-        if (!rbarrier<SH>(gs, P, s_st, s_fl, s_rseg, RED_PAP, k)) return false;
+        if (!rbarrier<SH>(gs, P, s_st, s_fl, bc, segs, RED_PAP, k)) return false;
         run_phase<PH_B, SH>(P, sv, cur, bc, segs, ps, smem);
-        if (!rbarrier<SH>(gs, P, s_st, s_fl, s_rseg, RED_RN, k)) return false;
+        if (!rbarrier<SH>(gs, P, s_st, s_fl, bc, segs, RED_RN, k)) return false;
         if (s_fl[FL_UPD]) {
             run_phase<PH_R1, SH>(P, sv, cur, bc, segs, ps, smem);
             if (!gs.sync()) return false;
             run_phase<PH_R2, SH>(P, sv, cur, bc, segs, ps, smem);
             if (!gs.sync()) return false;
             run_phase<PH_R3, SH>(P, sv, cur, bc, segs, ps, smem);
-            if (!rbarrier<SH>(gs, P, s_st, s_fl, s_rseg, RED_TRUE, k)) return false;
+            if (!rbarrier<SH>(gs, P, s_st, s_fl, bc, segs, RED_TRUE, k)) return false;
             if (s_fl[FL_R4]) {
                 run_phase<PH_R4, SH>(P, sv, cur, bc, segs, ps, smem);
-                if (!rbarrier<SH>(gs, P, s_st, s_fl, s_rseg, RED_R4, k)) return false;
+                if (!rbarrier<SH>(gs, P, s_st, s_fl, bc, segs, RED_R4, k)) return false;
             }
         }
         cur ^= 1;
@@ -666,14 +725,11 @@ __global__ void __launch_bounds__(TILE, 4) k_r_cg_mixed(const RCGP P) {
     __shared__ BlockCtx s_bc;
     __shared__ SegInfo s_seg[kSegCache];
     __shared__ PhaseScratch s_ps;
-    __shared__ int s_rseg[SH ? kSharedReps + 1 : 1];   // the replicas' segment ranges (SH)
     if (threadIdx.x < FL_N) s_fl[threadIdx.x] = 0;
-    if (SH)
-        for (int r = threadIdx.x; r <= P.nrep; r += blockDim.x) s_rseg[r] = P.rep_seg[r];
     block_ctx_init(P, s_bc, s_seg);
     GridSync gs{&P.ctl->bar, &P.ctl->gen, &P.ctl->err};
     int k = 0;
-    const bool ok = r_body<SH>(P, gs, k, smem, s_st, s_fl, s_rseg, s_bc, s_seg, s_ps);
+    const bool ok = r_body<SH>(P, gs, k, smem, s_st, s_fl, s_bc, s_seg, s_ps);
     if (blockIdx.x == 0) {
         if (SH && ok)   // every block holds the same records: block 0 stores them
             for (int r = threadIdx.x; r < P.nrep; r += blockDim.x) P.st[r] = s_st[r];
@@ -718,7 +774,7 @@ struct qed2d_batch {
     std::vector<double> beta, m2;
     int device = 0, num_sms = 148;
     cudaStream_t stream = nullptr;
-    int grid = 0, per_block = 0, nseg = 0, lg = 0;   // persistent CG geometry
+    int grid = 0, per_block = 0, nseg = 0;   // persistent CG geometry
     RepInfo* d_reps = nullptr;
     int4* d_tiles = nullptr;
     int* d_seg0 = nullptr;
@@ -731,7 +787,8 @@ struct qed2d_batch {
     uint64_t* d_seed = nullptr;
     RepState* d_st = nullptr;       // [nrep] solver records
     int* d_flags = nullptr;         // [FL_N]
-    double* d_red = nullptr;        // [nrep]
+    double* d_red = nullptr;        // [2][nrep]
+    int* d_cnt = nullptr;           // [nrep + 1]: per-replica counters, then the flag accumulator
     bool shared_state = false;      // records in shared memory (nrep <= kSharedReps)
     bool uniform = false;           // equal sizes, nrep <= kUniformReps: k_u_cg_mixed
     int usched = -1;                // its reduction schedule (-1: not tuned yet)
@@ -844,7 +901,6 @@ int r_solve(qed2d_batch* h, const double2* U, const float4* U32, const double2* 
             int maxiter, double eps) {
     RCGP P{};
     P.nrep = h->nrep;
-    P.lg = h->lg;
     P.reps = h->d_reps;
     P.segs = h->d_segs;
     P.seg0 = h->d_seg0;
@@ -868,6 +924,8 @@ int r_solve(qed2d_batch* h, const double2* U, const float4* U32, const double2* 
     P.st = h->d_st;
     P.flags = h->d_flags;
     P.red = h->d_red;
+    P.cnt = h->d_cnt;
+    P.flag_acc = h->d_cnt + h->nrep;
     P.part = h->d_part;
     P.ctl = h->ctl;
     QCHECK(cudaMemsetAsync(&h->ctl->bar, 0, 2 * sizeof(unsigned long long) + sizeof(int), h->stream));
@@ -910,6 +968,7 @@ int r_solve(qed2d_batch* h, const double2* U, const float4* U32, const double2* 
                                               h->ctl);
         return r_post("k_r_finish");
     } else {
+        QCHECK(cudaMemsetAsync(h->d_cnt, 0, sizeof(int) * (h->nrep + 1), h->stream));   // counters start at zero
         const void* kern = h->shared_state ? (const void*)k_r_cg_mixed<true> : (const void*)k_r_cg_mixed<false>;
         QCHECK(cudaLaunchCooperativeKernel(kern, dim3((unsigned)h->grid), dim3(TILE), args, 0, h->stream));
     }
@@ -1003,22 +1062,10 @@ int batch_setup(qed2d_batch* h, const int* L1, const int* L2, const double* beta
     seg0[h->grid] = (int)segs.size();
     h->nseg = (int)segs.size();
     std::vector<int> rep_seg(B + 1, 0);   // partial slots: replica by replica
-    int maxsegs = 0;
     for (int r = 0, slot = 0; r < B; r++) {
         rep_seg[r] = slot;
         for (int i : rep_segs[r]) segs[i].slot = slot++;
         rep_seg[r + 1] = slot;
-        maxsegs = std::max(maxsegs, (int)rep_segs[r].size());
-    }
-    // lanes per replica in the last block's sums: fewest rounds of loads
-    long long best = -1;
-    for (int lg = 0; lg <= 5; lg++) {
-        const long long G = 1LL << lg;
-        const long long cost = ((B * G + TILE - 1) / TILE) * ((maxsegs + G - 1) / G + 4 + lg);
-        if (best < 0 || cost < best) {
-            best = cost;
-            h->lg = lg;
-        }
     }
     // equal sizes and few replicas: the uniform kernel, whole blocks per replica
     bool same = B <= kUniformReps;
@@ -1058,7 +1105,8 @@ int batch_setup(qed2d_batch* h, const int* L1, const int* L2, const double* beta
     QCHECK(cudaMalloc(&h->d_seed, sizeof(uint64_t) * B));
     QCHECK(cudaMalloc(&h->d_st, sizeof(RepState) * B));
     QCHECK(cudaMalloc(&h->d_flags, sizeof(int) * FL_N));
-    QCHECK(cudaMalloc(&h->d_red, sizeof(double) * B));
+    QCHECK(cudaMalloc(&h->d_red, sizeof(double) * 2 * B));
+    QCHECK(cudaMalloc(&h->d_cnt, sizeof(int) * (B + 1)));
     if (h->uniform) {
         QCHECK(cudaMalloc(&h->d_upart, sizeof(double) * 2 * (size_t)h->ugrid));
         QCHECK(cudaMalloc(&h->d_ured, sizeof(double) * 2 * B));
@@ -1131,7 +1179,7 @@ int qed2d_batch_destroy(qed2d_batch* h) {
     else cudaDeviceSynchronize();
     for (auto& kv : h->ws) cudaFree(kv.second.first);
     void* dev[] = {h->d_reps, h->d_tiles, h->d_seg0, h->d_segs, h->d_rep_seg, h->d_dbase_c, h->d_dbase_r, h->d_m2,
-                   h->d_beta, h->d_seed,  h->d_st, h->d_flags, h->d_red, h->d_upart, h->d_ured,      h->d_out,     h->d_iters,   h->d_sums,
+                   h->d_beta, h->d_seed,  h->d_st, h->d_flags, h->d_red, h->d_cnt, h->d_upart, h->d_ured,      h->d_out,     h->d_iters,   h->d_sums,
                    h->d_tpart, h->d_part, h->ctl};
     for (void* p : dev)
         if (p) cudaFree(p);
