@@ -183,6 +183,72 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
+def run_configs(qed2d, torch, dev):
+    """Trajectories/s of the benchmark configurations on one GPU (timed with
+    CUDA events after warm-up; each a bounded number of trajectories):
+    C1 pure gauge 128^2 (OMF4 ns=10 eps=0.15), C2 Nf=2 64^2 (leapfrog ns=20
+    eps=0.05; mixed, fused FP64 and plain FP64 solvers), C3 Nf=1 RHMC 128^2 with
+    12 Zolotarev poles on the power-method interval (ns=20 eps=0.05), C5 master
+    field pure gauge 8192^2 (OMF4 ns=20 eps=0.025)."""
+    import numpy as np
+
+    def timed(fn, n):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(n):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return n / (e0.elapsed_time(e1) / 1e3)
+
+    out = {}
+    qed2d.seed(SEED)
+    # C1
+    p1 = qed2d.LattParm((128, 128), 11.25)
+    U = torch.from_numpy(hot_start(128, 128, 1234)).to(dev)
+    step = lambda: qed2d.HMC_(U, 0.15, 10, [], p1, None, integrator=qed2d.OMF4())
+    for _ in range(20):
+        step()
+    out["C1_pure_gauge_128_omf4"] = {"value": timed(step, 100), "unit": "traj/s", "trajectories": 100}
+    # C2
+    p2 = qed2d.LattParm((64, 64), 4.0)
+    U2 = torch.from_numpy(hot_start(64, 64, 64)).to(dev)
+    for _ in range(10):
+        qed2d.HMC_(U2, 0.1, 10, [], p2, None)   # pure-gauge thermalisation
+    c2 = {}
+    for prec in ("mixed", "f64", "plain"):
+        qed2d.set_precision(prec)
+        Uc = U2.clone()
+        st = lambda: qed2d.HMC_(Uc, 0.1, 0.05, 20, [], MAXITER, TOL, p2, None)
+        st()
+        c2[prec] = timed(st, 5)
+    qed2d.set_precision("f64")
+    out["C2_nf2_64_leapfrog"] = {"unit": "traj/s", "mixed": c2["mixed"], "f64_fused": c2["f64"], "plain_f64": c2["plain"],
+                                 "mixed_vs_plain": c2["mixed"] / c2["plain"], "trajectories": 5}
+    # C3
+    p3 = qed2d.LattParm((128, 128), 4.0)
+    U3 = torch.from_numpy(hot_start(128, 128, 128)).to(dev)
+    for _ in range(10):
+        qed2d.HMC_(U3, 0.1, 10, [], p3, None)
+    lmin, lmax = qed2d.power_method(U3, 0.1, p3, None, iter=300)
+    rp = [qed2d.get_rhmc_params(12, np.sqrt(0.9 * lmin), np.sqrt(1.1 * lmax))]
+    st3 = lambda: qed2d.HMC_(U3, [0.1], 0.05, 20, [], MAXITER, TOL, p3, None, rp)
+    st3()
+    out["C3_rhmc_128_12_poles"] = {"value": timed(st3, 3), "unit": "traj/s", "solver": "FP64 multi-shift, one launch for all poles",
+                                   "trajectories": 3}
+    del U, U2, U3
+    # C5
+    p5 = qed2d.LattParm((8192, 8192), 11.25)
+    U5 = torch.polar(torch.ones(2, 8192, 8192, dtype=torch.float64, device=dev),
+                     (torch.rand(2, 8192, 8192, dtype=torch.float64, device=dev) * 2 - 1) * np.pi)
+    st5 = lambda: qed2d.HMC_(U5, 0.025, 20, [], p5, None, integrator=qed2d.OMF4())
+    st5()
+    out["C5_master_field_8192_omf4"] = {"value": timed(st5, 2), "unit": "traj/s", "trajectories": 2}
+    del U5
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -431,6 +497,9 @@ def run_ours(args):
         del Ub, si, so, xb
         torch.cuda.empty_cache()
 
+    # --- throughput of the other benchmark configurations (C1, C2, C3, C5)
+    configs = None if args.skip_configs else run_configs(qed2d, torch, dev)
+
     # --- CPU baseline: the oracle on the host cores, bounded sample
     cpu = None
     if not args.skip_cpu:
@@ -468,6 +537,7 @@ def run_ours(args):
             "batched_vs_f64_fused": value / world / (1.0 / base["f64"][0])},
         "dslash_hbm": dslash,
         "ensemble": ensemble,
+        "configs": configs,
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -483,6 +553,7 @@ def main():
     ap.add_argument("--skip-sweep", action="store_true", help="skip the 8192^2 Dslash bandwidth sweep")
     ap.add_argument("--skip-cpu", action="store_true", help="skip the oracle CPU baseline")
     ap.add_argument("--skip-ensemble", action="store_true", help="skip the 512-replica ensemble measurement")
+    ap.add_argument("--skip-configs", action="store_true", help="skip the C1/C2/C3/C5 throughput measurements")
     ap.add_argument("--skip-baselines", action="store_true",
                     help="skip the plain-FP64 and fused-FP64 GPU trajectories")
     args = ap.parse_args()
