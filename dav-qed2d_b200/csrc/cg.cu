@@ -22,6 +22,8 @@
 //
 // QED2D_PREC_PLAIN mirrors the reference's own structure (src/QED2dSolver.jl):
 // unfused kernels and two device-to-host reads per iteration.
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstddef>
@@ -68,6 +70,33 @@ __device__ __forceinline__ void write_partials(double* part, const double* v, in
         for (int k = 0; k < nv; k++) part[(size_t)k * kMaxPartBlocks + blockIdx.x] = v[k];
 }
 
+// RS = 2: the whole solve runs in ONE thread-block cluster (at most 16 blocks,
+// small lattices).  The hardware cluster barrier (barrier.cluster arrive with
+// release, wait with acquire) orders the blocks' memory accesses at cluster
+// scope, so no atomics, polling or error flag are needed.  Every block computes
+// the same reductions from the same partials in the same order, so all blocks
+// take the same path and reach the same barriers.
+struct ClusterSync {
+    int nred = 0;
+    __device__ __forceinline__ bool sync() {
+        cooperative_groups::this_cluster().sync();
+        return true;
+    }
+};
+template <int RS>
+struct SyncOf {
+    using type = GridSync;
+};
+template <>
+struct SyncOf<2> {
+    using type = ClusterSync;
+};
+template <int RS>
+__device__ __forceinline__ typename SyncOf<RS>::type make_sync(DevCtl* c) {
+    if constexpr (RS == 2) return ClusterSync{};
+    else return GridSync{&c->bar, &c->gen, &c->err};
+}
+
 // Grid-wide sum of NV values (NV <= 4), deterministic: every block writes its
 // partials and arrives at a bounded grid barrier; the partials are summed in a
 // fixed order (thread t takes partials t, t+blockDim, ..., then a fixed-shape
@@ -81,8 +110,8 @@ __device__ __forceinline__ void write_partials(double* part, const double* v, in
 // buffer n's only after every block has passed barrier n+1, i.e. has read the
 // results of n.  (The error flag is read once per barrier: a status kept in
 // shared memory instead made these kernels spill, 7% slower at 2048^2.)
-template <int NV, int RS>
-__device__ __forceinline__ bool reduce_sync(GridSync& gs, double (&v)[NV], double* part_base, double* red_base,
+template <int NV, int RS, class S>
+__device__ __forceinline__ bool reduce_sync(S& gs, double (&v)[NV], double* part_base, double* red_base,
                                             double* smem) {
     static_assert(NV <= kMaxPartVals / 2, "too many values for the double-buffered partials");
     __shared__ int s_last;
@@ -90,6 +119,25 @@ __device__ __forceinline__ bool reduce_sync(GridSync& gs, double (&v)[NV], doubl
     double* part = part_base + (size_t)buf * (kMaxPartVals / 2) * kMaxPartBlocks;
     block_sum<NV>(v, smem);
     write_partials(part, v, NV);
+    if constexpr (RS == 2) {   // cluster barrier, then every block sums the partials (as RS = 1)
+        gs.sync();
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            double s = 0.0;
+            for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x)
+                s += __ldcg(part + (size_t)k * kMaxPartBlocks + i);
+            v[k] = s;
+        }
+        block_sum<NV>(v, smem);
+        __shared__ double s_v2[4];
+        if (threadIdx.x == 0)
+#pragma unroll
+            for (int k = 0; k < NV; k++) s_v2[k] = v[k];
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < NV; k++) v[k] = s_v2[k];
+        return true;
+    } else {
     const bool last = gs.arrive(&s_last);
     if constexpr (RS == 0) {
         double* red = red_base + buf * 4;
@@ -141,6 +189,7 @@ __device__ __forceinline__ bool reduce_sync(GridSync& gs, double (&v)[NV], doubl
         for (int k = 0; k < NV; k++) v[k] = s_v[k];
         return ok;
     }
+    }
 }
 
 __device__ __forceinline__ void finish_solve(const CGP& P, int iters, bool conv, double rr, double bb,
@@ -167,7 +216,7 @@ __device__ __forceinline__ void finish_solve(const CGP& P, int iters, bool conv,
 template <int RS>
 __global__ void __launch_bounds__(TILE, 3) k_cg_f64(const CGP P) {
     __shared__ double smem[32 * 2];
-    GridSync gs{&P.ctl->bar, &P.ctl->gen, &P.ctl->err};
+    auto gs = make_sync<RS>(P.ctl);
     const long long ntiles = num_tiles(P.g), V = P.g.V;
     const TileRange TR = tile_range(ntiles, (P.g.L1 + TX - 1) / TX, P.per_block, blockIdx.x);
     const LkD L{P.U, V};
@@ -264,7 +313,7 @@ done:
 template <int RS>
 __global__ void __launch_bounds__(TILE, 4) k_cg_mixed(const CGP P) {
     __shared__ double smem[32 * 2];
-    GridSync gs{&P.ctl->bar, &P.ctl->gen, &P.ctl->err};
+    auto gs = make_sync<RS>(P.ctl);
     const long long ntiles = num_tiles(P.g), V = P.g.V;
     const TileRange TR = tile_range(ntiles, (P.g.L1 + TX - 1) / TX, P.per_block, blockIdx.x);
     const LkD L{P.U, V};
@@ -631,8 +680,84 @@ static int launch_coop(Ctx& c, K kernel, Par P) {
 
 static int solve_plain(Ctx& c, const SolveArgs& a);
 
-// Schedule tuning.  The two reduction schedules of reduce_sync give the same
-// bits, so the choice changes only the time.  The first solve of each
+// One-cluster launch (RS = 2): grid = cluster = min(tiles, 16) blocks, each a
+// contiguous range of tiles.  Only for lattices of at most kClusterTiles tiles;
+// returns QED2D_ERR_UNSUPPORTED when no such cluster fits on the device.
+constexpr int kClusterTiles = 128;
+
+template <class K>
+static int cluster_grid(Ctx& c, K kernel, int* grid) {
+    const long long nt = num_tiles(c.g);
+    if (nt > kClusterTiles) return QED2D_ERR_UNSUPPORTED;
+    int g = (int)std::min<long long>(nt, 16);
+    if (g > 8 && cudaFuncSetAttribute((const void*)kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                     cudaSuccess) {
+        cudaGetLastError();
+        g = 8;
+    }
+    for (; g >= 1; g /= 2) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(g);
+        cfg.blockDim = dim3(TILE);
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = g;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, (const void*)kernel, &cfg) == cudaSuccess && n >= 1) {
+            *grid = g;
+            return QED2D_OK;
+        }
+        cudaGetLastError();
+        if (g == 1) break;
+    }
+    return QED2D_ERR_UNSUPPORTED;
+}
+
+template <class Par>
+static int launch_cluster(Ctx& c, void (*kernel)(Par), Par P) {
+    int grid = 0;
+    QTRY(cluster_grid(c, kernel, &grid));
+    const long long nt = num_tiles(c.g);
+    P.per_block = (int)((nt + grid - 1) / grid);
+    grid = (int)((nt + P.per_block - 1) / P.per_block);   // no block without tiles
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(TILE);
+    cfg.stream = c.stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = grid;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    QCHECK(cudaLaunchKernelEx(&cfg, kernel, P));
+    count_launch();
+    return QED2D_OK;
+}
+
+// the solver of precision slot (0 = F64, 1 = MIXED) under schedule rs
+static int launch_cg(Ctx& c, const CGP& P, int slot, int rs) {
+    if (slot == 0) {
+        if (rs == 2) return launch_cluster(c, k_cg_f64<2>, P);
+        return launch_coop(c, rs ? k_cg_f64<1> : k_cg_f64<0>, P);
+    }
+    if (rs == 2) return launch_cluster(c, k_cg_mixed<2>, P);
+    return launch_coop(c, rs ? k_cg_mixed<1> : k_cg_mixed<0>, P);
+}
+
+static bool cluster_possible(Ctx& c, int slot) {
+    int g = 0;
+    return (slot == 0 ? cluster_grid(c, k_cg_f64<2>, &g) : cluster_grid(c, k_cg_mixed<2>, &g)) == QED2D_OK;
+}
+
+// Schedule tuning.  The reduction schedules of reduce_sync give the same bits
+// (RS = 2 only changes the number of blocks, and is tried only for lattices that
+// fit one cluster), so the choice changes only the time.  The first solve of each
 // precision on a context times both on the caller's operator and source,
 // capped at kTuneIters iterations, into scratch outputs, and keeps the faster;
 // the device control block is saved before and restored after, so counters and
@@ -647,25 +772,33 @@ bool tuning_enabled() {
 }
 
 template <class Launch>
-static int time_schedules(Ctx& c, Launch launch, int* best) {
+static int time_schedules(Ctx& c, Launch launch, int ncand, int* best) {
     cudaEvent_t e0, e1;
     QCHECK(cudaEventCreate(&e0));
     QCHECK(cudaEventCreate(&e1));
-    float tbest[2] = {1e30f, 1e30f};
+    float tbest[3] = {1e30f, 1e30f, 1e30f};
     int st = QED2D_OK;
     for (int rep = 0; rep < 3 && st == QED2D_OK; rep++)
-        for (int rs = 0; rs < 2 && st == QED2D_OK; rs++) {
+        for (int rs = 0; rs < ncand && st == QED2D_OK; rs++) {
             cudaEventRecord(e0, c.stream);
-            st = launch(rs);
+            const int lst = launch(rs);
             cudaEventRecord(e1, c.stream);
+            if (lst != QED2D_OK && rs == 2) {   // the cluster launch was refused: drop the candidate
+                cudaGetLastError();
+                tbest[2] = 2e30f;
+                continue;
+            }
+            st = lst;
             if (cudaEventSynchronize(e1) != cudaSuccess) st = cuda_status(cudaGetLastError(), "schedule tuning");
             float ms = 0.f;
             cudaEventElapsedTime(&ms, e0, e1);
-            if (rep > 0) tbest[rs] = std::min(tbest[rs], ms);   // the first round warms up
+            if (rep > 0 && tbest[rs] < 2e30f) tbest[rs] = std::min(tbest[rs], ms);   // round 0 warms up
         }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    *best = tbest[1] <= tbest[0] ? 1 : 0;
+    *best = 0;
+    for (int rs = 1; rs < ncand; rs++)
+        if (tbest[rs] <= tbest[*best]) *best = rs;
     return st;
 }
 
@@ -683,15 +816,15 @@ static int tune_cg(Ctx& c, const CGP& P, int slot) {
     if (!T.x || (P.g5x && !T.g5x)) return QED2D_ERR_NO_MEMORY;
     T.maxiter = std::min(P.maxiter, kTuneIters);
     const size_t fb = sizeof(double2) * 2 * (size_t)c.g.V;
+    const int ncand = cluster_possible(c, slot) ? 3 : 2;
     int best = 1;
     const int st = time_schedules(
         c,
         [&](int rs) -> int {
             if (P.guess) QCHECK(cudaMemcpyAsync(T.x, P.x, fb, cudaMemcpyDeviceToDevice, c.stream));
-            if (slot == 0) return launch_coop(c, rs ? k_cg_f64<1> : k_cg_f64<0>, T);
-            return launch_coop(c, rs ? k_cg_mixed<1> : k_cg_mixed<0>, T);
+            return launch_cg(c, T, slot, rs);
         },
-        &best);
+        ncand, &best);
     QCHECK(cudaMemcpyAsync(c.ctl, &saved, sizeof(DevCtl), cudaMemcpyHostToDevice, c.stream));
     QCHECK(cudaStreamSynchronize(c.stream));
     if (st != QED2D_OK) return st;
@@ -721,7 +854,8 @@ int cg_solve(Ctx& c, const SolveArgs& a, int precision) {
         P.p0 = c.spinor("cg_p0");
         P.p1 = c.spinor("cg_p1");
         if (c.sched[0] < 0) QTRY(tune_cg(c, P, 0));
-        return launch_coop(c, c.sched[0] ? k_cg_f64<1> : k_cg_f64<0>, P);
+        if (c.sched[0] == 2 && !cluster_possible(c, 0)) c.sched[0] = 1;
+        return launch_cg(c, P, 0, c.sched[0]);
     }
     P.r32 = c.spinor32("cg_r32");
     P.q0 = c.spinor32("cg_q0");
@@ -736,7 +870,8 @@ int cg_solve(Ctx& c, const SolveArgs& a, int precision) {
         P.U32 = u32;
     }
     if (c.sched[1] < 0) QTRY(tune_cg(c, P, 1));
-    return launch_coop(c, c.sched[1] ? k_cg_mixed<1> : k_cg_mixed<0>, P);
+    if (c.sched[1] == 2 && !cluster_possible(c, 1)) c.sched[1] = 1;
+    return launch_cg(c, P, 1, c.sched[1]);
 }
 
 int multishift_solve(Ctx& c, const double2* U, const double2* b, double2* const* x, const double* mu2, int n,

@@ -406,7 +406,7 @@ int qed2d_ctx_get_dims(const qed2d_ctx* ctx, int* L1, int* L2) {
 int qed2d_ctx_set_schedule(qed2d_ctx* ctx, int precision, int schedule) {
     QCTX(ctx);
     if (precision != QED2D_PREC_F64 && precision != QED2D_PREC_MIXED) return bad_arg("schedule: F64 or MIXED only");
-    if (schedule < -1 || schedule > 1) return bad_arg("schedule must be -1, 0 or 1");
+    if (schedule < -1 || schedule > 2) return bad_arg("schedule must be -1, 0, 1 or 2");
     c.sched[precision == QED2D_PREC_F64 ? 0 : 1] = schedule;
     return QED2D_OK;
 }

@@ -296,8 +296,9 @@ _PRECS = {"f64": _lib.PREC_F64, "mixed": _lib.PREC_MIXED}
 
 def set_schedule(prm: LattParm, schedule: int, precision="mixed") -> None:
     """Fix the persistent solver's reduction schedule on this lattice's context:
-    0 (last block publishes the sums) or 1 (every block sums), or -1 to tune
-    again on the next solve.  Both schedules give the same bits."""
+    0 (last block publishes the sums), 1 (every block sums), 2 (one
+    thread-block cluster, small lattices), or -1 to tune again on the next
+    solve.  0 and 1 give the same bits."""
     check(lib().qed2d_ctx_set_schedule(_c(prm), _PRECS[precision], int(schedule)), "set_schedule")
 
 
