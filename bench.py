@@ -372,7 +372,9 @@ def run_ours(args):
                     "value": len(sizes) * n_traj / t_e, "unit": "traj/s", "ms_per_batched_traj": 1e3 * t_e / n_traj,
                     "cg_iterations_per_traj_mean": sum(p[0] for p in per_rep) / (n_traj * len(sizes)),
                     "accepted": sum(p[1] for p in per_rep), "of": n_traj * len(sizes),
-                    "timed": f"{n_traj} batched trajectories after 1 warm-up"}
+                    "timed": f"{n_traj} batched trajectories after 1 warm-up",
+                    "solver": {2: "one launch over all replicas, grid barriers",
+                               3: "one thread-block cluster per replica"}.get(eb.schedule, "untuned")}
         del eb, Ue
         torch.cuda.empty_cache()
 

@@ -37,6 +37,7 @@
 namespace qed2d {
 
 constexpr int kMaxReplicas = 1024;
+constexpr int kReplicaCluster = 8;   // blocks per cluster of the cluster solver
 
 struct RepInfo {
     int L1, L2, nt1, nt;   // extents, tiles along i1, tiles of the replica
@@ -762,6 +763,7 @@ __global__ void k_r_finish(const RepState* __restrict__ st, int nrep, int maxite
 }  // namespace qed2d
 
 #include "batch_cg_uniform.cuh"
+#include "batch_cg_cluster.cuh"
 
 // ===========================================================================
 // host side
@@ -792,6 +794,8 @@ struct qed2d_batch {
     bool shared_state = false;      // records in shared memory (nrep <= kSharedReps)
     bool uniform = false;           // equal sizes, nrep <= kUniformReps: k_u_cg_mixed
     int usched = -1;                // its reduction schedule (-1: not tuned yet)
+    int rsched = -1;                // uneven batches: 2 grid solver, 3 one cluster per replica (-1: not tuned)
+    int* d_order = nullptr;         // [nrep] replicas by decreasing size (cluster solver)
     UGeom ug{};
     int ugrid = 0, ubpr = 0, uper_block = 0;
     double* d_upart = nullptr;      // [2][ubpr * nrep]
@@ -897,6 +901,68 @@ int tune_uniform(qed2d_batch* h, const UCGP& Q, int maxiter, Launch launch) {
     return QED2D_OK;
 }
 
+// First solve of an uneven batch: time the grid solver (k_r_cg_mixed, one
+// launch over all replicas with grid barriers) and the cluster solver
+// (k_rc_cg_mixed, one cluster per replica), capped at 24 iterations into
+// scratch outputs, and keep the faster; the control block is saved and
+// restored.  QED2D_TUNE=0 or a device without room for the clusters: the grid
+// solver.  The two group their sums differently (same accuracy, not the same
+// bits).
+template <class Launch>
+int tune_ragged(qed2d_batch* h, const RCGP& P, const CCGP& C, int maxiter, Launch launch) {
+    h->rsched = 2;
+    if (!tuning_enabled()) return QED2D_OK;
+    {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(kReplicaCluster);
+        cfg.blockDim = dim3(TILE);
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = kReplicaCluster;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, (const void*)k_rc_cg_mixed<kReplicaCluster>, &cfg) != cudaSuccess ||
+            n < 1) {
+            cudaGetLastError();
+            return QED2D_OK;
+        }
+    }
+    DevCtl saved;
+    QCHECK(cudaMemcpyAsync(&saved, h->ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, h->stream));
+    QCHECK(cudaStreamSynchronize(h->stream));
+    RCGP TP = P;
+    CCGP TC = C;
+    TP.x = TC.x = h->field("tune_x");
+    TP.t64 = TC.t64 = h->field("tune_g5x");
+    TP.maxiter = TC.maxiter = std::min(maxiter, 24);
+    if (!TP.x || !TP.t64) return QED2D_ERR_NO_MEMORY;
+    cudaEvent_t e0, e1;
+    QCHECK(cudaEventCreate(&e0));
+    QCHECK(cudaEventCreate(&e1));
+    float tbest[2] = {1e30f, 1e30f};
+    int st = QED2D_OK;
+    for (int rep = 0; rep < 3 && st == QED2D_OK; rep++)
+        for (int c = 0; c < 2 && st == QED2D_OK; c++) {
+            cudaEventRecord(e0, h->stream);
+            st = launch(2 + c, TP, TC);
+            cudaEventRecord(e1, h->stream);
+            if (cudaEventSynchronize(e1) != cudaSuccess) st = cuda_status(cudaGetLastError(), "schedule tuning");
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep > 0) tbest[c] = std::min(tbest[c], ms);
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    QCHECK(cudaMemcpyAsync(h->ctl, &saved, sizeof(DevCtl), cudaMemcpyHostToDevice, h->stream));
+    QCHECK(cudaStreamSynchronize(h->stream));
+    if (st != QED2D_OK) return st;
+    h->rsched = tbest[1] < tbest[0] ? 3 : 2;
+    return QED2D_OK;
+}
+
 int r_solve(qed2d_batch* h, const double2* U, const float4* U32, const double2* b, double2* x, double2* g5x,
             int maxiter, double eps) {
     RCGP P{};
@@ -928,8 +994,6 @@ int r_solve(qed2d_batch* h, const double2* U, const float4* U32, const double2* 
     P.flag_acc = h->d_cnt + h->nrep;
     P.part = h->d_part;
     P.ctl = h->ctl;
-    QCHECK(cudaMemsetAsync(&h->ctl->bar, 0, 2 * sizeof(unsigned long long) + sizeof(int), h->stream));
-    void* args[] = {(void*)&P};
     if (h->uniform) {
         UCGP Q{};
         Q.g = h->ug;
@@ -968,11 +1032,53 @@ int r_solve(qed2d_batch* h, const double2* U, const float4* U32, const double2* 
                                               h->ctl);
         return r_post("k_r_finish");
     } else {
-        QCHECK(cudaMemsetAsync(h->d_cnt, 0, sizeof(int) * (h->nrep + 1), h->stream));   // counters start at zero
-        const void* kern = h->shared_state ? (const void*)k_r_cg_mixed<true> : (const void*)k_r_cg_mixed<false>;
-        QCHECK(cudaLaunchCooperativeKernel(kern, dim3((unsigned)h->grid), dim3(TILE), args, 0, h->stream));
+        CCGP C{};
+        C.reps = h->d_reps;
+        C.order = h->d_order;
+        C.m2 = h->d_m2;
+        C.U = U;
+        C.U32 = U32;
+        C.b = b;
+        C.x = x;
+        C.t64 = g5x;
+        C.r64 = P.r64;
+        C.r32 = P.r32;
+        C.q0 = P.q0;
+        C.q1 = P.q1;
+        C.t32 = P.t32;
+        C.x32 = P.x32;
+        C.eps = eps;
+        C.delta2 = P.delta2;
+        C.maxiter = maxiter;
+        C.st_out = h->d_st;
+        auto launch = [&](int sched, const RCGP& p, const CCGP& cc) -> int {
+            if (sched == 3) {
+                cudaLaunchConfig_t cfg = {};
+                cfg.gridDim = dim3((unsigned)(h->nrep * kReplicaCluster));
+                cfg.blockDim = dim3(TILE);
+                cfg.stream = h->stream;
+                cudaLaunchAttribute at[1];
+                at[0].id = cudaLaunchAttributeClusterDimension;
+                at[0].val.clusterDim.x = kReplicaCluster;
+                at[0].val.clusterDim.y = 1;
+                at[0].val.clusterDim.z = 1;
+                cfg.attrs = at;
+                cfg.numAttrs = 1;
+                QCHECK(cudaLaunchKernelEx(&cfg, k_rc_cg_mixed<kReplicaCluster>, cc));
+            } else {
+                QCHECK(cudaMemsetAsync(&h->ctl->bar, 0, 2 * sizeof(unsigned long long) + sizeof(int), h->stream));
+                QCHECK(cudaMemsetAsync(h->d_cnt, 0, sizeof(int) * (h->nrep + 1), h->stream));   // counters at zero
+                void* rargs[] = {(void*)&p};
+                const void* kern =
+                    h->shared_state ? (const void*)k_r_cg_mixed<true> : (const void*)k_r_cg_mixed<false>;
+                QCHECK(cudaLaunchCooperativeKernel(kern, dim3((unsigned)h->grid), dim3(TILE), rargs, 0, h->stream));
+            }
+            count_launch();
+            return QED2D_OK;
+        };
+        if (h->rsched < 0) QTRY(tune_ragged(h, P, C, maxiter, launch));
+        QTRY(launch(h->rsched, P, C));
     }
-    count_launch();
     k_r_finish<<<1, 256, 0, h->stream>>>(h->d_st, h->nrep, maxiter, h->d_out, h->d_out + h->nrep, h->d_iters, h->ctl);
     return r_post("k_r_finish");
 }
@@ -1097,6 +1203,12 @@ int batch_setup(qed2d_batch* h, const int* L1, const int* L2, const double* beta
     QTRY(upload(&h->d_tiles, tiles));
     QTRY(upload(&h->d_seg0, seg0));
     QTRY(upload(&h->d_segs, segs));
+    {   // cluster solver: largest replicas first (they take longest)
+        std::vector<int> order(B);
+        for (int r = 0; r < B; r++) order[r] = r;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b2) { return h->reps[a].nt > h->reps[b2].nt; });
+        QTRY(upload(&h->d_order, order));
+    }
     QTRY(upload(&h->d_rep_seg, rep_seg));
     QTRY(upload(&h->d_dbase_c, dbc));
     QTRY(upload(&h->d_dbase_r, dbr));
@@ -1178,7 +1290,7 @@ int qed2d_batch_destroy(qed2d_batch* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     else cudaDeviceSynchronize();
     for (auto& kv : h->ws) cudaFree(kv.second.first);
-    void* dev[] = {h->d_reps, h->d_tiles, h->d_seg0, h->d_segs, h->d_rep_seg, h->d_dbase_c, h->d_dbase_r, h->d_m2,
+    void* dev[] = {h->d_reps, h->d_tiles, h->d_seg0, h->d_segs, h->d_order, h->d_rep_seg, h->d_dbase_c, h->d_dbase_r, h->d_m2,
                    h->d_beta, h->d_seed,  h->d_st, h->d_flags, h->d_red, h->d_cnt, h->d_upart, h->d_ured,      h->d_out,     h->d_iters,   h->d_sums,
                    h->d_tpart, h->d_part, h->ctl};
     for (void* p : dev)
@@ -1195,17 +1307,20 @@ int qed2d_batch_set_stream(qed2d_batch* h, void* stream) {
 }
 
 int qed2d_batch_set_schedule(qed2d_batch* h, int schedule) {
-    if (!h || schedule < -1 || schedule > 1) {
-        set_error("qed2d_batch_set_schedule: schedule must be -1, 0 or 1");
+    const bool ok = h && (schedule == -1 || (h->uniform ? (schedule == 0 || schedule == 1)
+                                                         : (schedule == 2 || schedule == 3)));
+    if (!ok) {
+        set_error("qed2d_batch_set_schedule: -1, or 0/1 (equal sizes, at most 64 replicas), or 2/3 (otherwise)");
         return QED2D_ERR_BAD_ARG;
     }
-    h->usched = schedule;
+    if (h->uniform) h->usched = schedule;
+    else h->rsched = schedule;
     return QED2D_OK;
 }
 
 int qed2d_batch_get_schedule(const qed2d_batch* h, int* schedule) {
     if (!h || !schedule) return QED2D_ERR_BAD_ARG;
-    *schedule = h->uniform ? h->usched : 2;
+    *schedule = h->uniform ? h->usched : h->rsched;
     return QED2D_OK;
 }
 

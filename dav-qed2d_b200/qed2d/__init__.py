@@ -624,8 +624,9 @@ class Batch:
 
     @property
     def schedule(self) -> int:
-        """Reduction schedule of the batched solver: -1 untuned, 0/1 (equal-size
-        batches of at most 64 replicas), 2 (ragged solver)."""
+        """Schedule of the batched solver: -1 untuned; equal-size batches of at
+        most 64 replicas 0/1 (reduction schedules, same bits); other batches 2
+        (one launch with grid barriers) or 3 (one thread-block cluster per replica)."""
         v = C.c_int(0)
         check(lib().qed2d_batch_get_schedule(self.h, C.byref(v)), "batch_get_schedule")
         return v.value

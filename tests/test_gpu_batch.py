@@ -202,4 +202,45 @@ def test_batch_reduction_schedules_give_identical_bits():
         its, _ = b.cg(x, U, src, [0.2, 0.3, 0.25], 20000, 1e-24)
         res.append((its, to_host(x)))
     assert res[0][0] == res[1][0] and np.array_equal(res[0][1], res[1][1])
-    assert qed2d.Batch.ragged([(16, 16), (32, 8)], [4.0, 4.0]).schedule == 2
+    assert qed2d.Batch.ragged([(16, 16), (32, 8)], [4.0, 4.0]).schedule == -1
+
+
+@pytest.mark.parametrize("nrep", [6, 80])
+def test_ragged_cluster_solver_matches_grid_solver(nrep):
+    """Uneven batches have two solvers: one launch over all replicas with grid
+    barriers (schedule 2) and one thread-block cluster per replica (schedule 3).
+    They group their sums differently: solutions agree to 1e-9 relative and with
+    the single-lattice solve; the first solve tunes the choice."""
+    import qed2d
+    rng = np.random.default_rng(123 + nrep)
+    sizes = [(int(a), int(b)) for a, b in zip(rng.choice([8, 16, 33, 64, 96], nrep), rng.choice([4, 8, 17, 40], nrep))]
+    am0s = rng.uniform(0.1, 0.5, nrep).tolist()
+    b = qed2d.Batch.ragged(sizes, [4.0] * nrep)
+    U, src = b.field(), b.field()
+    for r, (l1, l2) in enumerate(sizes):
+        b.replica(U, r).copy_(to_dev(hot_links(l1, l2, 60 + r)))
+        b.replica(src, r).copy_(to_dev(cgauss(l1, l2, 90 + r, 2)))
+    x = b.field()
+    b.cg(x, U, src, am0s, 20000, 1e-24)
+    assert b.schedule in (2, 3)
+    res = {}
+    for sched in (2, 3):
+        b.schedule = sched
+        x = b.field()
+        its, upd = b.cg(x, U, src, am0s, 20000, 1e-24)
+        res[sched] = (its, to_host(x))
+        x2 = b.field()
+        b.cg(x2, U, src, am0s, 20000, 1e-24)
+        assert np.array_equal(to_host(x2), res[sched][1])   # each solver is deterministic
+    assert rel(res[3][1], res[2][1]) < 1e-9
+    for r in range(nrep):
+        assert abs(res[3][0][r] - res[2][0][r]) <= max(3, res[2][0][r] // 20), r
+    qed2d.set_precision("mixed")
+    for r in (0, nrep - 1):
+        l1, l2 = sizes[r]
+        prm = qed2d.LattParm((l1, l2), 4.0)
+        xs = qed2d.cfield(l1, l2)
+        qed2d.CG(xs, b.replica(U, r).contiguous(), b.replica(src, r).contiguous(), am0s[r], 20000, 1e-24,
+                 qed2d.gamm5Dw_sqr_msq, prm, None)
+        assert rel(to_host(b.replica(x2, r)), to_host(xs)) < 1e-9, r
+    qed2d.set_precision("f64")
