@@ -37,7 +37,7 @@
 namespace qed2d {
 
 constexpr int kMaxReplicas = 1024;
-constexpr int kReplicaCluster = 8;   // blocks per cluster of the cluster solver
+constexpr int kClusterSizes[3] = {4, 8, 16};   // blocks per cluster tried by the cluster solver's tuner
 
 struct RepInfo {
     int L1, L2, nt1, nt;   // extents, tiles along i1, tiles of the replica
@@ -795,6 +795,7 @@ struct qed2d_batch {
     bool uniform = false;           // equal sizes, nrep <= kUniformReps: k_u_cg_mixed
     int usched = -1;                // its reduction schedule (-1: not tuned yet)
     int rsched = -1;                // uneven batches: 2 grid solver, 3 one cluster per replica (-1: not tuned)
+    int rcs = 8;                    // blocks per cluster of the cluster solver (tuned)
     int* d_order = nullptr;         // [nrep] replicas by decreasing size (cluster solver)
     UGeom ug{};
     int ugrid = 0, ubpr = 0, uper_block = 0;
@@ -901,35 +902,66 @@ int tune_uniform(qed2d_batch* h, const UCGP& Q, int maxiter, Launch launch) {
     return QED2D_OK;
 }
 
+// One cluster of cs blocks per replica (k_rc_cg_mixed<cs>).
+static bool cluster_fits(int cs, const void* kern) {
+    if (cs > 8 && cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cs);
+    cfg.blockDim = dim3(TILE);
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) != cudaSuccess || n < 1) {
+        cudaGetLastError();
+        return false;
+    }
+    return true;
+}
+
+static const void* replica_cluster_kernel(int cs) {
+    return cs == 4 ? (const void*)k_rc_cg_mixed<4> : cs == 16 ? (const void*)k_rc_cg_mixed<16> : (const void*)k_rc_cg_mixed<8>;
+}
+
+int launch_replica_clusters(qed2d_batch* h, const CCGP& cc, int cs) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(h->nrep * cs));
+    cfg.blockDim = dim3(TILE);
+    cfg.stream = h->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    if (cs == 4) QCHECK(cudaLaunchKernelEx(&cfg, k_rc_cg_mixed<4>, cc));
+    else if (cs == 16) QCHECK(cudaLaunchKernelEx(&cfg, k_rc_cg_mixed<16>, cc));
+    else QCHECK(cudaLaunchKernelEx(&cfg, k_rc_cg_mixed<8>, cc));
+    return QED2D_OK;
+}
+
 // First solve of an uneven batch: time the grid solver (k_r_cg_mixed, one
 // launch over all replicas with grid barriers) and the cluster solver
-// (k_rc_cg_mixed, one cluster per replica), capped at 24 iterations into
-// scratch outputs, and keep the faster; the control block is saved and
-// restored.  QED2D_TUNE=0 or a device without room for the clusters: the grid
-// solver.  The two group their sums differently (same accuracy, not the same
-// bits).
+// (k_rc_cg_mixed, one cluster of 4, 8 or 16 blocks per replica), capped at 24
+// iterations into scratch outputs, and keep the fastest; the control block is
+// saved and restored.  QED2D_TUNE=0: the grid solver.  The solvers group their
+// sums differently (same accuracy, not the same bits).
 template <class Launch>
 int tune_ragged(qed2d_batch* h, const RCGP& P, const CCGP& C, int maxiter, Launch launch) {
     h->rsched = 2;
     if (!tuning_enabled()) return QED2D_OK;
-    {
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(kReplicaCluster);
-        cfg.blockDim = dim3(TILE);
-        cudaLaunchAttribute at[1];
-        at[0].id = cudaLaunchAttributeClusterDimension;
-        at[0].val.clusterDim.x = kReplicaCluster;
-        at[0].val.clusterDim.y = 1;
-        at[0].val.clusterDim.z = 1;
-        cfg.attrs = at;
-        cfg.numAttrs = 1;
-        int n = 0;
-        if (cudaOccupancyMaxActiveClusters(&n, (const void*)k_rc_cg_mixed<kReplicaCluster>, &cfg) != cudaSuccess ||
-            n < 1) {
-            cudaGetLastError();
-            return QED2D_OK;
-        }
-    }
+    std::vector<int> cand = {0};   // 0: grid solver; cs > 0: clusters of cs blocks
+    for (int cs : kClusterSizes)
+        if (cluster_fits(cs, replica_cluster_kernel(cs))) cand.push_back(cs);
+    if (cand.size() == 1) return QED2D_OK;
     DevCtl saved;
     QCHECK(cudaMemcpyAsync(&saved, h->ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, h->stream));
     QCHECK(cudaStreamSynchronize(h->stream));
@@ -942,12 +974,12 @@ int tune_ragged(qed2d_batch* h, const RCGP& P, const CCGP& C, int maxiter, Launc
     cudaEvent_t e0, e1;
     QCHECK(cudaEventCreate(&e0));
     QCHECK(cudaEventCreate(&e1));
-    float tbest[2] = {1e30f, 1e30f};
+    std::vector<float> tbest(cand.size(), 1e30f);
     int st = QED2D_OK;
     for (int rep = 0; rep < 3 && st == QED2D_OK; rep++)
-        for (int c = 0; c < 2 && st == QED2D_OK; c++) {
+        for (size_t c = 0; c < cand.size() && st == QED2D_OK; c++) {
             cudaEventRecord(e0, h->stream);
-            st = launch(2 + c, TP, TC);
+            st = cand[c] ? launch(3, TP, TC, cand[c]) : launch(2, TP, TC, 0);
             cudaEventRecord(e1, h->stream);
             if (cudaEventSynchronize(e1) != cudaSuccess) st = cuda_status(cudaGetLastError(), "schedule tuning");
             float ms = 0.f;
@@ -959,7 +991,13 @@ int tune_ragged(qed2d_batch* h, const RCGP& P, const CCGP& C, int maxiter, Launc
     QCHECK(cudaMemcpyAsync(h->ctl, &saved, sizeof(DevCtl), cudaMemcpyHostToDevice, h->stream));
     QCHECK(cudaStreamSynchronize(h->stream));
     if (st != QED2D_OK) return st;
-    h->rsched = tbest[1] < tbest[0] ? 3 : 2;
+    size_t best = 0;
+    for (size_t c = 1; c < cand.size(); c++)
+        if (tbest[c] < tbest[best]) best = c;
+    if (cand[best]) {
+        h->rsched = 3;
+        h->rcs = cand[best];
+    }
     return QED2D_OK;
 }
 
@@ -1051,20 +1089,9 @@ int r_solve(qed2d_batch* h, const double2* U, const float4* U32, const double2* 
         C.delta2 = P.delta2;
         C.maxiter = maxiter;
         C.st_out = h->d_st;
-        auto launch = [&](int sched, const RCGP& p, const CCGP& cc) -> int {
+        auto launch = [&](int sched, const RCGP& p, const CCGP& cc, int cs) -> int {
             if (sched == 3) {
-                cudaLaunchConfig_t cfg = {};
-                cfg.gridDim = dim3((unsigned)(h->nrep * kReplicaCluster));
-                cfg.blockDim = dim3(TILE);
-                cfg.stream = h->stream;
-                cudaLaunchAttribute at[1];
-                at[0].id = cudaLaunchAttributeClusterDimension;
-                at[0].val.clusterDim.x = kReplicaCluster;
-                at[0].val.clusterDim.y = 1;
-                at[0].val.clusterDim.z = 1;
-                cfg.attrs = at;
-                cfg.numAttrs = 1;
-                QCHECK(cudaLaunchKernelEx(&cfg, k_rc_cg_mixed<kReplicaCluster>, cc));
+                QTRY(launch_replica_clusters(h, cc, cs));
             } else {
                 QCHECK(cudaMemsetAsync(&h->ctl->bar, 0, 2 * sizeof(unsigned long long) + sizeof(int), h->stream));
                 QCHECK(cudaMemsetAsync(h->d_cnt, 0, sizeof(int) * (h->nrep + 1), h->stream));   // counters at zero
@@ -1077,7 +1104,7 @@ int r_solve(qed2d_batch* h, const double2* U, const float4* U32, const double2* 
             return QED2D_OK;
         };
         if (h->rsched < 0) QTRY(tune_ragged(h, P, C, maxiter, launch));
-        QTRY(launch(h->rsched, P, C));
+        QTRY(launch(h->rsched, P, C, h->rcs));
     }
     k_r_finish<<<1, 256, 0, h->stream>>>(h->d_st, h->nrep, maxiter, h->d_out, h->d_out + h->nrep, h->d_iters, h->ctl);
     return r_post("k_r_finish");
