@@ -215,16 +215,20 @@ def run_configs(qed2d, torch, dev):
     U2 = torch.from_numpy(hot_start(64, 64, 64)).to(dev)
     for _ in range(10):
         qed2d.HMC_(U2, 0.1, 10, [], p2, None)   # pure-gauge thermalisation
-    c2 = {}
+    c2, sched = {}, {}
+    names = {0: "grid, last block publishes", 1: "grid, every block sums", 2: "one thread-block cluster"}
     for prec in ("mixed", "f64", "plain"):
         qed2d.set_precision(prec)
         Uc = U2.clone()
         st = lambda: qed2d.HMC_(Uc, 0.1, 0.05, 20, [], MAXITER, TOL, p2, None)
         st()
-        c2[prec] = timed(st, 5)
+        c2[prec] = timed(st, 10)
+        if prec != "plain":
+            sched[prec] = names.get(qed2d.get_schedule(p2, prec), "untuned")
     qed2d.set_precision("f64")
     out["C2_nf2_64_leapfrog"] = {"unit": "traj/s", "mixed": c2["mixed"], "f64_fused": c2["f64"], "plain_f64": c2["plain"],
-                                 "mixed_vs_plain": c2["mixed"] / c2["plain"], "trajectories": 5}
+                                 "mixed_vs_plain": c2["mixed"] / c2["plain"], "trajectories": 10,
+                                 "solver_schedule": sched}
     # C3
     p3 = qed2d.LattParm((128, 128), 4.0)
     U3 = torch.from_numpy(hot_start(128, 128, 128)).to(dev)
