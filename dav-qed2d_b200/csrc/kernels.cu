@@ -14,6 +14,18 @@ int64_t launches() { return g_launches.load(); }
 
 static inline unsigned tiles_grid(const Lat& g) { return (unsigned)num_tiles(g); }
 
+// Tile kernels run on a 2D grid of tiles (x along i1, y along i2), so a thread
+// finds its site without an index division; lattices taller than 65535 tiles
+// fall back to a 1D grid.
+static inline dim3 tiles_grid2(const Lat& g) {
+    const unsigned nt1 = (unsigned)((g.L1 + TX - 1) / TX), nt2 = (unsigned)((g.L2 + TY - 1) / TY);
+    return nt2 <= 65535 ? dim3(nt1, nt2) : dim3(tiles_grid(g));
+}
+__device__ __forceinline__ Site tile_site(const Lat& g) {
+    return gridDim.y > 1 || g.L2 <= TY ? site_at(g, blockIdx.x, blockIdx.y, threadIdx.x)
+                                       : site_of_tile(g, blockIdx.x, threadIdx.x);
+}
+
 // ---------------------------------------------------------------------------
 // gamm5Dw (src/QED2dDirac.jl:2-33); optionally  so += addc * addv  with complex
 // addc (the mu^2 si term of gamm5Dw_sqr_musq, :92, and the +-i mu terms of
@@ -22,7 +34,7 @@ static inline unsigned tiles_grid(const Lat& g) { return (unsigned)num_tiles(g);
 __global__ void __launch_bounds__(TILE) k_g5dw(double2* __restrict__ so, const double2* __restrict__ U,
                                                const double2* __restrict__ si, double m2, Lat g,
                                                const double2* __restrict__ addv, double2 addc, int g5_out) {
-    const Site q = site_of_tile(g, blockIdx.x, threadIdx.x);
+    const Site q = tile_site(g);
     if (!q.ok) return;
     Pair<double> o = g5dw_at<double>(SpDro{si, g.V}, LkD{U, g.V}, q, m2);
     if (addv) {
@@ -37,7 +49,7 @@ __global__ void __launch_bounds__(TILE) k_g5dw(double2* __restrict__ so, const d
 // the mixed solver's inner iterations on complex64 spinors and links
 __global__ void __launch_bounds__(TILE) k_g5dw_c64(float2* __restrict__ so, const float2* __restrict__ U,
                                                    const float2* __restrict__ si, float m2, Lat g) {
-    const Site q = site_of_tile(g, blockIdx.x, threadIdx.x);
+    const Site q = tile_site(g);
     if (!q.ok) return;
     const Pair<float> o = g5dw_at<float>(SpF2{si, g.V}, LkF2{U, g.V}, q, m2);
     so[q.x] = o.a;
@@ -56,7 +68,7 @@ __global__ void k_g5(double2* __restrict__ so, const double2* __restrict__ si, l
 __global__ void __launch_bounds__(TILE) k_force(double* __restrict__ frc, const double2* __restrict__ U,
                                                 const double2* __restrict__ X, const double2* __restrict__ G,
                                                 Lat g, double rho, int accumulate) {
-    const Site q = site_of_tile(g, blockIdx.x, threadIdx.x);
+    const Site q = tile_site(g);
     if (!q.ok) return;
     double f1, f2;
     fermion_force_at(U, X, G, g.V, q, f1, f2);
@@ -72,7 +84,7 @@ __global__ void __launch_bounds__(TILE) k_force(double* __restrict__ frc, const 
 // plaquette! (mode 0, Re P) and qtop! (mode 1, arg P) -- src/QED2dAction.jl:2-32
 __global__ void __launch_bounds__(TILE) k_plaq_field(double* __restrict__ plx, const double2* __restrict__ U, Lat g,
                                                      int mode) {
-    const Site q = site_of_tile(g, blockIdx.x, threadIdx.x);
+    const Site q = tile_site(g);
     if (!q.ok) return;
     const double2 p = plaquette_of(__ldg(U + q.x), __ldg(U + g.V + q.xp1), __ldg(U + q.xp2), __ldg(U + g.V + q.x));
     plx[q.x] = mode == 0 ? p.x : atan2(p.y, p.x);
@@ -81,7 +93,7 @@ __global__ void __launch_bounds__(TILE) k_plaq_field(double* __restrict__ plx, c
 // krnl_force! -- src/QED2dAction.jl:34-53: every element of frc1 and frc2 written once
 __global__ void __launch_bounds__(TILE) k_krnl_force(double* __restrict__ frc1, double* __restrict__ frc2,
                                                      const double2* __restrict__ U, Lat g, double beta) {
-    const Site q = site_of_tile(g, blockIdx.x, threadIdx.x);
+    const Site q = tile_site(g);
     if (!q.ok) return;
     const double2 p = plaquette_of(__ldg(U + q.x), __ldg(U + g.V + q.xp1), __ldg(U + q.xp2), __ldg(U + g.V + q.x));
     const double v = beta * p.y;
@@ -159,7 +171,7 @@ __global__ void k_random_normal(double* __restrict__ out, long long n, uint64_t 
 __global__ void __launch_bounds__(TILE) k_mom_kick(double* __restrict__ mom, const double2* __restrict__ U, Lat g,
                                                    double beta, double eps, const double2* __restrict__ X,
                                                    const double2* __restrict__ G, const double* __restrict__ frc) {
-    const Site q = site_of_tile(g, blockIdx.x, threadIdx.x);
+    const Site q = tile_site(g);
     if (!q.ok) return;
     double F1, F2;
     gauge_force_at(U, g, q, beta, F1, F2);
@@ -293,13 +305,13 @@ static unsigned reduce_grid(long long n) {
 }
 
 int launch_g5dw_c64(Ctx& c, float2* so, const float2* U, const float2* si, double am0) {
-    k_g5dw_c64<<<tiles_grid(c.g), TILE, 0, c.stream>>>(so, U, si, (float)(2.0 + am0), c.g);
+    k_g5dw_c64<<<tiles_grid2(c.g), TILE, 0, c.stream>>>(so, U, si, (float)(2.0 + am0), c.g);
     return post_launch("k_g5dw_c64");
 }
 
 int launch_g5dw(Ctx& c, double2* so, const double2* U, const double2* si, double am0, const double2* addv,
                 double2 addc, bool g5_out) {
-    k_g5dw<<<tiles_grid(c.g), TILE, 0, c.stream>>>(so, U, si, 2.0 + am0, c.g, addv, addc, g5_out ? 1 : 0);
+    k_g5dw<<<tiles_grid2(c.g), TILE, 0, c.stream>>>(so, U, si, 2.0 + am0, c.g, addv, addc, g5_out ? 1 : 0);
     return post_launch("k_g5dw");
 }
 
@@ -309,23 +321,23 @@ int launch_g5(Ctx& c, double2* so, const double2* si) {
 }
 
 int launch_tr_dqwdu(Ctx& c, double* frc, const double2* U, const double2* X, const double2* G) {
-    k_force<<<tiles_grid(c.g), TILE, 0, c.stream>>>(frc, U, X, G, c.g, 1.0, 0);
+    k_force<<<tiles_grid2(c.g), TILE, 0, c.stream>>>(frc, U, X, G, c.g, 1.0, 0);
     return post_launch("k_force");
 }
 
 int launch_force_accum(Ctx& c, double* frc, const double2* U, const double2* X, const double2* G, double rho,
                        bool accumulate) {
-    k_force<<<tiles_grid(c.g), TILE, 0, c.stream>>>(frc, U, X, G, c.g, rho, accumulate ? 1 : 0);
+    k_force<<<tiles_grid2(c.g), TILE, 0, c.stream>>>(frc, U, X, G, c.g, rho, accumulate ? 1 : 0);
     return post_launch("k_force");
 }
 
 int launch_plaq_field(Ctx& c, double* plx, const double2* U, int mode) {
-    k_plaq_field<<<tiles_grid(c.g), TILE, 0, c.stream>>>(plx, U, c.g, mode);
+    k_plaq_field<<<tiles_grid2(c.g), TILE, 0, c.stream>>>(plx, U, c.g, mode);
     return post_launch("k_plaq_field");
 }
 
 int launch_krnl_force(Ctx& c, double* frc1, double* frc2, const double2* U) {
-    k_krnl_force<<<tiles_grid(c.g), TILE, 0, c.stream>>>(frc1, frc2, U, c.g, c.beta);
+    k_krnl_force<<<tiles_grid2(c.g), TILE, 0, c.stream>>>(frc1, frc2, U, c.g, c.beta);
     return post_launch("k_krnl_force");
 }
 
@@ -371,7 +383,7 @@ int launch_random_normal(Ctx& c, double* out, int64_t n, uint64_t seed, uint32_t
 
 int launch_mom_kick(Ctx& c, double* mom, const double2* U, double eps, const double2* X, const double2* G,
                     const double* frc) {
-    k_mom_kick<<<tiles_grid(c.g), TILE, 0, c.stream>>>(mom, U, c.g, c.beta, eps, X, G, frc);
+    k_mom_kick<<<tiles_grid2(c.g), TILE, 0, c.stream>>>(mom, U, c.g, c.beta, eps, X, G, frc);
     return post_launch("k_mom_kick");
 }
 
