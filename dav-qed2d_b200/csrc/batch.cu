@@ -76,6 +76,8 @@ __global__ void __launch_bounds__(TILE) k_r_mom_kick(double* __restrict__ mom, c
     const Site q = site_at(g, T.y, T.z, threadIdx.x);
     if (!q.ok) return;
     const long long o = 2 * R.off;
+    double* m = mom + o;
+    const double mo1 = m[q.x], mo2 = m[q.x + g.V];   // issued with the link loads
     double F1, F2;
     gauge_force_at(U + o, g, q, beta[T.x], F1, F2);
     if (X) {
@@ -84,9 +86,8 @@ __global__ void __launch_bounds__(TILE) k_r_mom_kick(double* __restrict__ mom, c
         F1 = F1 + f1;
         F2 = F2 + f2;
     }
-    double* m = mom + o;
-    m[q.x] = m[q.x] + eps * F1;
-    m[q.x + g.V] = m[q.x + g.V] + eps * F2;
+    m[q.x] = mo1 + eps * F1;
+    m[q.x + g.V] = mo2 + eps * F2;
 }
 
 // U <- exp(i eps mom) U (updt_fld!, src/QED2dAction.jl:55-65) and the packed FP32

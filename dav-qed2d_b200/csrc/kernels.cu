@@ -173,6 +173,7 @@ __global__ void __launch_bounds__(TILE) k_mom_kick(double* __restrict__ mom, con
                                                    const double2* __restrict__ G, const double* __restrict__ frc) {
     const Site q = tile_site(g);
     if (!q.ok) return;
+    const double mo1 = mom[q.x], mo2 = mom[q.x + g.V];   // issued with the link loads
     double F1, F2;
     gauge_force_at(U, g, q, beta, F1, F2);
     if (X) {
@@ -185,8 +186,8 @@ __global__ void __launch_bounds__(TILE) k_mom_kick(double* __restrict__ mom, con
         F1 = F1 + frc[q.x];
         F2 = F2 + frc[q.x + g.V];
     }
-    mom[q.x] = mom[q.x] + eps * F1;
-    mom[q.x + g.V] = mom[q.x + g.V] + eps * F2;
+    mom[q.x] = mo1 + eps * F1;
+    mom[q.x + g.V] = mo2 + eps * F2;
 }
 
 // y = a x + b z (complex scalars; z may alias y)

@@ -192,26 +192,23 @@ __device__ __forceinline__ Pair<R> g5dw_at_c(const S& s, const Pair<R>& c, const
     return o;
 }
 
-// v(y) = Im P(y) for the gauge force (src/QED2dAction.jl:42-45, without beta)
-__device__ __forceinline__ double im_plaq(const double2* U, const Lat& g, int i1, int i2) {
-    const long long V = g.V;
-    const int iu1 = (i1 + 1 == g.L1) ? 0 : i1 + 1;
-    const int iu2 = (i2 + 1 == g.L2) ? 0 : i2 + 1;
-    const long long x = i1 + (long long)g.L1 * i2;
-    const double2 p = plaquette_of(__ldg(U + x), __ldg(U + V + iu1 + (long long)g.L1 * i2),
-                                   __ldg(U + i1 + (long long)g.L1 * iu2), __ldg(U + V + x));
-    return p.y;
-}
-
 // total gauge force on the two links of site y: frc1+frc2 of krnl_force!
 //   F1(y) = -v(y) + v(y-2),  F2(y) = v(y) - v(y-1)
+// The three plaquettes share links: the 10 distinct links are addressed from
+// the site's neighbour indices and all loaded before any arithmetic, so a
+// thread waits for memory once (the diagonal neighbours y-1+2 and y+1-2 are
+// the row neighbours shifted by the same i1 offset).
 __device__ __forceinline__ void gauge_force_at(const double2* U, const Lat& g, const Site& q, double beta,
                                                double& F1, double& F2) {
-    const int im1 = (q.i1 == 0) ? g.L1 - 1 : q.i1 - 1;
-    const int im2 = (q.i2 == 0) ? g.L2 - 1 : q.i2 - 1;
-    const double v = beta * im_plaq(U, g, q.i1, q.i2);
-    const double vm2 = beta * im_plaq(U, g, q.i1, im2);
-    const double vm1 = beta * im_plaq(U, g, im1, q.i2);
+    const long long V = g.V;
+    const long long xm1p2 = q.xp2 + (q.xm1 - q.x), xp1m2 = q.xm2 + (q.xp1 - q.x);
+    const double2 u1x = __ldg(U + q.x), u2x = __ldg(U + V + q.x);
+    const double2 u2xp1 = __ldg(U + V + q.xp1), u1xp2 = __ldg(U + q.xp2);
+    const double2 u1xm2 = __ldg(U + q.xm2), u2xm2 = __ldg(U + V + q.xm2), u2xp1m2 = __ldg(U + V + xp1m2);
+    const double2 u1xm1 = __ldg(U + q.xm1), u2xm1 = __ldg(U + V + q.xm1), u1xm1p2 = __ldg(U + xm1p2);
+    const double v = beta * plaquette_of(u1x, u2xp1, u1xp2, u2x).y;
+    const double vm2 = beta * plaquette_of(u1xm2, u2xp1m2, u1x, u2xm2).y;
+    const double vm1 = beta * plaquette_of(u1xm1, u2x, u1xm1p2, u2xm1).y;
     F1 = -v + vm2;
     F2 = v - vm1;
 }
