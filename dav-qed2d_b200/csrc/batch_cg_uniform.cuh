@@ -63,8 +63,8 @@ __device__ __forceinline__ Site usite_at(const UGeom& g, int r, int t1, int t2, 
 // Barrier with one sum per replica (one warp per replica over its blocks'
 // partials, fixed order).  Two schedules give the same bits: RS = 0, the last
 // block to arrive sums and publishes red[] before releasing and every block
-// reads red[]; RS = 1, the last block releases at once and every block sums
-// the partials itself.  Then every block runs every replica's recurrences for
+// reads red[]; RS = 1, a counter barrier, then every block sums the partials
+// itself.  Then every block runs every replica's recurrences for
 // reduction `kind` on its shared records and flags.  A failed or timed-out
 // wait is passed on through shared memory.
 template <int RS>
@@ -81,7 +81,6 @@ __device__ __forceinline__ bool ureduce(GridSync& gs, double v, const UCGP& P, d
         part[blockIdx.x] = vv[0];
         s_bits = 0;
     }
-    const bool last = gs.arrive(&s_last);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     auto sum_partials = [&](double* out) {
         for (int r = warp; r < P.g.B; r += nw) {
@@ -93,8 +92,7 @@ __device__ __forceinline__ bool ureduce(GridSync& gs, double v, const UCGP& P, d
         }
     };
     if constexpr (RS == 0) {
-        if (last) {
-            __threadfence();
+        if (gs.arrive(&s_last)) {
             sum_partials(red);
             __syncthreads();
             if (threadIdx.x == 0) {
@@ -107,16 +105,8 @@ __device__ __forceinline__ bool ureduce(GridSync& gs, double v, const UCGP& P, d
         __syncthreads();
         if (threadIdx.x < P.g.B) s_red[threadIdx.x] = __ldcg(red + threadIdx.x);
     } else {
-        if (threadIdx.x == 0) {
-            if (last) {
-                gs.release();
-                s_ok = 1;
-            } else {
-                s_ok = gs.wait();
-            }
-        }
-        __syncthreads();
-        if (last) __threadfence();
+        gs.count_sync();
+        if (threadIdx.x == 0) s_ok = ld_volatile_int(gs.err) == 0;
         sum_partials(s_red);
     }
     __syncthreads();

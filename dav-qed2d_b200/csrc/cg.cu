@@ -103,8 +103,8 @@ __device__ __forceinline__ typename SyncOf<RS>::type make_sync(DevCtl* c) {
 // tree).  Two schedules give the same bits:
 //   RS = 0: the last block to arrive sums them, publishes the sums in red[]
 //           and releases; every block then reads red[] (one more round trip);
-//   RS = 1: the last block releases at once and every block sums all partials
-//           itself (no second round trip, more L2 reads).
+//   RS = 1: counter barrier, then every block sums all partials itself (no
+//           second round trip, more L2 reads).
 // Which one is faster depends on the lattice size; the context tunes it.
 // Partials and sums alternate between two buffers: reduction n+2 overwrites
 // buffer n's only after every block has passed barrier n+1, i.e. has read the
@@ -137,12 +137,10 @@ __device__ __forceinline__ bool reduce_sync(S& gs, double (&v)[NV], double* part
 #pragma unroll
         for (int k = 0; k < NV; k++) v[k] = s_v2[k];
         return true;
-    } else {
-    const bool last = gs.arrive(&s_last);
-    if constexpr (RS == 0) {
+    } else if constexpr (RS == 0) {
+        const bool last = gs.arrive(&s_last);
         double* red = red_base + buf * 4;
         if (last) {
-            __threadfence();
             double w[NV];
 #pragma unroll
             for (int k = 0; k < NV; k++) {
@@ -165,13 +163,8 @@ __device__ __forceinline__ bool reduce_sync(S& gs, double (&v)[NV], double* part
         for (int k = 0; k < NV; k++) v[k] = __ldcg(red + k);
         return ld_volatile_int(gs.err) == 0;
     } else {
-        if (threadIdx.x == 0) {
-            if (last) gs.release();
-            else gs.wait();
-        }
-        __syncthreads();
+        gs.count_sync();
         const bool ok = ld_volatile_int(gs.err) == 0;   // issued together with the partial loads
-        if (last) __threadfence();
 #pragma unroll
         for (int k = 0; k < NV; k++) {
             double s = 0.0;
@@ -188,7 +181,6 @@ __device__ __forceinline__ bool reduce_sync(S& gs, double (&v)[NV], double* part
 #pragma unroll
         for (int k = 0; k < NV; k++) v[k] = s_v[k];
         return ok;
-    }
     }
 }
 
@@ -503,12 +495,13 @@ struct MSP {
     double* part;
 };
 
+// RS: the reduction schedules of reduce_sync (tuned per context as for cg_solve).
+template <int RS>
 __global__ void __launch_bounds__(TILE, 3) k_cg_multishift(const MSP P) {
-    constexpr int RS = 1;   // latency-bound at the RHMC sizes: every block sums
     __shared__ double smem[32 * 2];
     __shared__ double z[kMaxShifts], zp[kMaxShifts], ai[kMaxShifts], bi[kMaxShifts];
     __shared__ int upd[kMaxShifts], act[kMaxShifts];
-    GridSync gs{&P.ctl->bar, &P.ctl->gen, &P.ctl->err};
+    auto gs = make_sync<RS>(P.ctl);
     const long long ntiles = num_tiles(P.g), V = P.g.V;
     const TileRange TR = tile_range(ntiles, (P.g.L1 + TX - 1) / TX, P.per_block, blockIdx.x);
     const LkD L{P.U, V};
@@ -874,6 +867,46 @@ int cg_solve(Ctx& c, const SolveArgs& a, int precision) {
     return launch_cg(c, P, 1, c.sched[1]);
 }
 
+static int launch_multishift(Ctx& c, const MSP& P, int rs) {
+    if (rs == 2) return launch_cluster(c, k_cg_multishift<2>, P);
+    return launch_coop(c, rs ? k_cg_multishift<1> : k_cg_multishift<0>, P);
+}
+
+static bool multishift_cluster_possible(Ctx& c) {
+    int g = 0;
+    return cluster_grid(c, k_cg_multishift<2>, &g) == QED2D_OK;
+}
+
+// As tune_cg: the first multishift solve of a context times the schedules on the
+// caller's operator and source, capped at kTuneIters iterations, into scratch
+// solutions (one per shift), and keeps the fastest.  The single cluster wins on
+// the smallest lattices (one barrier round trip less than the grid, a few tiles
+// per block); the grid wins once a cluster's blocks walk many tiles each, the
+// shift updates growing with them.
+static int tune_multishift(Ctx& c, const MSP& P) {
+    if (!tuning_enabled()) {
+        c.sched[2] = 1;
+        return QED2D_OK;
+    }
+    DevCtl saved;
+    QCHECK(cudaMemcpyAsync(&saved, c.ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, c.stream));
+    QCHECK(cudaStreamSynchronize(c.stream));
+    MSP T = P;
+    for (int i = 0; i < P.n; i++) {
+        T.x[i] = c.spinor("tune_ms_x_" + std::to_string(i));
+        if (!T.x[i]) return QED2D_ERR_NO_MEMORY;
+    }
+    T.maxiter = std::min(P.maxiter, kTuneIters);
+    const int ncand = multishift_cluster_possible(c) ? 3 : 2;
+    int best = 1;
+    const int st = time_schedules(c, [&](int rs) -> int { return launch_multishift(c, T, rs); }, ncand, &best);
+    QCHECK(cudaMemcpyAsync(c.ctl, &saved, sizeof(DevCtl), cudaMemcpyHostToDevice, c.stream));
+    QCHECK(cudaStreamSynchronize(c.stream));
+    if (st != QED2D_OK) return st;
+    c.sched[2] = best;
+    return QED2D_OK;
+}
+
 int multishift_solve(Ctx& c, const double2* U, const double2* b, double2* const* x, const double* mu2, int n,
                      double am0, int maxiter, double eps) {
     if (n < 1 || n > kMaxShifts) return QED2D_ERR_BAD_ARG;
@@ -901,7 +934,9 @@ int multishift_solve(Ctx& c, const double2* U, const double2* b, double2* const*
     P.maxiter = maxiter;
     P.ctl = c.ctl;
     P.part = c.part;
-    return launch_coop(c, k_cg_multishift, P);
+    if (c.sched[2] < 0) QTRY(tune_multishift(c, P));
+    if (c.sched[2] == 2 && !multishift_cluster_possible(c)) c.sched[2] = 1;
+    return launch_multishift(c, P, c.sched[2]);
 }
 
 // ---------------------------------------------------------------------------

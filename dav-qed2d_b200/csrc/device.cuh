@@ -114,14 +114,25 @@ __device__ __forceinline__ void normal_pair(uint64_t seed, uint32_t stream, uint
 }
 
 // ---------------------------------------------------------------------------
-// Grid-wide barrier for persistent kernels launched cooperatively (all blocks
-// co-resident).  Every block adds one arrival to `arrivals`; the block that
-// arrives last (it sees target-1) does the barrier's completion work (e.g. the
-// final sum of a reduction) and then publishes the barrier's generation in
-// `gen`; the others poll `gen`.  Both counters only grow within a launch and
-// are zeroed before it.  The wait is bounded: after ~2^26 polls (seconds) a
-// block records QED2D_ERR_TIMEOUT in *err and leaves, and every block stops at
-// its next check of *err.
+// Grid-wide barriers for persistent kernels launched cooperatively (all blocks
+// co-resident).  Every block's thread 0 adds one arrival to `arrivals` after a
+// __syncthreads, with release semantics: the block's earlier writes, by any of
+// its threads, are ordered before its arrival.  Two ways to leave:
+//  * count_sync: thread 0 polls `arrivals` with acquire loads until it reaches
+//    the barrier's target (gridDim.x per barrier so far), then the block
+//    follows through a __syncthreads.  One fire-and-forget add and one poll per
+//    block: the short path;
+//  * arrive / release / wait: the block whose add sees target-1 arrived last; it
+//    does the barrier's completion work (e.g. the final sum of a reduction) and
+//    publishes the barrier's generation in `gen` (release), the others poll
+//    `gen` (acquire).
+// The adds of all blocks form one chain of atomic updates of `arrivals`, so an
+// acquire that sees the final count is ordered after every block's release.
+// No sequentially-consistent fence (__threadfence) is needed on either path.
+// Both counters only grow within a launch and are zeroed before it; the two
+// kinds of barrier can follow each other in one kernel.  Waits are bounded:
+// after ~2^26 polls (seconds) a block records QED2D_ERR_TIMEOUT in *err and
+// leaves, and every block stops at its next check of *err.
 __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
     unsigned long long v;
     asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
@@ -129,6 +140,14 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
 }
 __device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
     asm volatile("st.release.gpu.global.u64 [%0], %1;" : : "l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ void red_release_add_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("red.release.gpu.global.add.u64 [%0], %1;" : : "l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long atom_acq_rel_add_u64(unsigned long long* p, unsigned long long v) {
+    unsigned long long old;
+    asm volatile("atom.acq_rel.gpu.global.add.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+    return old;
 }
 __device__ __forceinline__ int ld_volatile_int(const int* p) {
     return *reinterpret_cast<const volatile int*>(p);
@@ -141,58 +160,52 @@ struct GridSync {
     unsigned long long target = 0;
     int nred = 0;   // reductions done so far: selects the double-buffered partials/results
 
-    // Arrive (thread 0 of each block).  Returns true in the last-arriving block.
+    // Poll *c (acquire) until it reaches target, bounded.  False when the wait
+    // ended on the error flag or timed out.
+    __device__ __forceinline__ bool poll(const unsigned long long* c) {
+        unsigned long long polls = 0;
+        while (ld_acquire_u64(c) < target) {
+            if (ld_volatile_int(err) != 0) return false;
+            if (++polls > (1ULL << 26)) {
+                atomicExch(err, 2 /* QED2D_ERR_TIMEOUT */);
+                return false;
+            }
+            __nanosleep(32);
+        }
+        return true;
+    }
+    // Counter barrier (all threads).  No status: a failed wait has set *err,
+    // which the caller reads.
+    __device__ __forceinline__ void count_sync() {
+        __syncthreads();
+        target += gridDim.x;
+        if (threadIdx.x == 0) {
+            red_release_add_u64(arrivals, 1ULL);
+            poll(arrivals);
+        }
+        __syncthreads();
+    }
+    // Arrive (all threads; thread 0 adds).  Returns true in the last-arriving
+    // block, whose threads are then ordered after every block's arrival.
     __device__ __forceinline__ bool arrive(int* s_last) {
         __syncthreads();
         target += gridDim.x;
         if (threadIdx.x == 0) {
-            __threadfence();
-            const unsigned long long old = atomicAdd(arrivals, 1ULL);
+            const unsigned long long old = atom_acq_rel_add_u64(arrivals, 1ULL);
             *s_last = old == target - 1;
         }
         __syncthreads();
         return *s_last != 0;
     }
-    // Release (called by thread 0 of the last block after its completion work).
-    __device__ __forceinline__ void release() {
-        __threadfence();
-        st_release_u64(gen, target);
-    }
-    // Wait for the release (thread 0 of the other blocks), bounded.  Returns
-    // false when the wait ended on the error flag or timed out.
-    __device__ __forceinline__ bool wait() {
-        unsigned long long polls = 0;
-        bool ok = true;
-        while (ld_acquire_u64(gen) < target) {
-            if (ld_volatile_int(err) != 0) {
-                ok = false;
-                break;
-            }
-            if (++polls > (1ULL << 26)) {
-                atomicExch(err, 2 /* QED2D_ERR_TIMEOUT */);
-                ok = false;
-                break;
-            }
-            __nanosleep(32);
-        }
-        __threadfence();
-        return ok;
-    }
-    // Plain grid barrier; false in a block whose wait failed (the error is
-    // passed on through shared memory, so no block reads the flag again).
+    // Release (thread 0 of the last block, after its completion work and a
+    // __syncthreads if other threads took part in it).
+    __device__ __forceinline__ void release() { st_release_u64(gen, target); }
+    // Wait for the release (thread 0 of the other blocks), bounded.
+    __device__ __forceinline__ bool wait() { return poll(gen); }
+    // Plain grid barrier; false once any block has given up.
     __device__ __forceinline__ bool sync() {
-        __shared__ int s_last, s_ok;
-        const bool last = arrive(&s_last);
-        if (threadIdx.x == 0) {
-            if (last) {
-                release();
-                s_ok = 1;
-            } else {
-                s_ok = wait();
-            }
-        }
-        __syncthreads();
-        return s_ok != 0;
+        count_sync();
+        return ld_volatile_int(err) == 0;
     }
 };
 

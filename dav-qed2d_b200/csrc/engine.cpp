@@ -403,18 +403,30 @@ int qed2d_ctx_get_dims(const qed2d_ctx* ctx, int* L1, int* L2) {
     return QED2D_OK;
 }
 
+// the Ctx::sched slot of a solver selector, -1 for none
+static int sched_slot(int solver) {
+    switch (solver) {
+        case QED2D_PREC_F64: return 0;
+        case QED2D_PREC_MIXED: return 1;
+        case QED2D_MULTISHIFT: return 2;
+        default: return -1;
+    }
+}
+
 int qed2d_ctx_set_schedule(qed2d_ctx* ctx, int precision, int schedule) {
     QCTX(ctx);
-    if (precision != QED2D_PREC_F64 && precision != QED2D_PREC_MIXED) return bad_arg("schedule: F64 or MIXED only");
+    const int slot = sched_slot(precision);
+    if (slot < 0) return bad_arg("schedule: QED2D_PREC_F64, QED2D_PREC_MIXED or QED2D_MULTISHIFT only");
     if (schedule < -1 || schedule > 2) return bad_arg("schedule must be -1, 0, 1 or 2");
-    c.sched[precision == QED2D_PREC_F64 ? 0 : 1] = schedule;
+    c.sched[slot] = schedule;
     return QED2D_OK;
 }
 
 int qed2d_ctx_get_schedule(const qed2d_ctx* ctx, int precision, int* schedule) {
     if (!ctx || !schedule) return bad_arg("context or schedule is NULL");
-    if (precision != QED2D_PREC_F64 && precision != QED2D_PREC_MIXED) return bad_arg("schedule: F64 or MIXED only");
-    *schedule = ctx->c.sched[precision == QED2D_PREC_F64 ? 0 : 1];
+    const int slot = sched_slot(precision);
+    if (slot < 0) return bad_arg("schedule: QED2D_PREC_F64, QED2D_PREC_MIXED or QED2D_MULTISHIFT only");
+    *schedule = ctx->c.sched[slot];
     return QED2D_OK;
 }
 

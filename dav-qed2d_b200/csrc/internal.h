@@ -52,7 +52,7 @@ struct Ctx {
     int64_t last_iters = 0;
     int64_t last_updates = 0;
     double last_relres = 0.0;
-    int sched[2] = {-1, -1};     // reduction schedule of the F64 / MIXED solvers (-1: not tuned yet)
+    int sched[3] = {-1, -1, -1};   // reduction schedule of the F64 / MIXED / multishift solvers (-1: not tuned yet)
 
     void* buf(const std::string& name, size_t bytes);   // grow-only named workspace
     double2* spinor(const std::string& name) { return (double2*)buf(name, sizeof(double2) * 2 * g.V); }

@@ -291,14 +291,15 @@ def CG(so, U, si, am0, *args, so_as_guess=False):
     raise TypeError("CG: unsupported argument list")
 
 
-_PRECS = {"f64": _lib.PREC_F64, "mixed": _lib.PREC_MIXED}
+_PRECS = {"f64": _lib.PREC_F64, "mixed": _lib.PREC_MIXED, "multishift": _lib.MULTISHIFT}
 
 
 def set_schedule(prm: LattParm, schedule: int, precision="mixed") -> None:
-    """Fix the persistent solver's reduction schedule on this lattice's context:
+    """Fix a persistent solver's reduction schedule on this lattice's context:
     0 (last block publishes the sums), 1 (every block sums), 2 (one
     thread-block cluster, small lattices), or -1 to tune again on the next
-    solve.  0 and 1 give the same bits."""
+    solve.  0 and 1 give the same bits.  `precision` selects the solver:
+    "f64" or "mixed" (CG), "multishift" (the RHMC shifted solves)."""
     check(lib().qed2d_ctx_set_schedule(_c(prm), _PRECS[precision], int(schedule)), "set_schedule")
 
 

@@ -13,6 +13,7 @@ MAXPOLES = 32
 NOALLOC_MAX_SITES = 16384
 OK, NOT_CONVERGED, TIMEOUT, BAD_ARG, CUDA_ERR, NO_MEMORY, UNSUPPORTED = range(7)
 PREC_F64, PREC_MIXED, PREC_PLAIN = 0, 1, 2
+MULTISHIFT = 3   # schedule selector of the multishift solver (QED2D_MULTISHIFT)
 LEAPFROG, OMF4 = 0, 1
 STREAM_MOMENTA, STREAM_METROPOLIS, STREAM_POWER, STREAM_NOISE, STREAM_REWEIGHT = 1, 3, 4, 16, 64
 

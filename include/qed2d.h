@@ -100,16 +100,19 @@ int qed2d_ctx_set_beta(qed2d_ctx* ctx, double beta);
 int qed2d_ctx_set_stream(qed2d_ctx* ctx, void* cuda_stream);
 int qed2d_ctx_set_precision(qed2d_ctx* ctx, int precision);
 int qed2d_ctx_get_dims(const qed2d_ctx* ctx, int* L1, int* L2);
-/* Reduction schedule of the persistent F64 / MIXED solvers: 0 = the last block
- * to reach a grid barrier sums the partials and publishes them, 1 = every block
- * sums them itself, 2 = the whole solve in one thread-block cluster with the
- * hardware cluster barrier (lattices of at most 128 tiles of 32x8 sites).  0 and
- * 1 give the same bits; 2 uses fewer blocks, so its sums are grouped
- * differently.  The first solve of each precision on a context times the
- * candidates and keeps the fastest (a host synchronisation; QED2D_TUNE=0 in the
+/* Reduction schedule of a persistent solver, selected by `precision`:
+ * QED2D_PREC_F64 or QED2D_PREC_MIXED (qed2d_cg and the HMC solves), or
+ * QED2D_MULTISHIFT (qed2d_multishift_cg and the RHMC solves).  0 = the last
+ * block to reach a grid barrier sums the partials and publishes them, 1 = every
+ * block sums them itself, 2 = the whole solve in one thread-block cluster with
+ * the hardware cluster barrier (lattices of at most 128 tiles of 32x8 sites).
+ * 0 and 1 give the same bits; 2 uses fewer blocks, so its sums are grouped
+ * differently.  The first solve of each kind on a context times the candidates
+ * and keeps the fastest (a host synchronisation; QED2D_TUNE=0 in the
  * environment selects a fixed size rule instead).  set: 0, 1 or 2 to fix it
  * (2 falls back to 1 where no cluster fits), -1 to tune again on the next
  * solve; get: -1 while untuned. */
+#define QED2D_MULTISHIFT 3   /* schedule selector of the multishift solver (FP64) */
 int qed2d_ctx_set_schedule(qed2d_ctx* ctx, int precision, int schedule);
 int qed2d_ctx_get_schedule(const qed2d_ctx* ctx, int precision, int* schedule);
 /* iterations, final |r|^2/|b|^2 and (QED2D_PREC_MIXED) FP64 reliable updates of

@@ -268,3 +268,39 @@ def test_cluster_schedule_matches_grid_schedule(L1, L2, prec):
     finally:
         qed2d.set_schedule(prm, -1, prec)
         qed2d.set_precision("f64")
+
+
+@pytest.mark.parametrize("L1,L2", [(32, 32), (64, 64), (128, 128), (256, 128)])
+def test_multishift_schedules(L1, L2):
+    """The multishift solver runs under the same reduction schedules as the CG:
+    the first solve tunes it; 0 and 1 give identical bits; 2 (one thread-block
+    cluster, lattices of at most 128 tiles; 256x128 falls back to the grid)
+    agrees to the solver's accuracy.  Every shift is checked against its own
+    residual."""
+    import qed2d
+    prm = qed2d.LattParm((L1, L2), 4.0)
+    U, src = to_dev(hot_links(L1, L2, 25)), to_dev(cgauss(L1, L2, 26, 2))
+    am0, mus = 0.15, [0.02, 0.1, 0.4, 1.5, 6.0, 20.0]
+    try:
+        qed2d.set_schedule(prm, -1, "multishift")
+        xs = [qed2d.cfield(L1, L2) for _ in mus]
+        qed2d.multishift_CG(xs, U, src, am0, mus, 20000, 1e-24, prm)
+        assert qed2d.get_schedule(prm, "multishift") in (0, 1, 2)
+        out = {}
+        for sched in (0, 1, 2):
+            qed2d.set_schedule(prm, sched, "multishift")
+            xs = [qed2d.cfield(L1, L2) for _ in mus]
+            it = qed2d.multishift_CG(xs, U, src, am0, mus, 20000, 1e-24, prm)
+            out[sched] = (it, [to_host(x) for x in xs])
+        assert out[0][0] == out[1][0]
+        for a, b in zip(out[0][1], out[1][1]):
+            assert np.array_equal(a, b)
+        assert abs(out[2][0] - out[1][0]) <= 2
+        for a, b in zip(out[2][1], out[1][1]):
+            assert rel(a, b) < 1e-9
+        y, b = qed2d.cfield(L1, L2), to_host(src)
+        for mu, x in zip(mus, out[1][1]):   # (A + mu^2) x = src
+            qed2d.gamm5Dw_sqr_musq(y, None, U, to_dev(x), am0, mu, prm)
+            assert rel(to_host(y), b) < 1e-9, mu
+    finally:
+        qed2d.set_schedule(prm, -1, "multishift")
