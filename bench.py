@@ -238,8 +238,9 @@ def run_configs(qed2d, torch, dev):
     rp = [qed2d.get_rhmc_params(12, np.sqrt(0.9 * lmin), np.sqrt(1.1 * lmax))]
     st3 = lambda: qed2d.HMC_(U3, [0.1], 0.05, 20, [], MAXITER, TOL, p3, None, rp)
     st3()
-    out["C3_rhmc_128_12_poles"] = {"value": timed(st3, 3), "unit": "traj/s", "solver": "FP64 multi-shift, one launch for all poles",
-                                   "trajectories": 3}
+    out["C3_rhmc_128_12_poles"] = {"value": timed(st3, 10), "unit": "traj/s", "solver": "FP64 multi-shift, one launch for all poles",
+                                   "solver_schedule": names.get(qed2d.get_schedule(p3, "multishift"), "untuned"),
+                                   "trajectories": 10}
     del U, U2, U3
     # C5
     p5 = qed2d.LattParm((8192, 8192), 11.25)
@@ -409,11 +410,15 @@ def run_ours(args):
     traffic = V * sum(its) * U_DRAM_PER_SITE_ITER
     roofline = {"kernel": "k_u_cg_mixed", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                "schedule": {0: "last block publishes the sums", 1: "every block sums"}.get(batch.schedule, "untuned"),
+                "dram_achieved": traffic / t_k / 1e9, "dram_frac": traffic / t_k / 1e9 / peak,
+                "schedule": {0: "last block publishes the sums", 1: "every block sums",
+                             4: "independent replicas (a barrier per replica)"}.get(batch.schedule, "untuned"),
                 "note": f"one launch = one solve of all {B} replicas: per replica iterations {min(its)}-{max(its)} "
                         f"x {B_MIXED_ITER:.0f} B/site + reliable updates {min(upd)}-{max(upd)} x "
-                        f"{B_MIXED_UPDATE:.0f} B/site; {B} x {L}^2 working set partly L2-resident; traffic = ncu DRAM bytes per site-iteration at this size "
-                        f"x the solve's site-iterations"}
+                        f"{B_MIXED_UPDATE:.0f} B/site; {B} x {L}^2 working set partly L2-resident, so achieved "
+                        f"(algorithmic bytes) can exceed the copy bandwidth; traffic = ncu DRAM bytes per "
+                        f"site-iteration at this size x the solve's site-iterations, dram_achieved = traffic / time "
+                        f"(the kernel is latency-bound)"}
 
     # --- single-chain baselines on the same field and draws as replica 0's first
     # timed step: mixed (no batching), fused FP64, and the plain FP64 GPU path

@@ -794,7 +794,7 @@ struct qed2d_batch {
     int* d_cnt = nullptr;           // [nrep + 1]: per-replica counters, then the flag accumulator
     bool shared_state = false;      // records in shared memory (nrep <= kSharedReps)
     bool uniform = false;           // equal sizes, nrep <= kUniformReps: k_u_cg_mixed
-    int usched = -1;                // its reduction schedule (-1: not tuned yet)
+    int usched = -1;                // its schedule: 0, 1 (grid reductions), 4 (independent replicas); -1 untuned
     int rsched = -1;                // uneven batches: 2 grid solver, 3 one cluster per replica (-1: not tuned)
     int rcs = 8;                    // blocks per cluster of the cluster solver (tuned)
     int* d_order = nullptr;         // [nrep] replicas by decreasing size (cluster solver)
@@ -802,6 +802,7 @@ struct qed2d_batch {
     int ugrid = 0, ubpr = 0, uper_block = 0;
     double* d_upart = nullptr;      // [2][ubpr * nrep]
     double* d_ured = nullptr;       // [2][nrep]
+    unsigned long long* d_ubar = nullptr;   // [nrep][16] per-replica barrier counters (schedule 4)
     int* d_out = nullptr;           // [2][nrep]: iterations, reliable updates of the last solve
     long long* d_iters = nullptr;   // [nrep] iterations accumulated over a trajectory
     double* d_sums = nullptr;       // [2][nrep][5] start / end sums of a trajectory
@@ -861,14 +862,18 @@ int r_pack(qed2d_batch* h, double2* U, const double* mom, double eps, float4* U3
     return r_post("k_r_updt");
 }
 
-// First solve of an equal-size batch: time both reduction schedules of
-// k_u_cg_mixed (same bits) on the caller's operator and sources, capped at 24
-// iterations, into scratch outputs, and keep the faster; the device control
-// block is saved and restored around it.  QED2D_TUNE=0: every block sums.
+// First solve of an equal-size batch: time the schedules of k_u_cg_mixed
+// (same bits) on the caller's operator and sources, capped at 24 iterations,
+// into scratch outputs, and keep the fastest; the device control block is saved
+// and restored around it.  Independent replicas (4) are a candidate from two
+// replicas up (with one they are schedule 1).  QED2D_TUNE=0: the size rule
+// measured on B200 instead -- independent replicas from two replicas up
+// (schedule 1 -> 4 per iteration: 2 x 512^2 23.1 -> 20.2 us, 4 x 512^2 39.1 ->
+// 30.8 us, 32 x 64^2 28.8 -> 9.8 us), every block sums for one.
 template <class Launch>
 int tune_uniform(qed2d_batch* h, const UCGP& Q, int maxiter, Launch launch) {
     if (!tuning_enabled()) {
-        h->usched = 1;
+        h->usched = h->nrep >= 2 ? 4 : 1;
         return QED2D_OK;
     }
     DevCtl saved;
@@ -882,12 +887,14 @@ int tune_uniform(qed2d_batch* h, const UCGP& Q, int maxiter, Launch launch) {
     cudaEvent_t e0, e1;
     QCHECK(cudaEventCreate(&e0));
     QCHECK(cudaEventCreate(&e1));
-    float tbest[2] = {1e30f, 1e30f};
+    constexpr int cand[3] = {0, 1, 4};
+    const int ncand = h->nrep >= 2 ? 3 : 2;
+    float tbest[3] = {1e30f, 1e30f, 1e30f};
     int st = QED2D_OK;
     for (int rep = 0; rep < 3 && st == QED2D_OK; rep++)
-        for (int rs = 0; rs < 2 && st == QED2D_OK; rs++) {
+        for (int rs = 0; rs < ncand && st == QED2D_OK; rs++) {
             cudaEventRecord(e0, h->stream);
-            st = launch(rs, T);
+            st = launch(cand[rs], T);
             cudaEventRecord(e1, h->stream);
             if (cudaEventSynchronize(e1) != cudaSuccess) st = cuda_status(cudaGetLastError(), "schedule tuning");
             float ms = 0.f;
@@ -899,7 +906,10 @@ int tune_uniform(qed2d_batch* h, const UCGP& Q, int maxiter, Launch launch) {
     QCHECK(cudaMemcpyAsync(h->ctl, &saved, sizeof(DevCtl), cudaMemcpyHostToDevice, h->stream));
     QCHECK(cudaStreamSynchronize(h->stream));
     if (st != QED2D_OK) return st;
-    h->usched = tbest[1] <= tbest[0] ? 1 : 0;
+    int best = 1;
+    for (int i = 0; i < ncand; i++)
+        if (tbest[i] < tbest[best]) best = i;
+    h->usched = cand[best];
     return QED2D_OK;
 }
 
@@ -1056,12 +1066,16 @@ int r_solve(qed2d_batch* h, const double2* U, const float4* U32, const double2* 
         Q.ctl = h->ctl;
         Q.part = h->d_upart;
         Q.red = h->d_ured;
+        Q.rbar = h->d_ubar;
         Q.st_out = h->d_st;
-        auto launch = [&](int rs, const UCGP& q) -> int {
+        auto launch = [&](int sched, const UCGP& q) -> int {
             QCHECK(cudaMemsetAsync(&h->ctl->bar, 0, 2 * sizeof(unsigned long long) + sizeof(int), h->stream));
+            if (sched == 4) QCHECK(cudaMemsetAsync(h->d_ubar, 0, sizeof(unsigned long long) * 16 * h->nrep, h->stream));
             void* uargs[] = {(void*)&q};
-            QCHECK(cudaLaunchCooperativeKernel(rs ? (const void*)k_u_cg_mixed<1> : (const void*)k_u_cg_mixed<0>,
-                                               dim3((unsigned)h->ugrid), dim3(TILE), uargs, 0, h->stream));
+            const void* kern = sched == 4   ? (const void*)k_u_cg_mixed<2>
+                               : sched == 1 ? (const void*)k_u_cg_mixed<1>
+                                            : (const void*)k_u_cg_mixed<0>;
+            QCHECK(cudaLaunchCooperativeKernel(kern, dim3((unsigned)h->ugrid), dim3(TILE), uargs, 0, h->stream));
             count_launch();
             return QED2D_OK;
         };
@@ -1207,9 +1221,11 @@ int batch_setup(qed2d_batch* h, const int* L1, const int* L2, const double* beta
     if (same) {
         int per_smu = 0;
         int per_smu1 = 0;
+        int per_smu2 = 0;
         QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_smu, k_u_cg_mixed<0>, TILE, 0));
         QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_smu1, k_u_cg_mixed<1>, TILE, 0));
-        per_smu = std::min(per_smu, per_smu1);
+        QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_smu2, k_u_cg_mixed<2>, TILE, 0));
+        per_smu = std::min(per_smu, std::min(per_smu1, per_smu2));
         const long long maxgu = std::min<long long>((long long)per_smu * h->num_sms, kMaxPartBlocks);
         const RepInfo& R0 = h->reps[0];
         if (per_smu >= 1 && maxgu / B >= 1) {
@@ -1250,6 +1266,7 @@ int batch_setup(qed2d_batch* h, const int* L1, const int* L2, const double* beta
     if (h->uniform) {
         QCHECK(cudaMalloc(&h->d_upart, sizeof(double) * 2 * (size_t)h->ugrid));
         QCHECK(cudaMalloc(&h->d_ured, sizeof(double) * 2 * B));
+        QCHECK(cudaMalloc(&h->d_ubar, sizeof(unsigned long long) * 16 * B));
     }
     QCHECK(cudaMalloc(&h->d_out, sizeof(int) * 2 * B));
     QCHECK(cudaMalloc(&h->d_iters, sizeof(long long) * B));
@@ -1318,9 +1335,10 @@ int qed2d_batch_destroy(qed2d_batch* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     else cudaDeviceSynchronize();
     for (auto& kv : h->ws) cudaFree(kv.second.first);
-    void* dev[] = {h->d_reps, h->d_tiles, h->d_seg0, h->d_segs, h->d_order, h->d_rep_seg, h->d_dbase_c, h->d_dbase_r, h->d_m2,
-                   h->d_beta, h->d_seed,  h->d_st, h->d_flags, h->d_red, h->d_cnt, h->d_upart, h->d_ured,      h->d_out,     h->d_iters,   h->d_sums,
-                   h->d_tpart, h->d_part, h->ctl};
+    void* dev[] = {h->d_reps,  h->d_tiles, h->d_seg0,  h->d_segs,  h->d_order, h->d_rep_seg, h->d_dbase_c,
+                   h->d_dbase_r, h->d_m2,  h->d_beta,  h->d_seed,  h->d_st,    h->d_flags,   h->d_red,
+                   h->d_cnt,   h->d_upart, h->d_ured,  h->d_ubar,  h->d_out,   h->d_iters,   h->d_sums,
+                   h->d_tpart, h->d_part,  h->ctl};
     for (void* p : dev)
         if (p) cudaFree(p);
     if (h->ctl_host) cudaFreeHost(h->ctl_host);
@@ -1335,10 +1353,10 @@ int qed2d_batch_set_stream(qed2d_batch* h, void* stream) {
 }
 
 int qed2d_batch_set_schedule(qed2d_batch* h, int schedule) {
-    const bool ok = h && (schedule == -1 || (h->uniform ? (schedule == 0 || schedule == 1)
+    const bool ok = h && (schedule == -1 || (h->uniform ? (schedule == 0 || schedule == 1 || schedule == 4)
                                                          : (schedule == 2 || schedule == 3)));
     if (!ok) {
-        set_error("qed2d_batch_set_schedule: -1, or 0/1 (equal sizes, at most 64 replicas), or 2/3 (otherwise)");
+        set_error("qed2d_batch_set_schedule: -1, or 0/1/4 (equal sizes, at most 64 replicas), or 2/3 (otherwise)");
         return QED2D_ERR_BAD_ARG;
     }
     if (h->uniform) h->usched = schedule;

@@ -4,10 +4,13 @@
 // Block b serves replica b / bpr only, and a contiguous range of that
 // replica's tiles, so every block's geometry, masses and pointers are kernel
 // constants and a phase starts without any loads.  Each replica's partials are
-// summed in a fixed order (deterministic) under one of two schedules (ureduce),
-// and every block runs the per-replica CG scalar recurrences itself in shared
-// memory.  Replicas that have converged
-// stop working but keep joining the barriers until all are done.  The
+// summed in a fixed order (deterministic) under one of three schedules
+// (ureduce), and the blocks run the per-replica CG scalar recurrences
+// themselves in shared memory.  Under the grid schedules (RS = 0, 1) all
+// replicas pass the same barriers, and replicas that have converged stop
+// working but keep joining them until all are done; under RS = 2 each replica
+// has its own barrier, so one replica's wait overlaps another's work on the
+// same SMs, and a converged replica's blocks leave.  The
 // recurrences are those of the ragged kernel (rep_step) and of the
 // single-lattice mixed solver.
 //
@@ -42,6 +45,7 @@ struct UCGP {
     DevCtl* ctl;
     double* part;       // [2][bpr * B] block partials (alternating)
     double* red;        // [2][B] published per-replica sums (RS = 0)
+    unsigned long long* rbar;   // [B][16] per-replica barrier counters, one 128-byte line each (RS = 2)
     RepState* st_out;   // [B] final records
 };
 
@@ -61,17 +65,21 @@ __device__ __forceinline__ Site usite_at(const UGeom& g, int r, int t1, int t2, 
 }
 
 // Barrier with one sum per replica (one warp per replica over its blocks'
-// partials, fixed order).  Two schedules give the same bits: RS = 0, the last
+// partials, fixed order).  Three schedules give the same bits: RS = 0, the last
 // block to arrive sums and publishes red[] before releasing and every block
 // reads red[]; RS = 1, a counter barrier, then every block sums the partials
-// itself.  Then every block runs every replica's recurrences for
-// reduction `kind` on its shared records and flags.  A failed or timed-out
-// wait is passed on through shared memory.
+// itself; then every block runs every replica's recurrences for reduction
+// `kind` on its shared records and flags.  RS = 2 (independent replicas): gs is
+// the barrier of this block's replica alone (its own counter, its bpr blocks),
+// the block sums its replica's partials and runs that replica's recurrences
+// only, and its flags are that replica's.  A failed or timed-out wait is passed
+// on through shared memory.
 template <int RS>
 __device__ __forceinline__ bool ureduce(GridSync& gs, double v, const UCGP& P, double* smem, RepState* s_st,
                                         int* s_fl, int kind, int k) {
     __shared__ int s_last, s_bits, s_ok;
     __shared__ double s_red[kUniformReps];
+    const int myr = RS == 2 ? blockIdx.x / P.bpr : 0;
     const int buf = gs.nred++ & 1;
     double* part = P.part + (size_t)buf * P.bpr * P.g.B;
     double* red = P.red + (size_t)buf * P.g.B;
@@ -82,8 +90,14 @@ __device__ __forceinline__ bool ureduce(GridSync& gs, double v, const UCGP& P, d
         s_bits = 0;
     }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    // the replicas whose sums this block needs: all of them, or (RS = 2) its own.
+    // RS = 2 goes through the same loop shapes as RS = 1 on purpose: a
+    // single-replica copy of them (warp 0 sums, thread myr steps) compiled to
+    // code whose barrier waits took 50% longer (one replica of 512^2: 25.0
+    // against 16.9 us per iteration, same arithmetic).
+    const int r0 = RS == 2 ? myr : 0, r1 = RS == 2 ? myr + 1 : P.g.B;
     auto sum_partials = [&](double* out) {
-        for (int r = warp; r < P.g.B; r += nw) {
+        for (int r = r0 + warp; r < r1; r += nw) {
             double s = 0.0;
             for (int i = lane; i < P.bpr; i += 32) s += __ldcg(part + (size_t)r * P.bpr + i);
 #pragma unroll
@@ -111,7 +125,7 @@ __device__ __forceinline__ bool ureduce(GridSync& gs, double v, const UCGP& P, d
     }
     __syncthreads();
     int fl[FL_N] = {0, 0, 0};
-    if (threadIdx.x < P.g.B) {
+    if ((int)threadIdx.x >= r0 && (int)threadIdx.x < r1) {
         RepState st = s_st[threadIdx.x];
         rep_step(st, kind, s_red[threadIdx.x], k, P.eps, P.delta2, P.maxiter, fl);
         s_st[threadIdx.x] = st;
@@ -264,8 +278,20 @@ __global__ void __launch_bounds__(TILE, 4) k_u_cg_mixed(const UCGP P) {
     __shared__ int s_fl[FL_N];
     if (threadIdx.x < FL_N) s_fl[threadIdx.x] = 0;
     __syncthreads();
-    GridSync gs{&P.ctl->bar, &P.ctl->gen, &P.ctl->err};
     int k = 0;
+    if constexpr (RS == 2) {   // independent replicas: a barrier per replica; its blocks leave when it is done
+        const int myr = blockIdx.x / P.bpr;
+        GridSync gs{P.rbar + 16 * myr, &P.ctl->gen, &P.ctl->err, (unsigned)P.bpr};
+        const bool ok = u_body<RS>(P, gs, k, smem, s_st, s_fl);
+        if (blockIdx.x == myr * P.bpr && threadIdx.x == 0) {   // the replica's first block
+            if (ok) P.st_out[myr] = s_st[myr];
+            DevCtl* c = P.ctl;
+            if (myr == 0) c->last_iters = k;
+            if (ld_volatile_int(&c->err) || !ok) atomicCAS(&c->status, 0, QED2D_ERR_TIMEOUT);
+        }
+        return;
+    }
+    GridSync gs{&P.ctl->bar, &P.ctl->gen, &P.ctl->err};
     const bool ok = u_body<RS>(P, gs, k, smem, s_st, s_fl);
     if (blockIdx.x == 0) {
         if (ok)   // every block holds the same records: block 0 stores them

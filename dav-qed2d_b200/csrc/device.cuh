@@ -119,13 +119,15 @@ __device__ __forceinline__ void normal_pair(uint64_t seed, uint32_t stream, uint
 // __syncthreads, with release semantics: the block's earlier writes, by any of
 // its threads, are ordered before its arrival.  Two ways to leave:
 //  * count_sync: thread 0 polls `arrivals` with acquire loads until it reaches
-//    the barrier's target (gridDim.x per barrier so far), then the block
+//    the barrier's target (n() per barrier so far), then the block
 //    follows through a __syncthreads.  One fire-and-forget add and one poll per
 //    block: the short path;
 //  * arrive / release / wait: the block whose add sees target-1 arrived last; it
 //    does the barrier's completion work (e.g. the final sum of a reduction) and
 //    publishes the barrier's generation in `gen` (release), the others poll
 //    `gen` (acquire).
+// A group of the grid (e.g. the blocks of one replica) can have a barrier of its
+// own: its own counter, and `members` = its number of blocks.
 // The adds of all blocks form one chain of atomic updates of `arrivals`, so an
 // acquire that sees the final count is ordered after every block's release.
 // No sequentially-consistent fence (__threadfence) is needed on either path.
@@ -157,8 +159,11 @@ struct GridSync {
     unsigned long long* arrivals;
     unsigned long long* gen;
     int* err;
+    unsigned members = 0;   // blocks taking part (a group of the grid with its own counter); 0: the grid
     unsigned long long target = 0;
     int nred = 0;   // reductions done so far: selects the double-buffered partials/results
+
+    __device__ __forceinline__ unsigned n() const { return members ? members : gridDim.x; }
 
     // Poll *c (acquire) until it reaches target, bounded.  False when the wait
     // ended on the error flag or timed out.
@@ -178,7 +183,7 @@ struct GridSync {
     // which the caller reads.
     __device__ __forceinline__ void count_sync() {
         __syncthreads();
-        target += gridDim.x;
+        target += n();
         if (threadIdx.x == 0) {
             red_release_add_u64(arrivals, 1ULL);
             poll(arrivals);
@@ -189,7 +194,7 @@ struct GridSync {
     // block, whose threads are then ordered after every block's arrival.
     __device__ __forceinline__ bool arrive(int* s_last) {
         __syncthreads();
-        target += gridDim.x;
+        target += n();
         if (threadIdx.x == 0) {
             const unsigned long long old = atom_acq_rel_add_u64(arrivals, 1ULL);
             *s_last = old == target - 1;

@@ -626,7 +626,8 @@ class Batch:
     @property
     def schedule(self) -> int:
         """Schedule of the batched solver: -1 untuned; equal-size batches of at
-        most 64 replicas 0/1 (reduction schedules, same bits); other batches 2
+        most 64 replicas 0/1 (reduction schedules) or 4 (independent replicas,
+        a barrier per replica), all three with the same bits; other batches 2
         (one launch with grid barriers) or 3 (one thread-block cluster per replica)."""
         v = C.c_int(0)
         check(lib().qed2d_batch_get_schedule(self.h, C.byref(v)), "batch_get_schedule")

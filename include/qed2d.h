@@ -276,11 +276,13 @@ int qed2d_batch_layout(const qed2d_batch* batch, int64_t* site_offsets);
 int qed2d_batch_destroy(qed2d_batch* batch);
 int qed2d_batch_set_stream(qed2d_batch* batch, void* cuda_stream);
 /* the batched solver's schedule.  Equal-size batches of at most 64 replicas: 0/1
- * as qed2d_ctx_set_schedule (same bits).  Other batches: 2 = one launch over all
- * replicas with grid barriers, 3 = one thread-block cluster per replica (no
- * grid barrier; replicas stream through the GPU, largest first); these group
- * their sums differently.  The first solve times the candidates and keeps the
- * faster; -1 = tune again on the next solve (get: -1 while untuned). */
+ * as qed2d_ctx_set_schedule, 4 = independent replicas (each replica's blocks
+ * have a barrier of their own and leave when it has converged); 0, 1 and 4 give
+ * the same bits.  Other batches: 2 = one launch over all replicas with grid
+ * barriers, 3 = one thread-block cluster per replica (no grid barrier; replicas
+ * stream through the GPU, largest first); these group their sums differently.
+ * The first solve times the candidates and keeps the fastest; -1 = tune again
+ * on the next solve (get: -1 while untuned). */
 int qed2d_batch_set_schedule(qed2d_batch* batch, int schedule);
 int qed2d_batch_get_schedule(const qed2d_batch* batch, int* schedule);
 /* every replica's CG method 1 (src/QED2dSolver.jl:3-46) in one launch:

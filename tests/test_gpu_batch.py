@@ -182,8 +182,10 @@ def test_many_replicas_global_state_cg():
 
 
 def test_batch_reduction_schedules_give_identical_bits():
-    """Equal-size batches: both reduction schedules of the batched solver give
-    bitwise identical solutions; the first solve tunes the schedule."""
+    """Equal-size batches: the three schedules of the batched solver (two grid
+    reduction schedules; independent replicas with a barrier each, whose blocks
+    leave as their replica converges) give bitwise identical solutions and
+    per-replica iteration counts; the first solve tunes the schedule."""
     import qed2d
     nrep, L1, L2 = 3, 64, 48
     b = qed2d.Batch(nrep, L1, L2, 4.0)
@@ -194,14 +196,16 @@ def test_batch_reduction_schedules_give_identical_bits():
         src[r] = to_dev(cgauss(L1, L2, 50 + r, 2))
     x = b.field()
     b.cg(x, U, src, [0.2, 0.3, 0.25], 20000, 1e-24)
-    assert b.schedule in (0, 1)
+    assert b.schedule in (0, 1, 4)
     res = []
-    for sched in (0, 1):
+    for sched in (0, 1, 4):
         b.schedule = sched
         x = b.field()
         its, _ = b.cg(x, U, src, [0.2, 0.3, 0.25], 20000, 1e-24)
-        res.append((its, to_host(x)))
-    assert res[0][0] == res[1][0] and np.array_equal(res[0][1], res[1][1])
+        res.append((list(its), to_host(x)))
+    assert len(set(res[0][0])) == 3   # the replicas converge at different iterations
+    for i in (1, 2):
+        assert res[0][0] == res[i][0] and np.array_equal(res[0][1], res[i][1])
     assert qed2d.Batch.ragged([(16, 16), (32, 8)], [4.0, 4.0]).schedule == -1
 
 
@@ -244,3 +248,23 @@ def test_ragged_cluster_solver_matches_grid_solver(nrep):
                  qed2d.gamm5Dw_sqr_msq, prm, None)
         assert rel(to_host(b.replica(x2, r)), to_host(xs)) < 1e-9, r
     qed2d.set_precision("f64")
+
+
+def test_independent_replica_schedule_trajectories():
+    """Batched Nf=2 trajectories under the grid schedule (1) and the independent-
+    replica schedule (4) from the same start: identical dH, iterations and links."""
+    import qed2d
+    nrep, L = 4, 64
+    out = []
+    for sched in (1, 4):
+        b = qed2d.Batch(nrep, L, L, 4.0)
+        b.schedule = sched
+        U = b.field()
+        for r in range(nrep):
+            U[r] = to_dev(hot_links(L, L, 70 + r))
+        seeds = [900 + r for r in range(nrep)]
+        am0 = [0.1 + 0.05 * r for r in range(nrep)]   # replicas converge at different iterations
+        infos = [b.hmc_nf2(U, am0, 0.1, 5, 20000, 1e-24, seeds, c) for c in (0, 1)]
+        out.append(([(i.dH, i.cg_iterations) for inf in infos for i in inf], to_host(U)))
+    assert out[0][0] == out[1][0]
+    assert np.array_equal(out[0][1], out[1][1])
