@@ -963,15 +963,26 @@ int launch_replica_clusters(qed2d_batch* h, const CCGP& cc, int cs) {
 // launch over all replicas with grid barriers) and the cluster solver
 // (k_rc_cg_mixed, one cluster of 4, 8 or 16 blocks per replica), capped at 24
 // iterations into scratch outputs, and keep the fastest; the control block is
-// saved and restored.  QED2D_TUNE=0: the grid solver.  The solvers group their
-// sums differently (same accuracy, not the same bits).
+// saved and restored.  QED2D_TUNE=0: the size rule measured on B200 instead --
+// clusters of 8 blocks where they fit (grid -> clusters per solve: 6 replicas of
+// 8..96 x 4..40 sites 1.83 -> 0.49 ms, 32 of 32^2..128^2 4.30 -> 1.40 ms, 128 of
+// 32^2..256^2 19.7 -> 11.9 ms, the 512-replica ensemble 46.1 -> 30.3 ms), else
+// the grid solver.  The solvers group their sums differently (same accuracy, not
+// the same bits).
 template <class Launch>
 int tune_ragged(qed2d_batch* h, const RCGP& P, const CCGP& C, int maxiter, Launch launch) {
     h->rsched = 2;
-    if (!tuning_enabled()) return QED2D_OK;
     std::vector<int> cand = {0};   // 0: grid solver; cs > 0: clusters of cs blocks
     for (int cs : kClusterSizes)
         if (cluster_fits(cs, replica_cluster_kernel(cs))) cand.push_back(cs);
+    if (!tuning_enabled()) {
+        for (int cs : cand)
+            if (cs == 8) {
+                h->rsched = 3;
+                h->rcs = 8;
+            }
+        return QED2D_OK;
+    }
     if (cand.size() == 1) return QED2D_OK;
     DevCtl saved;
     QCHECK(cudaMemcpyAsync(&saved, h->ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, h->stream));
