@@ -1045,7 +1045,7 @@ int r_solve(qed2d_batch* h, const double2* U, const float4* U32, const double2* 
     P.x32 = h->field32("b_x32");
     if (!P.r64 || !P.r32 || !P.q0 || !P.q1 || !P.t32 || !P.x32) return QED2D_ERR_NO_MEMORY;
     P.eps = eps;
-    P.delta2 = 0.05 * 0.05;
+    P.delta2 = kReliableDelta * kReliableDelta;
     P.maxiter = maxiter;
     P.st = h->d_st;
     P.flags = h->d_flags;

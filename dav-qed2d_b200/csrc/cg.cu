@@ -842,7 +842,7 @@ int cg_solve(Ctx& c, const SolveArgs& a, int precision) {
     P.guess = a.guess ? 1 : 0;
     P.ctl = c.ctl;
     P.part = c.part;
-    P.delta2 = 0.05 * 0.05;
+    P.delta2 = kReliableDelta * kReliableDelta;
     if (precision == QED2D_PREC_F64) {
         P.p0 = c.spinor("cg_p0");
         P.p1 = c.spinor("cg_p1");
