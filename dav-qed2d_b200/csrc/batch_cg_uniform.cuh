@@ -166,6 +166,14 @@ __device__ __forceinline__ bool u_body(const UCGP& P, GridSync& gs, int& k, doub
     const Pair<double> z{make_double2(0, 0), make_double2(0, 0)};
     const Pair<float> zf{make_float2(0, 0), make_float2(0, 0)};
     int cur = 0;
+    // x32 += alpha p is applied every second iteration, for two directions at
+    // once: while `pend`, the update of the previous iteration (alpha `apend`,
+    // direction in the buffer that the next phase A reads as p_old) is still to
+    // be added.  Same operations in the same order as one update per iteration,
+    // so the same bits; x32 and one direction are read and x32 written half as
+    // often (192 -> 176 algorithmic bytes per site-iteration).
+    bool pend = false;
+    float apend = 0.f;
 
     {   // |b|^2 per replica; x = 0
         double v = 0.0;
@@ -215,32 +223,53 @@ __device__ __forceinline__ bool u_body(const UCGP& P, GridSync& gs, int& k, doub
             const RepState st = s_st[myr];
             if (st.act) {
                 const float alpha = (float)st.alpha;
-                FOR_MY_UTILES(q) {
-                    const Pair<float> pc = SpF{qn}.ld(q.x);
-                    const Pair<float> a = g5dw_at<float>(SpF{P.t32}, Lf, q, m2f);
-                    Pair<float> xv = SpF{P.x32}.ld(q.x), r = SpF{P.r32}.ld(q.x);
-                    xv.a = xv.a + alpha * pc.a;
-                    xv.b = xv.b + alpha * pc.b;
-                    r.a = r.a - alpha * a.a;
-                    r.b = r.b - alpha * a.b;
-                    st_f(P.x32, q.x, xv);
-                    st_f(P.r32, q.x, r);
-                    f += norm2(r.a) + norm2(r.b);
+                if (pend) {
+                    FOR_MY_UTILES(q) {   // x += apend p_old, then x += alpha p
+                        const Pair<float> po = SpF{qo}.ld(q.x), pc = SpF{qn}.ld(q.x);
+                        const Pair<float> a = g5dw_at<float>(SpF{P.t32}, Lf, q, m2f);
+                        Pair<float> xv = SpF{P.x32}.ld(q.x), r = SpF{P.r32}.ld(q.x);
+                        xv.a = xv.a + apend * po.a;
+                        xv.b = xv.b + apend * po.b;
+                        xv.a = xv.a + alpha * pc.a;
+                        xv.b = xv.b + alpha * pc.b;
+                        r.a = r.a - alpha * a.a;
+                        r.b = r.b - alpha * a.b;
+                        st_f(P.x32, q.x, xv);
+                        st_f(P.r32, q.x, r);
+                        f += norm2(r.a) + norm2(r.b);
+                    }
+                } else {
+                    FOR_MY_UTILES(q) {   // x's update waits for the next iteration
+                        const Pair<float> a = g5dw_at<float>(SpF{P.t32}, Lf, q, m2f);
+                        Pair<float> r = SpF{P.r32}.ld(q.x);
+                        r.a = r.a - alpha * a.a;
+                        r.b = r.b - alpha * a.b;
+                        st_f(P.r32, q.x, r);
+                        f += norm2(r.a) + norm2(r.b);
+                    }
                 }
+                apend = alpha;
+                pend = !pend;
             }
             if (!ureduce<RS>(gs, (double)f, P, smem, s_st, s_fl, RED_RN, k)) return false;
         }
         if (s_fl[FL_UPD]) {   // FP64 reliable update of the replicas that asked for one
             const RepState st = s_st[myr];
             const double inv_s = 1.0 / st.s;
-            if (st.upd) FOR_MY_UTILES(q) {   // x += x32 / s
-                    const Pair<float> d = SpF{P.x32}.ld(q.x);
+            if (st.upd) FOR_MY_UTILES(q) {   // x += x32 / s, with this iteration's x32 update if it waits
+                    Pair<float> d = SpF{P.x32}.ld(q.x);
+                    if (pend) {
+                        const Pair<float> pc = SpF{qn}.ld(q.x);
+                        d.a = d.a + apend * pc.a;
+                        d.b = d.b + apend * pc.b;
+                    }
                     Pair<double> xv = SpD{xx, V}.ld(q.x);
                     xv.a = xv.a + inv_s * to_d(d.a);
                     xv.b = xv.b + inv_s * to_d(d.b);
                     st_d(xx, V, q.x, xv);
                     st_f(P.x32, q.x, zf);
                 }
+            if (st.upd) pend = false;
             if (!gs.sync()) return false;
             if (st.upd) FOR_MY_UTILES(q) st_d(t64, V, q.x, g5dw_at<double>(SpD{xx, V}, L, q, m2));
             if (!gs.sync()) return false;
