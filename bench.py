@@ -49,9 +49,9 @@ B_F64_ITER = 384.0       # FP64 fused iteration: phase A 160 B + phase B 224 B
 B_DSLASH_F64 = 96.0      # g5Dw apply, FP64: spinor in 32 + links 32 + out 32
 B_DSLASH_C64 = 48.0      # g5Dw apply on complex64 fields: spinor in 16 + links 16 + out 16
 # DRAM bytes (read + write) per site-iteration of k_u_cg_mixed at 4 x 512^2, from an
-# ncu capture of one 100-iteration launch (8.773 GB over 1,048,576 sites x 100);
+# ncu capture of one 100-iteration launch (6.400 GB over 1,048,576 sites x 100);
 # traffic grows in proportion to the iterations at fixed size
-U_DRAM_PER_SITE_ITER = 83.7
+U_DRAM_PER_SITE_ITER = 61.0
 ENS_NS, ENS_EPS = 10, 0.1   # replica ensemble: leapfrog ns=10, eps=0.1
 
 

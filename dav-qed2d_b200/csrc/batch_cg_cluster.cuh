@@ -91,6 +91,8 @@ __device__ __forceinline__ void c_body(const CCGP& P, int r, int& k, double* sme
     const Pair<double> z{make_double2(0, 0), make_double2(0, 0)};
     const Pair<float> zf{make_float2(0, 0), make_float2(0, 0)};
     int cur = 0, nred = 0;
+    bool pend = false;   // x32 += alpha p every second iteration, as in k_u_cg_mixed (same bits)
+    float apend = 0.f;
 #define FOR_MY_CTILES(q) FOR_RANGE(q, g, TR)
     {   // |b|^2; x = 0
         double v = 0.0;
@@ -133,33 +135,54 @@ __device__ __forceinline__ void c_body(const CCGP& P, int r, int& k, double* sme
             }
             cluster_step(S, RED_PAP, cluster_sum<CS>((double)f, smem, s_slot, nred), k, P);
         }
-        {   // x += alpha p, r -= alpha g5Dw t
+        {   // x += alpha p (every second iteration, for two directions), r -= alpha g5Dw t
             float f = 0.f;
             const float alpha = (float)S->alpha;
-            FOR_MY_CTILES(q) {
-                const Pair<float> pc = SpF{qn}.ld(q.x);
-                const Pair<float> a = g5dw_at<float>(SpF{t32}, Lf, q, m2f);
-                Pair<float> xv = SpF{x32}.ld(q.x), rv = SpF{r32}.ld(q.x);
-                xv.a = xv.a + alpha * pc.a;
-                xv.b = xv.b + alpha * pc.b;
-                rv.a = rv.a - alpha * a.a;
-                rv.b = rv.b - alpha * a.b;
-                st_f(x32, q.x, xv);
-                st_f(r32, q.x, rv);
-                f += norm2(rv.a) + norm2(rv.b);
+            if (pend) {
+                FOR_MY_CTILES(q) {
+                    const Pair<float> po = SpF{qo}.ld(q.x), pc = SpF{qn}.ld(q.x);
+                    const Pair<float> a = g5dw_at<float>(SpF{t32}, Lf, q, m2f);
+                    Pair<float> xv = SpF{x32}.ld(q.x), rv = SpF{r32}.ld(q.x);
+                    xv.a = xv.a + apend * po.a;
+                    xv.b = xv.b + apend * po.b;
+                    xv.a = xv.a + alpha * pc.a;
+                    xv.b = xv.b + alpha * pc.b;
+                    rv.a = rv.a - alpha * a.a;
+                    rv.b = rv.b - alpha * a.b;
+                    st_f(x32, q.x, xv);
+                    st_f(r32, q.x, rv);
+                    f += norm2(rv.a) + norm2(rv.b);
+                }
+            } else {
+                FOR_MY_CTILES(q) {
+                    const Pair<float> a = g5dw_at<float>(SpF{t32}, Lf, q, m2f);
+                    Pair<float> rv = SpF{r32}.ld(q.x);
+                    rv.a = rv.a - alpha * a.a;
+                    rv.b = rv.b - alpha * a.b;
+                    st_f(r32, q.x, rv);
+                    f += norm2(rv.a) + norm2(rv.b);
+                }
             }
+            apend = alpha;
+            pend = !pend;
             cluster_step(S, RED_RN, cluster_sum<CS>((double)f, smem, s_slot, nred), k, P);
         }
         if (S->upd) {   // FP64 reliable update
             const double inv_s = 1.0 / S->s;
-            FOR_MY_CTILES(q) {   // x += x32 / s
-                const Pair<float> d = SpF{x32}.ld(q.x);
+            FOR_MY_CTILES(q) {   // x += x32 / s, with this iteration's x32 update if it waits
+                Pair<float> d = SpF{x32}.ld(q.x);
+                if (pend) {
+                    const Pair<float> pc = SpF{qn}.ld(q.x);
+                    d.a = d.a + apend * pc.a;
+                    d.b = d.b + apend * pc.b;
+                }
                 Pair<double> xv = SpD{xx, V}.ld(q.x);
                 xv.a = xv.a + inv_s * to_d(d.a);
                 xv.b = xv.b + inv_s * to_d(d.b);
                 st_d(xx, V, q.x, xv);
                 st_f(x32, q.x, zf);
             }
+            pend = false;
             cgr::this_cluster().sync();
             FOR_MY_CTILES(q) st_d(t64, V, q.x, g5dw_at<double>(SpD{xx, V}, L, q, m2));
             cgr::this_cluster().sync();
