@@ -41,8 +41,9 @@ WORKLOAD = (f"Nf=2 HMC trajectory, {L}x{L}, beta={BETA}, m0={AM0}, leapfrog ns={
             f"CG to |r|/|b|<1e-12 (eps=1e-24)")
 THERM_TRAJ = 10
 # algorithmic bytes per site of the solver phases (FP32 packed spinors and links)
-B_MIXED_ITER = 192.0     # FP32 fused iteration: phase A 80 B + phase B 112 B
-B_U_MIXED_ITER = 176.0   # the same in k_u_cg_mixed, which updates x every second iteration: phase B 64 / 128 B
+# FP32 fused iteration: phase A 80 B + phase B 96 B on average -- the mixed solvers
+# update x every second iteration for two directions (phase B 64 B, then 128 B)
+B_MIXED_ITER = 176.0
 B_MIXED_UPDATE = 400.0   # one FP64 reliable update (4 phases)
 B_MIXED_SETUP = 112.0    # |b|^2, x=0, r32 = b/|b|, x32 = 0
 B_F64_ITER = 384.0       # FP64 fused iteration: phase A 160 B + phase B 224 B
@@ -406,7 +407,7 @@ def run_ours(args):
         kern.append((a0.elapsed_time(a1) / 1e3, its, upd))
     t_k, its, upd = min(kern[1:], key=lambda z: z[0])
     V = L * L
-    bytes_k = V * sum(B_MIXED_SETUP + i * B_U_MIXED_ITER + u * B_MIXED_UPDATE for i, u in zip(its, upd))
+    bytes_k = V * sum(B_MIXED_SETUP + i * B_MIXED_ITER + u * B_MIXED_UPDATE for i, u in zip(its, upd))
     achieved = bytes_k / t_k / 1e9
     traffic = V * sum(its) * U_DRAM_PER_SITE_ITER
     roofline = {"kernel": "k_u_cg_mixed", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -415,7 +416,7 @@ def run_ours(args):
                 "schedule": {0: "last block publishes the sums", 1: "every block sums",
                              4: "independent replicas (a barrier per replica)"}.get(batch.schedule, "untuned"),
                 "note": f"one launch = one solve of all {B} replicas: per replica iterations {min(its)}-{max(its)} "
-                        f"x {B_U_MIXED_ITER:.0f} B/site + reliable updates {min(upd)}-{max(upd)} x "
+                        f"x {B_MIXED_ITER:.0f} B/site + reliable updates {min(upd)}-{max(upd)} x "
                         f"{B_MIXED_UPDATE:.0f} B/site; {B} x {L}^2 working set partly L2-resident, so achieved "
                         f"(algorithmic bytes) can exceed the copy bandwidth; traffic = ncu DRAM bytes per "
                         f"site-iteration at this size x the solve's site-iterations, dram_achieved = traffic / time "
