@@ -838,7 +838,7 @@ static int time_schedules(Ctx& c, Launch launch, int ncand, int* best) {
             if (cudaEventSynchronize(e1) != cudaSuccess) st = cuda_status(cudaGetLastError(), "schedule tuning");
             float ms = 0.f;
             cudaEventElapsedTime(&ms, e0, e1);
-            if (rep > 0 && tbest[rs] < 2e30f) tbest[rs] = std::min(tbest[rs], ms);   // round 0 warms up
+            if (rep > 0 && tbest[rs] < 2e30f) tbest[rs] = std::min(tbest[rs], ms);   // the first repetition warms up
         }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
