@@ -268,3 +268,60 @@ def test_independent_replica_schedule_trajectories():
         out.append(([(i.dH, i.cg_iterations) for inf in infos for i in inf], to_host(U)))
     assert out[0][0] == out[1][0]
     assert np.array_equal(out[0][1], out[1][1])
+
+
+@pytest.mark.parametrize("maxiter", [7, 8])
+def test_capped_solves_agree_across_solvers(maxiter):
+    """A solve capped at `maxiter` iterations returns the FP64 iterate x_k of
+    every mixed solver: the single-lattice solver with one x update per iteration
+    (one-cluster schedule) and with the update deferred to every second iteration
+    for two directions (grid schedule), the equal-size batched solver under its
+    schedules, and both uneven-batch solvers.  The cap forces a final reliable
+    update, which has to fold a deferred update in (odd and even caps); a lost one
+    would move x by alpha_k p_k, orders of magnitude above the FP32 spread
+    between the solvers."""
+    import qed2d
+    L, am0 = 64, 0.15
+    prm = qed2d.LattParm((L, L), 4.0)
+    U, b = to_dev(hot_links(L, L, 81)), to_dev(cgauss(L, L, 82, 2))
+
+    def capped(fn):
+        try:
+            fn()
+        except qed2d.Qed2dError:
+            pass   # not converged at the cap, as intended
+
+    ref = {}
+    qed2d.set_precision("mixed")
+    try:
+        for sched in (2, 1):
+            qed2d.set_schedule(prm, sched, "mixed")
+            x = qed2d.cfield(L, L)
+            capped(lambda: qed2d.CG(x, U, b, am0, maxiter, 1e-24, qed2d.gamm5Dw_sqr_msq, prm, None))
+            ref[sched] = to_host(x)
+    finally:
+        qed2d.set_schedule(prm, -1, "mixed")
+        qed2d.set_precision("f64")
+    assert np.abs(ref[2]).max() > 0
+    assert rel(ref[1], ref[2]) < 1e-4
+    bt = qed2d.Batch(2, L, L, 4.0)
+    Ub, bb = bt.field(), bt.field()
+    for r in range(2):
+        Ub[r], bb[r] = U, b
+    for sched in (1, 4):
+        bt.schedule = sched
+        x = bt.field()
+        capped(lambda: bt.cg(x, Ub, bb, [am0, am0], maxiter, 1e-24))
+        for r in range(2):
+            assert rel(to_host(x[r]), ref[2]) < 1e-4, (sched, r)
+    rb = qed2d.Batch.ragged([(L, L), (32, 32)], [4.0, 4.0])
+    Ur, br = rb.field(), rb.field()
+    rb.replica(Ur, 0).copy_(U)
+    rb.replica(br, 0).copy_(b)
+    rb.replica(Ur, 1).copy_(to_dev(hot_links(32, 32, 83)))
+    rb.replica(br, 1).copy_(to_dev(cgauss(32, 32, 84, 2)))
+    for sched in (2, 3):
+        rb.schedule = sched
+        x = rb.field()
+        capped(lambda: rb.cg(x, Ur, br, [am0, am0], maxiter, 1e-24))
+        assert rel(to_host(rb.replica(x, 0)), ref[2]) < 1e-4, sched
