@@ -259,6 +259,14 @@ __global__ void __launch_bounds__(TILE, 3) k_cg_f64(const CGP P) {
             rr = bb;
         }
         double beta = 0.0;
+        // x += alpha p every second iteration, for two directions at once (the
+        // same operations in the same order, so the same bits); an update still
+        // waiting when the loop ends is added after it.  Grid schedules only, as
+        // in the mixed solver.
+        constexpr bool kPair = RS != 2;
+        bool pend = false;
+        double apend = 0.0;
+        const double2* plast = nullptr;   // the direction of the waiting update
         for (k = 1; k <= P.maxiter; k++) {
             double2* pn = (k & 1) ? P.p0 : P.p1;
             const double2* po = (k & 1) ? P.p1 : P.p0;
@@ -274,18 +282,38 @@ __global__ void __launch_bounds__(TILE, 3) k_cg_f64(const CGP P) {
             if (!reduce_sync<1, RS>(gs, v, P.part, P.ctl->red, smem)) goto done;
             const double alpha = rr / v[0];
             v[0] = 0.0;
-            FOR_TILES(q) {
-                const Pair<double> pc = SpD{pn, V}.ld(q.x);
-                const Pair<double> a = g5dw_at<double>(SpD{P.t, V}, L, q, m2);
-                Pair<double> xv = SpD{P.x, V}.ld(q.x), r = SpD{P.r, V}.ld(q.x);
-                xv.a = xv.a + alpha * pc.a;
-                xv.b = xv.b + alpha * pc.b;
-                r.a = r.a - alpha * (a.a + mu2 * pc.a);
-                r.b = r.b - alpha * (a.b + mu2 * pc.b);
-                st_d(P.x, V, q.x, xv);
-                st_d(P.r, V, q.x, r);
-                v[0] += norm2(r.a) + norm2(r.b);
+            if (!kPair || pend) {
+                FOR_TILES(q) {
+                    const Pair<double> pc = SpD{pn, V}.ld(q.x);
+                    const Pair<double> a = g5dw_at<double>(SpD{P.t, V}, L, q, m2);
+                    Pair<double> xv = SpD{P.x, V}.ld(q.x), r = SpD{P.r, V}.ld(q.x);
+                    if (kPair) {   // the previous iteration's update first
+                        const Pair<double> pp = SpD{po, V}.ld(q.x);
+                        xv.a = xv.a + apend * pp.a;
+                        xv.b = xv.b + apend * pp.b;
+                    }
+                    xv.a = xv.a + alpha * pc.a;
+                    xv.b = xv.b + alpha * pc.b;
+                    r.a = r.a - alpha * (a.a + mu2 * pc.a);
+                    r.b = r.b - alpha * (a.b + mu2 * pc.b);
+                    st_d(P.x, V, q.x, xv);
+                    st_d(P.r, V, q.x, r);
+                    v[0] += norm2(r.a) + norm2(r.b);
+                }
+            } else {
+                FOR_TILES(q) {   // x's update waits for the next iteration
+                    const Pair<double> pc = SpD{pn, V}.ld(q.x);
+                    const Pair<double> a = g5dw_at<double>(SpD{P.t, V}, L, q, m2);
+                    Pair<double> r = SpD{P.r, V}.ld(q.x);
+                    r.a = r.a - alpha * (a.a + mu2 * pc.a);
+                    r.b = r.b - alpha * (a.b + mu2 * pc.b);
+                    st_d(P.r, V, q.x, r);
+                    v[0] += norm2(r.a) + norm2(r.b);
+                }
             }
+            apend = alpha;
+            plast = pn;
+            pend = kPair && !pend;
             if (!reduce_sync<1, RS>(gs, v, P.part, P.ctl->red, smem)) goto done;
             const double rn = v[0];
             if (rn < tol) { rr = rn; conv = true; break; }
@@ -293,6 +321,16 @@ __global__ void __launch_bounds__(TILE, 3) k_cg_f64(const CGP P) {
             rr = rn;
         }
         if (!conv) k = P.maxiter;
+        if (pend) {   // the update still waiting (each block its own sites)
+            FOR_TILES(q) {
+                const Pair<double> pc = SpD{plast, V}.ld(q.x);
+                Pair<double> xv = SpD{P.x, V}.ld(q.x);
+                xv.a = xv.a + apend * pc.a;
+                xv.b = xv.b + apend * pc.b;
+                st_d(P.x, V, q.x, xv);
+            }
+            if (P.g5x && !gs.sync()) goto done;   // the epilogue's stencil reads other blocks' x
+        }
     }
 epilogue:
     if (P.g5x) FOR_TILES(q) st_d(P.g5x, V, q.x, g5dw_at<double>(SpD{P.x, V}, L, q, m2));
