@@ -749,6 +749,27 @@ static int reset_barrier(Ctx& c) {   // bar, gen and err are contiguous
     return QED2D_OK;
 }
 
+// Self-test of the bounded barrier wait: thread 0 of a one-block launch arrives
+// at a barrier of two members whose second never comes and polls with the
+// caller's (small) limit, so the wait gives up exactly as a persistent kernel's
+// barrier does when a block never arrives: QED2D_ERR_TIMEOUT in err and status.
+__global__ void k_barrier_timeout_probe(DevCtl* c, unsigned long long limit) {
+    if (threadIdx.x != 0) return;
+    GridSync gs{&c->bar, &c->gen, &c->err, 2u};
+    gs.target = 2;
+    red_release_add_u64(gs.arrivals, 1ULL);
+    if (!gs.poll(gs.arrivals, limit) && c->status == 0)
+        c->status = ld_volatile_int(&c->err) ? QED2D_ERR_TIMEOUT : QED2D_ERR_CUDA;
+}
+
+int barrier_timeout_probe(Ctx& c, long long polls) {
+    QTRY(reset_barrier(c));
+    k_barrier_timeout_probe<<<1, 32, 0, c.stream>>>(c.ctl, (unsigned long long)polls);
+    count_launch();
+    QCHECK(cudaGetLastError());
+    return QED2D_OK;
+}
+
 template <class K, class Par>
 static int launch_coop(Ctx& c, K kernel, Par P) {
     int grid = 0;
@@ -808,6 +829,7 @@ static int launch_cluster(Ctx& c, void (*kernel)(Par), Par P) {
     const long long nt = num_tiles(c.g);
     P.per_block = (int)((nt + grid - 1) / grid);
     grid = (int)((nt + P.per_block - 1) / P.per_block);   // no block without tiles
+    QTRY(reset_barrier(c));   // no barrier here, but the epilogue reads err: clear one a timeout left
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(TILE);

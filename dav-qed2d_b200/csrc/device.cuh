@@ -165,13 +165,13 @@ struct GridSync {
 
     __device__ __forceinline__ unsigned n() const { return members ? members : gridDim.x; }
 
-    // Poll *c (acquire) until it reaches target, bounded.  False when the wait
-    // ended on the error flag or timed out.
-    __device__ __forceinline__ bool poll(const unsigned long long* c) {
+    // Poll *c (acquire) until it reaches target, at most `limit` times.  False
+    // when the wait ended on the error flag or timed out.
+    __device__ __forceinline__ bool poll(const unsigned long long* c, unsigned long long limit = 1ULL << 26) {
         unsigned long long polls = 0;
         while (ld_acquire_u64(c) < target) {
             if (ld_volatile_int(err) != 0) return false;
-            if (++polls > (1ULL << 26)) {
+            if (++polls > limit) {
                 atomicExch(err, 2 /* QED2D_ERR_TIMEOUT */);
                 return false;
             }

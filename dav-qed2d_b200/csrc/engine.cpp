@@ -430,6 +430,14 @@ int qed2d_ctx_get_schedule(const qed2d_ctx* ctx, int precision, int* schedule) {
     return QED2D_OK;
 }
 
+int qed2d_selftest_barrier_timeout(qed2d_ctx* ctx, int64_t polls) {
+    QCTX(ctx);
+    if (polls < 1 || polls > (1LL << 26)) return bad_arg("polls must be in [1, 2^26]");
+    QTRY(reset_seq(c));
+    QTRY(barrier_timeout_probe(c, (long long)polls));
+    return finish_seq(c, nullptr);
+}
+
 int qed2d_last_solve(const qed2d_ctx* ctx, int64_t* iterations, double* rel, int64_t* reliable_updates) {
     if (!ctx) return bad_arg("context is NULL");
     if (iterations) *iterations = ctx->c.last_iters;

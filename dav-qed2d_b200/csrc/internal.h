@@ -85,6 +85,9 @@ void count_launch(int n = 1);
 // solvers need the same iterations (122) at 0.02 and 0.05 alike.
 constexpr double kReliableDelta = 0.01;
 
+// launches the bounded-wait self-test kernel (cg.cu); the status lands in ctl->status
+int barrier_timeout_probe(Ctx& c, long long polls);
+
 bool tuning_enabled();   // QED2D_TUNE=0 in the environment turns schedule tuning off
 int64_t launches();
 

@@ -50,6 +50,7 @@ SIGNATURES = {
     "qed2d_ctx_set_schedule": (I, [P, I, I]),
     "qed2d_ctx_get_schedule": (I, [P, I, PI]),
     "qed2d_last_solve": (I, [P, PI64, PD, PI64]),
+    "qed2d_selftest_barrier_timeout": (I, [P, I64]),
     "qed2d_status_string": (C.c_char_p, [I]),
     "qed2d_last_error": (C.c_char_p, []),
     "qed2d_launch_count": (I64, []),

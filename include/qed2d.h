@@ -115,6 +115,12 @@ int qed2d_ctx_get_dims(const qed2d_ctx* ctx, int* L1, int* L2);
 #define QED2D_MULTISHIFT 3   /* schedule selector of the multishift solver (FP64) */
 int qed2d_ctx_set_schedule(qed2d_ctx* ctx, int precision, int schedule);
 int qed2d_ctx_get_schedule(const qed2d_ctx* ctx, int precision, int* schedule);
+/* Self-test of failure detection (no counterpart in the reference): runs one
+ * kernel whose grid-barrier wait can never complete, with the wait bounded to
+ * `polls` polls (1..2^26) instead of the solvers' 2^26.  The wait gives up as a
+ * solver's barrier does when a block never arrives, and the call returns
+ * QED2D_ERR_TIMEOUT; the context stays usable for the next call. */
+int qed2d_selftest_barrier_timeout(qed2d_ctx* ctx, int64_t polls);
 /* iterations, final |r|^2/|b|^2 and (QED2D_PREC_MIXED) FP64 reliable updates of
  * the most recent solve on this context; any pointer may be NULL */
 int qed2d_last_solve(const qed2d_ctx* ctx, int64_t* iterations, double* rel_residual_sq,
