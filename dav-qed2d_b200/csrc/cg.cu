@@ -861,9 +861,11 @@ static bool cluster_possible(Ctx& c, int slot) {
     return (slot == 0 ? cluster_grid(c, k_cg_f64<2>, &g) : cluster_grid(c, k_cg_mixed<2>, &g)) == QED2D_OK;
 }
 
-// Schedule tuning.  The reduction schedules of reduce_sync give the same bits
-// (RS = 2 only changes the number of blocks, and is tried only for lattices that
-// fit one cluster), so the choice changes only the time.  The first solve of each
+// Schedule tuning.  The grid reduction schedules RS = 0 and RS = 1 give the same
+// bits.  RS = 2 (one cluster, tried only for lattices that fit one) runs fewer
+// blocks than the cooperative grid, so its partial sums are grouped differently
+// and its results agree with the others only to the solver's accuracy; exact-bit
+// comparisons must fix the schedule.  The first solve of each
 // precision on a context times both on the caller's operator and source,
 // capped at kTuneIters iterations, into scratch outputs, and keeps the faster;
 // the device control block is saved before and restored after, so counters and
@@ -1176,10 +1178,14 @@ namespace qed2d {
 //
 // Set-up: the first call on a device looks up the array's device address with
 // cudaGetSymbolAddress (this can also load the library's device code) and caches
-// it per device; make that first call before any stream capture.  Every call
+// it per device; make that first call before any stream capture.  The cached
+// address belongs to the device context it was looked up in: a caller that ends
+// that context with cudaDeviceReset must not call this entry point on that
+// device again in the same process (the address would be stale).  Every call
 // shares the one array, so calls that overlap on the GPU (two streams, two host
-// threads) race; serialise them.  The control block is zeroed by each call; the
-// vectors are always written before they are read.
+// threads) race; serialise them.  Each call synchronises its stream before it
+// returns.  The control block is zeroed by each call; the vectors are always
+// written before they are read.
 namespace {
 constexpr size_t kNaCtlBytes = 512;
 constexpr size_t kNaPartBytes = sizeof(double) * kMaxPartVals * kMaxPartBlocks;
@@ -1235,9 +1241,9 @@ extern "C" int qed2d_cg_noalloc(int L1, int L2, double* so, const double* U, con
         return QED2D_ERR_BAD_ARG;
     }
     const size_t fb = sizeof(double2) * 2 * (size_t)V;
-    const char *a = (const char*)so, *b = (const char*)si;
-    if (a < b + fb && b < a + fb) {
-        set_error("qed2d_cg_noalloc: so aliases si");
+    const char *a = (const char*)so, *b = (const char*)si, *u = (const char*)U;
+    if ((a < b + fb && b < a + fb) || (a < u + fb && u < a + fb)) {
+        set_error("qed2d_cg_noalloc: so aliases si or U");
         return QED2D_ERR_BAD_ARG;
     }
     void* base = nullptr;

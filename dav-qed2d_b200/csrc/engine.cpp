@@ -483,6 +483,7 @@ int qed2d_gamm5dw(qed2d_ctx* ctx, double* so, const double* U, const double* si,
     QPTR(U);
     QPTR(si);
     QTRY(check_out(c, so, si, "gamm5Dw"));
+    QTRY(check_out(c, so, U, "gamm5Dw"));
     return launch_g5dw(c, C2(so), C2(U), C2(si), am0, nullptr, make_double2(0, 0), false);
 }
 
@@ -492,7 +493,8 @@ int qed2d_gamm5dw_c64(qed2d_ctx* ctx, float* so, const float* U, const float* si
     QPTR(U);
     QPTR(si);
     const size_t nb = sizeof(float2) * 2 * (size_t)c.g.V;
-    if (overlap(so, nb, si, nb)) return bad_arg("gamm5Dw (complex64): output aliases an input");
+    if (overlap(so, nb, si, nb) || overlap(so, nb, U, nb))
+        return bad_arg("gamm5Dw (complex64): output aliases an input");
     return launch_g5dw_c64(c, reinterpret_cast<float2*>(so), reinterpret_cast<const float2*>(U),
                            reinterpret_cast<const float2*>(si), am0);
 }
@@ -510,6 +512,7 @@ int qed2d_dw(qed2d_ctx* ctx, double* so, const double* U, const double* si, doub
     QPTR(U);
     QPTR(si);
     QTRY(check_out(c, so, si, "Dw"));
+    QTRY(check_out(c, so, U, "Dw"));
     return launch_g5dw(c, C2(so), C2(U), C2(si), am0, nullptr, make_double2(0, 0), true);
 }
 
@@ -519,6 +522,7 @@ int qed2d_gamm5dw_sqr(qed2d_ctx* ctx, double* so, const double* U, const double*
     QPTR(U);
     QPTR(si);
     QTRY(check_out(c, so, si, "gamm5Dw_sqr"));
+    QTRY(check_out(c, so, U, "gamm5Dw_sqr"));
     return op_sqr(c, C2(so), C2(U), C2(si), am0, 0.0);
 }
 
@@ -528,6 +532,7 @@ int qed2d_gamm5dw_sqr_musq(qed2d_ctx* ctx, double* so, const double* U, const do
     QPTR(U);
     QPTR(si);
     QTRY(check_out(c, so, si, "gamm5Dw_sqr_musq"));
+    QTRY(check_out(c, so, U, "gamm5Dw_sqr_musq"));
     return op_sqr(c, C2(so), C2(U), C2(si), am0, mu);
 }
 
@@ -537,6 +542,7 @@ int qed2d_gamm5dw_sqr_sqr(qed2d_ctx* ctx, double* so, const double* U, const dou
     QPTR(U);
     QPTR(si);
     QTRY(check_out(c, so, si, "gamm5Dw_sqr_sqr"));
+    QTRY(check_out(c, so, U, "gamm5Dw_sqr_sqr"));
     double2* t = c.spinor("op_t2");
     if (!t) return QED2D_ERR_NO_MEMORY;
     QTRY(op_sqr(c, t, C2(U), C2(si), am0, 0.0));
@@ -550,6 +556,7 @@ int qed2d_gamm5dw_sqr_sqr_musq(qed2d_ctx* ctx, double* so, const double* U, cons
     QPTR(U);
     QPTR(si);
     QTRY(check_out(c, so, si, "gamm5Dw_sqr_sqr_musq"));
+    QTRY(check_out(c, so, U, "gamm5Dw_sqr_sqr_musq"));
     double2* t = c.spinor("op_t2");
     double2* t3 = c.spinor("op_t3");
     if (!t || !t3) return QED2D_ERR_NO_MEMORY;
@@ -661,6 +668,7 @@ int qed2d_cg(qed2d_ctx* ctx, double* so, const double* U, const double* si, doub
     QPTR(U);
     QPTR(si);
     QTRY(check_out(c, so, si, "CG"));
+    QTRY(check_out(c, so, U, "CG"));
     if (maxiter < 0) return bad_arg("maxiter < 0");
     QTRY(reset_seq(c));
     QTRY(solve(c, C2(so), C2(U), C2(si), am0, 0.0, maxiter, eps, false, nullptr));
@@ -676,6 +684,7 @@ int qed2d_cg_shift(qed2d_ctx* ctx, double* so, const double* U, const double* si
     QPTR(U);
     QPTR(si);
     QTRY(check_out(c, so, si, "CG"));
+    QTRY(check_out(c, so, U, "CG"));
     if (maxiter < 0) return bad_arg("maxiter < 0");
     QTRY(reset_seq(c));
     QTRY(solve(c, C2(so), C2(U), C2(si), am0, mu, maxiter, eps, so_as_guess != 0, nullptr));
@@ -695,6 +704,7 @@ int qed2d_multishift_cg(qed2d_ctx* ctx, double* const* so, const double* U, cons
     for (int i = 0; i < n; i++) {
         QTRY(check_ptr(so[i], "so[i]"));
         QTRY(check_out(c, so[i], si, "multishift CG"));
+        QTRY(check_out(c, so[i], U, "multishift CG"));
         xs[i] = C2(so[i]);
         mu2[i] = mu[i] * mu[i];
     }
@@ -725,6 +735,7 @@ int qed2d_multi_cg(qed2d_ctx* ctx, double* so, const double* U, const double* si
     QPTR(si);
     QTRY(check_rhmc(rprm));
     QTRY(check_out(c, so, si, "MultiCG"));
+    QTRY(check_out(c, so, U, "MultiCG"));
     QTRY(reset_seq(c));
     QTRY(multi_cg_core(c, C2(so), C2(U), C2(si), am0, maxiter, eps, rprm, false));
     int64_t it = 0;
@@ -741,6 +752,7 @@ int qed2d_rational(qed2d_ctx* ctx, double* so, const double* U, const double* si
     QPTR(si);
     QTRY(check_rhmc(rprm));
     QTRY(check_out(c, so, si, "R"));
+    QTRY(check_out(c, so, U, "R"));
     QTRY(reset_seq(c));
     QTRY(multi_cg_core(c, C2(so), C2(U), C2(si), am0, maxiter, eps, rprm, true));
     int64_t it = 0;
@@ -757,6 +769,7 @@ int qed2d_generate_pseudofermion(qed2d_ctx* ctx, double* F, const double* U, con
     QPTR(X);
     QTRY(check_rhmc(rprm));
     QTRY(check_out(c, F, X, "generate_pseudofermion!"));
+    QTRY(check_out(c, F, U, "generate_pseudofermion!"));
     QTRY(reset_seq(c));
     QTRY(pf_generate_core(c, C2(F), C2(U), C2(X), am0, maxiter, tol, rprm));
     int64_t it = 0;
@@ -830,6 +843,7 @@ int qed2d_luscher_z(qed2d_ctx* ctx, double* Z, const double* U, const double* Xi
     QPTR(Xin);
     QTRY(check_rhmc(rprm));
     QTRY(check_out(c, Z, Xin, "LuscherZ"));
+    QTRY(check_out(c, Z, U, "LuscherZ"));
     QTRY(reset_seq(c));
     QTRY(luscher_z_core(c, C2(Z), C2(U), C2(Xin), am0, maxiter, tol, rprm));
     return finish_seq(c, nullptr);

@@ -89,3 +89,24 @@ int zolotarev_params(int n, double r_a, double r_b, qed2d_rhmc_params* out) {
 }
 
 }  // namespace qed2d
+
+// Elliptic.K(m) and Jacobi.sn/cn(u, m) of Elliptic.jl, the functions behind the
+// reference's Zolotarev helpers (src/QED2dRHMC.jl:3-5), on the same AGM/Landen
+// restatement as the coefficients above.
+extern "C" int qed2d_ellip_K(double m, double* K) {
+    if (!K || !(m >= 0.0 && m < 1.0)) {
+        qed2d::set_error("ellip_K: need 0 <= m < 1 and a non-NULL output");
+        return QED2D_ERR_BAD_ARG;
+    }
+    *K = qed2d::Elliptic(m).K;
+    return QED2D_OK;
+}
+
+extern "C" int qed2d_ellip_sncn(double u, double m, double* sn, double* cn) {
+    if (!sn || !cn || !(m >= 0.0 && m < 1.0) || !std::isfinite(u)) {
+        qed2d::set_error("ellip_sncn: need 0 <= m < 1, finite u and non-NULL outputs");
+        return QED2D_ERR_BAD_ARG;
+    }
+    qed2d::Elliptic(m).sncn(u, *sn, *cn);
+    return QED2D_OK;
+}

@@ -37,7 +37,8 @@ __all__ = [
     "unfold_fld_", "unfold_reflect_",
     "gamm5Dw", "gamm5Dw_sqr", "gamm5Dw_sqr_msq", "tr_dQwdU", "gamm5Dw_sqr_musq", "gamm5Dw_sqr_sqr_musq",
     "gamm5Dw_sqr_sqr", "gamm5", "Dw", "CG", "save_gauge", "load_gauge", "get_rhmc_params", "power_method",
-    "reweighting_factor", "R", "MultiCG", "generate_pseudofermion_", "plwv", "LuscherZ",
+    "reweighting_factor", "R", "MultiCG", "generate_pseudofermion_", "plwv", "LuscherZ", "LuscherZp",
+    "k", "v", "a_r", "c_r", "mu", "nu", "rho_mu", "rho_nu", "P", "d", "A", "delta", "error",
     "seed", "set_precision", "set_schedule", "get_schedule", "Qed2dError", "cfield", "rfield", "context",
 ]
 
@@ -419,6 +420,118 @@ def get_rhmc_params(n_rhmc, r_a_rhmc, r_b_rhmc, reweighting_N=1, reweighting_Tay
     return r
 
 
+# Zolotarev helpers exported by the reference (src/QED2dRHMC.jl:2-89), written on
+# the library's Elliptic.K and Jacobi sn/cn (the reference calls Elliptic.jl).
+# Host scalars; no device work.
+def _ellip_K(m):
+    K = C.c_double(0)
+    check(lib().qed2d_ellip_K(float(m), C.byref(K)), "Elliptic.K")
+    return K.value
+
+
+def _sncn(u, m):
+    s, c = C.c_double(0), C.c_double(0)
+    check(lib().qed2d_ellip_sncn(float(u), float(m), C.byref(s), C.byref(c)), "Jacobi.sn/cn")
+    return s.value, c.value
+
+
+def k(eps):
+    """k(eps) = sqrt(1 - eps) (:2)."""
+    return math.sqrt(1.0 - eps)
+
+
+def v(n, eps):
+    """v(n, eps) = K(k^2) / (2n + 1) (:3)."""
+    return _ellip_K(k(eps) ** 2) / (2.0 * n + 1.0)
+
+
+def a_r(r, n, eps):
+    """a_r = cn^2 / sn^2 at r v(n, eps) (:4)."""
+    s, c = _sncn(r * v(n, eps), k(eps) ** 2)
+    return c * c / (s * s)
+
+
+def c_r(r, n, eps):
+    """c_r = sn^2 at r v(n, eps) (:5)."""
+    return _sncn(r * v(n, eps), k(eps) ** 2)[0] ** 2
+
+
+def mu(j, n, eps, r_b):
+    """mu_j = r_b sqrt(a_{2j}) (:8)."""
+    return r_b * math.sqrt(a_r(2 * j, n, eps))
+
+
+def nu(j, n, eps, r_b):
+    """nu_j = r_b sqrt(a_{2j-1}) (:9)."""
+    return r_b * math.sqrt(a_r(2 * j - 1, n, eps))
+
+
+def rho_mu(j, k_, l, n, eps, r_b):
+    """Residue of the pole at -mu_j^2, Luscher eq. (3.5) (:11-25)."""
+    if j < k_ or j > l:
+        raise ValueError("j is not between k and l")
+    res = nu(j, n, eps, r_b) ** 2 - mu(j, n, eps, r_b) ** 2
+    for m in range(k_, l + 1):
+        if m != j:
+            res *= (nu(m, n, eps, r_b) ** 2 - mu(j, n, eps, r_b) ** 2) / \
+                   (mu(m, n, eps, r_b) ** 2 - mu(j, n, eps, r_b) ** 2)
+    return res
+
+
+def rho_nu(j, k_, l, n, eps, r_b):
+    """Luscher eq. (3.9) (:27-41)."""
+    if j < k_ or j > l:
+        raise ValueError("j is not between k and l")
+    res = mu(j, n, eps, r_b) - nu(j, n, eps, r_b)
+    for m in range(k_, l + 1):
+        if m != j:
+            res *= (mu(m, n, eps, r_b) - nu(j, n, eps, r_b)) / (nu(m, n, eps, r_b) - nu(j, n, eps, r_b))
+    return res
+
+
+def P(k_, l, n, eps, r_b, Y):
+    """P_{k,l}(Y) = 1 + sum_j rho_j (Y + mu_j^2)^-1, Luscher eq. (3.4) (:43-57); Y a
+    scalar or a square matrix, the result a matrix (the reference also prints it)."""
+    import numpy as np
+    Y = np.atleast_2d(np.asarray(Y, dtype=float))
+    eye = np.eye(Y.shape[1])
+    res = eye.copy()
+    if k_ != 0 and l != 0:
+        for j in range(k_, l + 1):
+            res = res + rho_mu(j, k_, l, n, eps, r_b) * np.linalg.inv(Y + mu(j, n, eps, r_b) ** 2 * eye)
+    return res
+
+
+def d(n, eps):
+    """d(n, eps) (:60-68)."""
+    res = k(eps) ** (2 * n + 1)
+    for i in range(1, 2 * n + 2, 2):
+        res *= c_r(i, n, eps) ** 2
+    return res
+
+
+def delta(n, eps):
+    """Maximal relative error of the approximation (:70)."""
+    dd = d(n, eps)
+    return dd ** 2 / (1 + math.sqrt(1 - dd ** 2)) ** 2
+
+
+def A(n, eps):
+    """Normalisation A(n, eps) (:72-84)."""
+    res = 2 / (1 + math.sqrt(1 - d(n, eps) ** 2))
+    for i in range(1, 2 * n, 2):
+        res *= c_r(i, n, eps)
+    for i in range(2, 2 * n + 1, 2):
+        res *= 1 / c_r(i, n, eps)
+    return res
+
+
+def error(Y, Yapprox):
+    """|1 - sqrt(Y) Yapprox[1]| (:87-89), Yapprox[1] its first element."""
+    import numpy as np
+    return abs(1 - math.sqrt(Y) * np.asarray(Yapprox).flat[0])
+
+
 def MultiCG(so, U, si, am0, maxiter, eps, A, rprm: RHMCParm, prm: LattParm, kprm=None):
     """MultiCG (:281-290)."""
     it = C.c_int(0)
@@ -460,6 +573,14 @@ def LuscherZ(Z, U, X_in, am0, CGmaxiter, CGtol, rprm: RHMCParm, prm: LattParm, k
     rp = rprm.to_c()
     check(lib().qed2d_luscher_z(_c(prm), _cp(Z, prm), _cp(U, prm), _cp(X_in, prm), float(am0), int(CGmaxiter),
                                 float(CGtol), C.byref(rp)), "LuscherZ")
+
+
+def LuscherZp(Z, p: int, U, X_in, am0, CGmaxiter, CGtol, rprm: RHMCParm, prm: LattParm, kprm=None):
+    """LuscherZp (:189-202): Z = ((g5Dw)^2 R^2 - 1)^p X_in, p applications of LuscherZ."""
+    tmp = X_in.clone()
+    for _ in range(int(p)):
+        LuscherZ(Z, U, tmp, am0, CGmaxiter, CGtol, rprm, prm, kprm)
+        tmp.copy_(Z)
 
 
 def reweighting_factor(U, am0, CGmaxiter, CGtol, prm: LattParm, kprm, rprm):

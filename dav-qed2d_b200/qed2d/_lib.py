@@ -80,6 +80,8 @@ SIGNATURES = {
     "qed2d_multishift_cg": (I, [P, PP, P, P, D, PD, I, I, D, PI]),
     "qed2d_cg_noalloc": (I, [I, I, P, P, P, D, I, D, P, PI]),
     "qed2d_get_rhmc_params": (I, [I, D, D, PR]),
+    "qed2d_ellip_K": (I, [D, PD]),
+    "qed2d_ellip_sncn": (I, [D, D, PD, PD]),
     "qed2d_multi_cg": (I, [P, P, P, P, D, I, D, PR, PI]),
     "qed2d_rational": (I, [P, P, P, P, D, I, D, PR, PI]),
     "qed2d_generate_pseudofermion": (I, [P, P, P, P, D, I, D, PR, PI]),

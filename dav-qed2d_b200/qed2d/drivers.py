@@ -12,11 +12,15 @@ its README and extra/*.in).  Outputs:
     in the reference's text format every 100 (hmc-nf2) / 10 (rhmc) trajectories, and
     `--cont n` resumes from checkpoint n (main/hmc-nf2.jl:93-145, main/rhmc.jl:100-160);
   * mc / master-field: `<Run.name>.log` with the per-trajectory lines of HMC!
-    (src/QED2dHMC.jl:53-57) and the measurements.  The reference writes its
-    measurement series to BDIO files (third-party BDIO.jl, not available here);
-    these drivers write the same series as `<Run.name>_plaq.txt` / `_qtop.txt`
-    (mc) or per-site density arrays `<Run.name>_msm<j>_{plaq,qtop}.npy`
-    (master-field) instead.
+    (src/QED2dHMC.jl:53-57) and the measurements, and `<Run.name>.bdio` with the
+    records the reference writes (qed2d/bdio.py; the BDIO container is restated
+    from its published format, byte compatibility with BDIO.jl unverified):
+      1 the input file (ASC_GENERIC), 2 F64LE [L1, L2, beta, n] (n = ntraj for mc,
+      measurements for master-field), then for mc 3 / 4 the plaquette / Q series of
+      the measured trajectories -- written L1 times over, as main/MC.jl:140-152
+      does -- and for master-field, at every measurement, 3 / 4 the per-site
+      plaquette / arg-plaquette densities in rows of fixed i1
+      (main/master_field.jl:105-131); every record long and followed by its MD5.
 """
 import argparse
 import json
@@ -25,6 +29,7 @@ import os
 import random
 import sys
 
+from . import bdio
 from . import io as qio
 
 
@@ -67,8 +72,14 @@ def _config_name(savedir, L1, L2, beta, mass, i):
 
 
 # ---------------------------------------------------------------------------
+def _bdio_title(beta, L1, L2):
+    # the protocol text both drivers give BDIO_open (main/MC.jl:87-88, main/master_field.jl:87-88)
+    return f"Data from Master field simulation in QED [2d]; beta = {_julia(beta)}; {L1} x {L2}"
+
+
 def run_mc(args):
     """main/MC.jl: pure-gauge HMC (OMF4); seeds are fixed to 1234 as in MC.jl:70-71."""
+    import numpy as np
     import torch
 
     import qed2d
@@ -85,6 +96,7 @@ def run_mc(args):
     log.info(f"  MD PARAMETER eps      = {_julia(eps)}")
     log.info(f"  TRAJECTORY tau        = {_julia(eps * ns)}")
     log.info(f"  THERMALIZATION MDU's  = {_julia(eps * ns * nthm)}")
+    fb = bdio.open_run_file(name, s, args.i, _bdio_title(beta, L1, L2), nt)
     U = torch.ones((2, L2, L1), dtype=torch.complex128, device="cuda")   # cold start, MC.jl:119
     acc = []
     for i in range(1, nthm + 1):
@@ -102,10 +114,12 @@ def run_mc(args):
         qt.append(qed2d.Qtop(U, prm))
         log.info(f"   Plaquette: {_julia(pl[-1])}")
         log.info(f"   Qtop:      {_julia(qt[-1])}")
-    with open(name + "_plaq.txt", "w") as fh:
-        fh.writelines(_julia(v) + "\n" for v in pl)
-    with open(name + "_qtop.txt", "w") as fh:
-        fh.writelines(_julia(v) + "\n" for v in qt)
+    for uinfo, series in ((3, pl), (4, qt)):
+        fb.start_record(bdio.BIN_F64LE, uinfo, True)
+        for _ in range(L1):
+            fb.write(np.asarray(series, dtype=np.float64))
+        fb.write_hash()
+    fb.close()
     return pl, qt
 
 
@@ -205,6 +219,15 @@ def run_rhmc(args):
     return U
 
 
+def _err_avg(dfoo):
+    """err_avg (main/master_field.jl:41-56): mean and error of the per-site density
+    dfoo[i1, i2] from its averages over 16 x 16 blocks (std with Bessel's correction / 16)."""
+    import numpy as np
+    l1, l2 = dfoo.shape[0] // 16, dfoo.shape[1] // 16
+    blks = dfoo[:16 * l1, :16 * l2].reshape(16, l1, 16, l2).sum(axis=(1, 3)) / (l1 * l2)
+    return float(blks.mean()), float(blks.std(ddof=1) / 16)
+
+
 # ---------------------------------------------------------------------------
 def run_master_field(args):
     """main/master_field.jl: thermalise 16x16, unfold 2x2 until the target size,
@@ -221,6 +244,7 @@ def run_master_field(args):
     nt, qzero = int(s["HMC"]["ntraj"]), bool(s["HMC"]["Qzero"])
     nmsm = int(s["Run"].get("measurements", 1))
     log = _logger(name + ".log")
+    fb = bdio.open_run_file(name, s, args.i, _bdio_title(beta, Lt1, Lt2), nmsm)
     qed2d.seed(1234)
     l1 = l2 = 16
     U = torch.ones((2, l2, l1), dtype=torch.complex128, device="cuda")
@@ -239,10 +263,18 @@ def run_master_field(args):
     plx = torch.empty((l2, l1), dtype=torch.float64, device="cuda")
 
     def save_msm(j):
-        qed2d.plaquette_(plx, U, prm)
-        np.save(f"{name}_msm{j}_plaq.npy", plx.cpu().numpy())
-        qed2d.qtop_(plx, U, prm)
-        np.save(f"{name}_msm{j}_qtop.npy", plx.cpu().numpy())
+        # rows of fixed i1 (Julia's dfoo[i, :]): the (L2, L1) density transposed
+        for uinfo, kernel in ((3, qed2d.plaquette_), (4, qed2d.qtop_)):
+            kernel(plx, U, prm)
+            dens = plx.cpu().numpy()
+            fb.start_record(bdio.BIN_F64LE, uinfo, True)
+            for i1 in range(l1):
+                fb.write(dens[:, i1])
+            fb.write_hash()
+            if uinfo == 3:
+                pavg, perr = _err_avg(dens.T)
+                log.info(f" MEASUREMENT {j} of {nmsm}")
+                log.info(f"   Plaquette and error: {_julia(pavg)} +/- {_julia(perr)}")
 
     for j in range(1, nmsm + 1):
         save_msm(j)
@@ -250,6 +282,7 @@ def run_master_field(args):
             info = qed2d.HMC_(U, eps, ns, acc, prm, None, qzero=qzero)
             log.info(_hmc_line(info, acc))
     save_msm(nmsm + 1)
+    fb.close()
     return U
 
 

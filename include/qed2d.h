@@ -201,9 +201,11 @@ int qed2d_multishift_cg(qed2d_ctx* ctx, double* const* so, const double* U, cons
  * nothing.  Its scratch is one static device array, held by every GPU that loads
  * the library, sized for at most QED2D_NOALLOC_MAX_SITES = L1*L2 sites (larger
  * lattices are rejected with QED2D_ERR_BAD_ARG).  The first call on a device looks
- * up that array's address (make it before any stream capture).  All calls share
- * the array: calls that overlap on the GPU race.  Work runs on `stream` (NULL:
- * the legacy default stream); the call synchronises it. */
+ * up that array's address (make it before any stream capture) and keeps it for
+ * the process: after a cudaDeviceReset of that device, do not call this entry
+ * point on it again.  All calls share the array: calls that overlap on the GPU
+ * race.  so must not overlap si or U.  Work runs on `stream` (NULL: the legacy
+ * default stream); the call synchronises it. */
 #define QED2D_NOALLOC_MAX_SITES 16384
 int qed2d_cg_noalloc(int L1, int L2, double* so, const double* U, const double* si, double am0, int maxiter,
                      double eps, void* stream, int* iterations);
@@ -211,6 +213,12 @@ int qed2d_cg_noalloc(int L1, int L2, double* so, const double* U, const double* 
 /* ---- RHMC: src/QED2dRHMC.jl ---- */
 /* get_rhmc_params -- :93-110 (host; Zolotarev coefficients) */
 int qed2d_get_rhmc_params(int n, double r_a, double r_b, qed2d_rhmc_params* out);
+/* Elliptic.K(m) and Jacobi.sn(u, m), Jacobi.cn(u, m) of Elliptic.jl -- the
+ * functions the reference's Zolotarev helpers k, v, a_r, c_r, mu, nu, rho_mu, d,
+ * A, delta are written on (src/QED2dRHMC.jl:2-89; calls at :3-5), with the
+ * parameter m = k^2, 0 <= m < 1.  Host only (no device work). */
+int qed2d_ellip_K(double m, double* K);
+int qed2d_ellip_sncn(double u, double m, double* sn, double* cn);
 /* MultiCG -- :281-290: so = (1 + sum_j rho_j ((g5Dw)^2 + mu_j^2)^-1) si */
 int qed2d_multi_cg(qed2d_ctx* ctx, double* so, const double* U, const double* si, double am0, int maxiter,
                    double eps, const qed2d_rhmc_params* rprm, int* iterations);

@@ -16,7 +16,7 @@ LIB = os.path.join(REPO, "dav-qed2d_b200", "lib", "libqed2d.so")
 
 def declared():
     txt = open(HEADER).read()
-    return sorted(set(re.findall(r"\b(qed2d_[a-z0-9_]+)\s*\(", txt)))
+    return sorted(set(re.findall(r"\b(qed2d_[A-Za-z0-9_]+)\s*\(", txt)))
 
 
 @pytest.fixture(scope="module")

@@ -5,7 +5,7 @@ relative, Delta H 1e-8 absolute, identical accept/reject."""
 import numpy as np
 import pytest
 
-from helpers import cgauss, hot_links, rel, to_dev, to_host
+from helpers import bound, cgauss, hot_links, rel, to_dev, to_host
 from oracle.oracle import Oracle
 
 pytestmark = pytest.mark.gpu
@@ -33,9 +33,9 @@ def test_batch_matches_single_and_oracle(L1, L2):
         Ud = to_dev(U0[r])
         qed2d.seed(seeds[r])
         single = qed2d.HMC_(Ud, am0s[r], 0.1, 5, [], 10000, 1e-24, prm, None, counter=counter)
-        assert abs(single.dH - infos[r].dH) < 1e-8
+        bound("abs(single.dH - infos[r].dH)", abs(single.dH - infos[r].dH), 1e-8)
         assert single.accepted == infos[r].accepted
-        assert rel(to_host(Ub[r]), to_host(Ud)) < 1e-9
+        bound("rel err vs to_host(Ud)", rel(to_host(Ub[r]), to_host(Ud)), 1e-9)
     qed2d.set_precision("f64")
     # replica 1 against the oracle replaying its draws
     r = 1
@@ -45,8 +45,8 @@ def test_batch_matches_single_and_oracle(L1, L2):
     st, Uo, acc, hi, hf, _ = o.hmc_nf2(U0[r], am0s[r], 0.1, 5, 10000, 1e-24, mom0, noise,
                                         Oracle.uniform(seeds[r], 3, counter))
     assert st == 0 and acc == infos[r].accepted
-    assert abs(infos[r].dH - (hf - hi)) < 1e-8
-    assert rel(to_host(Ub[r]), Uo) < 1e-9
+    bound("abs(infos[r].dH - (hf - hi))", abs(infos[r].dH - (hf - hi)), 1e-8)
+    bound("rel err vs Uo", rel(to_host(Ub[r]), Uo), 1e-9)
 
 
 def test_batch_rejects_bad_shape():
@@ -77,7 +77,7 @@ def test_batch_cg_matches_single_cg():
         xs = qed2d.cfield(L1, L2)
         it = qed2d.CG(xs, U[r].contiguous(), src[r].contiguous(), am0s[r], 20000, 1e-24,
                       qed2d.gamm5Dw_sqr_msq, prm, None)
-        assert rel(to_host(x[r]), to_host(xs)) < 1e-9
+        bound("rel err vs to_host(xs)", rel(to_host(x[r]), to_host(xs)), 1e-9)
         assert abs(its[r] - it) <= max(3, it // 20) and upd[r] >= 1
     qed2d.set_precision("f64")
 
@@ -107,9 +107,9 @@ def test_ragged_batch_matches_single_and_oracle():
         Ud = to_dev(U0[r])
         qed2d.seed(seeds[r])
         single = qed2d.HMC_(Ud, am0s[r], 0.1, 5, [], 10000, 1e-24, prm, None, counter=counter)
-        assert abs(single.dH - infos[r].dH) < 1e-8, r
+        bound("abs(single.dH - infos[r].dH)", abs(single.dH - infos[r].dH), 1e-8)  # r
         assert single.accepted == infos[r].accepted, r
-        assert rel(to_host(b.replica(Ub, r)), to_host(Ud)) < 1e-9, r
+        bound("rel err vs to_host(Ud)", rel(to_host(b.replica(Ub, r)), to_host(Ud)), 1e-9)  # r
     qed2d.set_precision("f64")
     r = 5   # the odd-sized replica against the oracle replaying its draws
     l1, l2 = RAGGED[r]
@@ -119,8 +119,8 @@ def test_ragged_batch_matches_single_and_oracle():
     st, Uo, acc, hi, hf, _ = o.hmc_nf2(U0[r], am0s[r], 0.1, 5, 10000, 1e-24, mom0, noise,
                                         Oracle.uniform(seeds[r], 3, counter))
     assert st == 0 and acc == infos[r].accepted
-    assert abs(infos[r].dH - (hf - hi)) < 1e-8
-    assert rel(to_host(b.replica(Ub, r)), Uo) < 1e-9
+    bound("abs(infos[r].dH - (hf - hi))", abs(infos[r].dH - (hf - hi)), 1e-8)
+    bound("rel err vs Uo", rel(to_host(b.replica(Ub, r)), Uo), 1e-9)
 
 
 def test_ragged_batch_cg_matches_single_and_is_deterministic():
@@ -141,7 +141,7 @@ def test_ragged_batch_cg_matches_single_and_is_deterministic():
         xs = qed2d.cfield(l1, l2)
         it = qed2d.CG(xs, b.replica(U, r).contiguous(), b.replica(src, r).contiguous(), am0s[r], 20000, 1e-24,
                       qed2d.gamm5Dw_sqr_msq, prm, None)
-        assert rel(to_host(b.replica(x, r)), to_host(xs)) < 1e-9, r
+        bound("rel err vs to_host(xs)", rel(to_host(b.replica(x, r)), to_host(xs)), 1e-9)  # r
         assert abs(its[r] - it) <= max(3, it // 20) and upd[r] >= 1, r
     qed2d.set_precision("f64")
 
@@ -177,7 +177,7 @@ def test_many_replicas_global_state_cg():
         xs = qed2d.cfield(l1, l2)
         qed2d.CG(xs, b.replica(U, r).contiguous(), b.replica(src, r).contiguous(), am0s[r], 20000, 1e-24,
                  qed2d.gamm5Dw_sqr_msq, prm, None)
-        assert rel(to_host(b.replica(x, r)), to_host(xs)) < 1e-9, r
+        bound("rel err vs to_host(xs)", rel(to_host(b.replica(x, r)), to_host(xs)), 1e-9)  # r
     qed2d.set_precision("f64")
 
 
@@ -236,9 +236,9 @@ def test_ragged_cluster_solver_matches_grid_solver(nrep):
         x2 = b.field()
         b.cg(x2, U, src, am0s, 20000, 1e-24)
         assert np.array_equal(to_host(x2), res[sched][1])   # each solver is deterministic
-    assert rel(res[3][1], res[2][1]) < 1e-9
+    bound("rel err vs res[2][1]", rel(res[3][1], res[2][1]), 1e-9)
     for r in range(nrep):
-        assert abs(res[3][0][r] - res[2][0][r]) <= max(3, res[2][0][r] // 20), r
+        bound("abs(res[3][0][r] - res[2][0][r])", abs(res[3][0][r] - res[2][0][r]), max(3, res[2][0][r] // 20))  # r
     qed2d.set_precision("mixed")
     for r in (0, nrep - 1):
         l1, l2 = sizes[r]
@@ -246,7 +246,7 @@ def test_ragged_cluster_solver_matches_grid_solver(nrep):
         xs = qed2d.cfield(l1, l2)
         qed2d.CG(xs, b.replica(U, r).contiguous(), b.replica(src, r).contiguous(), am0s[r], 20000, 1e-24,
                  qed2d.gamm5Dw_sqr_msq, prm, None)
-        assert rel(to_host(b.replica(x2, r)), to_host(xs)) < 1e-9, r
+        bound("rel err vs to_host(xs)", rel(to_host(b.replica(x2, r)), to_host(xs)), 1e-9)  # r
     qed2d.set_precision("f64")
 
 
@@ -303,7 +303,7 @@ def test_capped_solves_agree_across_solvers(maxiter):
         qed2d.set_schedule(prm, -1, "mixed")
         qed2d.set_precision("f64")
     assert np.abs(ref[2]).max() > 0
-    assert rel(ref[1], ref[2]) < 1e-4
+    bound("rel err vs ref[2]", rel(ref[1], ref[2]), 1e-4)
     bt = qed2d.Batch(2, L, L, 4.0)
     Ub, bb = bt.field(), bt.field()
     for r in range(2):
@@ -313,7 +313,7 @@ def test_capped_solves_agree_across_solvers(maxiter):
         x = bt.field()
         capped(lambda: bt.cg(x, Ub, bb, [am0, am0], maxiter, 1e-24))
         for r in range(2):
-            assert rel(to_host(x[r]), ref[2]) < 1e-4, (sched, r)
+            bound("rel err vs ref[2]", rel(to_host(x[r]), ref[2]), 1e-4)  # (sched, r)
     rb = qed2d.Batch.ragged([(L, L), (32, 32)], [4.0, 4.0])
     Ur, br = rb.field(), rb.field()
     rb.replica(Ur, 0).copy_(U)
@@ -324,4 +324,4 @@ def test_capped_solves_agree_across_solvers(maxiter):
         rb.schedule = sched
         x = rb.field()
         capped(lambda: rb.cg(x, Ur, br, [am0, am0], maxiter, 1e-24))
-        assert rel(to_host(rb.replica(x, 0)), ref[2]) < 1e-4, sched
+        bound("rel err vs ref[2]", rel(to_host(rb.replica(x, 0)), ref[2]), 1e-4)  # sched

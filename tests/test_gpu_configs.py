@@ -11,7 +11,7 @@
 import numpy as np
 import pytest
 
-from helpers import cgauss, hot_links, rel, to_dev, to_host
+from helpers import bound, cgauss, hot_links, rel, to_dev, to_host
 from oracle.oracle import Oracle, zolotarev
 
 pytestmark = pytest.mark.gpu
@@ -40,10 +40,10 @@ def test_rhmc_128_twelve_poles_vs_oracle(q):
     noise = [cgauss(L, L, 5, 16, ctr)]
     st, Uo, acc, hi, hf, _ = o.hmc_rhmc(U0, am0, 0.05, 4, 20000, 1e-24, ro, mom0, noise, Oracle.uniform(5, 3, ctr))
     assert st == 0
-    assert abs(info.hini - hi) < 1e-9 * abs(hi)
-    assert abs(info.dH - (hf - hi)) < 1e-7
+    bound("abs(info.hini - hi)", abs(info.hini - hi), 1e-9 * abs(hi))
+    bound("abs(info.dH - (hf - hi))", abs(info.dH - (hf - hi)), 1e-7)
     assert info.accepted == acc
-    assert rel(to_host(Ud), Uo) < 1e-9
+    bound("rel err vs Uo", rel(to_host(Ud), Uo), 1e-9)
 
 
 def test_master_field_8192(q):
@@ -63,18 +63,18 @@ def test_master_field_8192(q):
     prm = q.LattParm((L, L), beta)
     # integer topological charge of the unfolded field
     Q = q.Qtop(U, prm)
-    assert abs(Q - round(Q)) < 1e-6
+    bound("abs(Q - round(Q))", abs(Q - round(Q)), 1e-6)
     # OMF4 reversibility at 8192^2 (ns=20, eps=0.025 as the master-field config)
     U0 = U.clone()
     mom = torch.randn((2, L, L), dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(3))
     H0 = q.Hamiltonian(mom, U, prm)
     q.OMF4_(mom, U, 0.025, 20, prm, None)
     H1 = q.Hamiltonian(mom, U, prm)
-    assert abs(H1 - H0) < 1e-2 * L * L / 1e6 + 50.0   # OMF4 energy error: small, extensive
+    bound("abs(H1 - H0)", abs(H1 - H0), 1e-2 * L * L / 1e6 + 50.0)   # OMF4 energy error: small, extensive
     mom.neg_()
     q.OMF4_(mom, U, 0.025, 20, prm, None)
     assert float((U - U0).abs().max()) < 1e-9
-    assert abs(q.Hamiltonian(mom, U, prm) - H0) < 1e-6 * abs(H0)
+    bound("abs(q.Hamiltonian(mom, U, prm) - H0)", abs(q.Hamiltonian(mom, U, prm) - H0), 1e-6 * abs(H0))
 
 
 def test_nf2_64_mixed_vs_f64_and_oracle(q):
@@ -97,9 +97,9 @@ def test_nf2_64_mixed_vs_f64_and_oracle(q):
     assert st == 0
     for prec in ("f64", "mixed"):
         i, Uh = out[prec]
-        assert abs(i.dH - (hf - hi)) < 1e-7, prec
+        bound("abs(i.dH - (hf - hi))", abs(i.dH - (hf - hi)), 1e-7)  # prec
         assert i.accepted == acc, prec
-        assert rel(Uh, Uo) < 1e-8, prec
+        bound("rel err vs Uo", rel(Uh, Uo), 1e-8)  # prec
 
 
 def test_ensemble_512_ragged_replicas(q):
@@ -125,7 +125,7 @@ def test_ensemble_512_ragged_replicas(q):
         Ud = b.replica(U0, r).clone()
         q.seed(seeds[r])
         single = q.HMC_(Ud, am0s[r], 0.1, 10, [], 20000, 1e-24, prm, None, counter=counter)
-        assert abs(single.dH - infos[r].dH) < 1e-9 * abs(single.hini) + 1e-8, r
+        bound("abs(single.dH - infos[r].dH)", abs(single.dH - infos[r].dH), 1e-9 * abs(single.hini) + 1e-8)  # r
         assert single.accepted == infos[r].accepted, r
-        assert rel(to_host(b.replica(U, r)), to_host(Ud)) < 1e-9, r
+        bound("rel err vs to_host(Ud)", rel(to_host(b.replica(U, r)), to_host(Ud)), 1e-9)  # r
     q.set_precision("f64")

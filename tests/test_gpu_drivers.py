@@ -6,6 +6,8 @@ import os
 import numpy as np
 import pytest
 
+from bdio_reader import read_bdio
+
 pytestmark = pytest.mark.gpu
 
 
@@ -44,8 +46,15 @@ def test_mc_rhmc_master_field_drivers(tmp_path, monkeypatch):
                                      "Lattice": {"size": [16, 16], "beta": 4.0},
                                      "HMC": {"ns": 5, "eps": 0.1, "nthm": 2, "ntraj": 3, "Qzero": False}})
     drivers.main(["mc", "-i", mc])
-    assert len(open("mc_plaq.txt").read().split()) == 3
     assert "MEASUREMENT Trajectory 3 / 3" in open("mc.log").read()
+    h, recs = read_bdio("mc.bdio")
+    data = [r for r in recs if r["uinfo"] != 7]
+    assert [r["uinfo"] for r in data] == [1, 2, 3, 4]
+    assert np.array_equal(np.frombuffer(data[1]["data"], "<f8"), [16, 16, 4.0, 3])
+    pl = np.frombuffer(data[2]["data"], "<f8").reshape(16, 3)   # the series, written L1 times
+    qt = np.frombuffer(data[3]["data"], "<f8").reshape(16, 3)
+    assert (pl == pl[0]).all() and (qt == qt[0]).all() and (0 < pl).all() and (pl < 1).all()
+    assert np.abs(qt - np.rint(qt)).max() < 1e-9
     rh = write(tmp_path / "rh.in", {"Run": {"user": "u", "host": "h", "name": "rh", "seed": 7},
                                      "Lattice": {"size": [8, 8], "beta": 5.0},
                                      "HMC": {"tau": 0.5, "ns": 4, "nthm": 0, "ntraj": 2, "Qzero": False},
@@ -61,9 +70,15 @@ def test_mc_rhmc_master_field_drivers(tmp_path, monkeypatch):
                                      "Lattice": {"size": [64, 64], "beta": 11.25},
                                      "HMC": {"ns": 5, "eps": 0.05, "ntraj": 1, "Qzero": False}})
     drivers.main(["master-field", "-i", mf])
-    for j in (1, 2):
-        p = np.load(f"mf_msm{j}_plaq.npy")
-        q = np.load(f"mf_msm{j}_qtop.npy")
-        assert p.shape == (64, 64) and q.shape == (64, 64)
+    h, recs = read_bdio("mf.bdio")
+    data = [r for r in recs if r["uinfo"] != 7]
+    assert [r["uinfo"] for r in data] == [1, 2, 3, 4, 3, 4]   # two measurements (before and after)
+    assert np.array_equal(np.frombuffer(data[1]["data"], "<f8"), [64, 64, 11.25, 1])
+    for j in (0, 1):
+        p = np.frombuffer(data[2 + 2 * j]["data"], "<f8")
+        q = np.frombuffer(data[3 + 2 * j]["data"], "<f8")
+        assert p.size == 64 * 64 and q.size == 64 * 64
+        assert (np.abs(p) <= 1).all() and (np.abs(q) <= np.pi).all()
         Q = q.sum() / (2 * np.pi)
         assert abs(Q - round(Q)) < 1e-9
+    assert "Plaquette and error:" in open("mf.log").read()

@@ -6,7 +6,7 @@ complete (its second member does not exist), with a small poll limit, through
 the C ABI; afterwards the same context must solve as usual."""
 import pytest
 
-from helpers import cgauss, hot_links, rel, to_dev, to_host
+from helpers import bound, cgauss, hot_links, rel, to_dev, to_host
 from oracle.oracle import Oracle
 
 pytestmark = pytest.mark.gpu
@@ -27,4 +27,4 @@ def test_barrier_wait_gives_up_and_context_stays_usable():
     qed2d.set_precision("f64")
     x = qed2d.cfield(L1, L2)
     qed2d.CG(x, to_dev(Uh), to_dev(bh), am0, 20000, 1e-24, qed2d.gamm5Dw_sqr_msq, prm, None)
-    assert rel(to_host(x), xo) < 1e-9
+    bound("rel err vs xo", rel(to_host(x), xo), 1e-9)

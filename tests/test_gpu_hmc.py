@@ -6,7 +6,7 @@ relative, energies within 1e-8 absolute, identical accept/reject."""
 import numpy as np
 import pytest
 
-from helpers import cgauss, hot_links, rel, to_dev, to_host
+from helpers import bound, cgauss, hot_links, rel, to_dev, to_host
 from oracle.oracle import LEAPFROG as O_LEAPFROG, OMF4 as O_OMF4, Oracle, zolotarev
 
 pytestmark = pytest.mark.gpu
@@ -43,8 +43,8 @@ def test_hmc_gauge(q, integ):
                                             integrator=O_OMF4 if integ == "omf4" else O_LEAPFROG)
         assert abs(info.hini - hi) < 1e-8 * abs(hi) and abs(info.dH - (hf - hi)) < 1e-8
         assert info.accepted == acco == acc[0]
-        assert rel(to_host(Ud), Uo) < 1e-10
-        assert abs(info.qtop - o.qtop(Uo)) < 1e-8
+        bound("rel err vs Uo", rel(to_host(Ud), Uo), 1e-10)
+        bound("abs(info.qtop - o.qtop(Uo))", abs(info.qtop - o.qtop(Uo)), 1e-8)
 
 
 def test_omf4_gauge_reversible(q):
@@ -56,7 +56,7 @@ def test_omf4_gauge_reversible(q):
     q.OMF4_(mom, Ud, 0.1, 10, prm, None)
     mom.neg_()
     q.OMF4_(mom, Ud, 0.1, 10, prm, None)
-    assert rel(to_host(Ud), U0) < 1e-11
+    bound("rel err vs U0", rel(to_host(Ud), U0), 1e-11)
 
 
 @pytest.mark.parametrize("integ", ["leapfrog", "omf4"])
@@ -76,11 +76,11 @@ def test_hmc_nf2(q, integ):
     st, Uo, acco, hi, hf, ito = o.hmc_nf2(U0, am0, 0.1, ns, 10000, 1e-24, mom0, noise[0], u,
                                            integrator=O_LEAPFROG if integ == "leapfrog" else O_OMF4)
     assert st == 0
-    assert abs(info.hini - hi) < 1e-9 * abs(hi)
-    assert abs(info.dH - (hf - hi)) < 1e-8
+    bound("abs(info.hini - hi)", abs(info.hini - hi), 1e-9 * abs(hi))
+    bound("abs(info.dH - (hf - hi))", abs(info.dH - (hf - hi)), 1e-8)
     assert info.accepted == acco
-    assert rel(to_host(Ud), Uo) < 1e-9
-    assert abs(info.cg_iterations - ito) <= 2 * (ns + 1) * (6 if integ == "omf4" else 1)
+    bound("rel err vs Uo", rel(to_host(Ud), Uo), 1e-9)
+    bound("abs(info.cg_iterations - ito)", abs(info.cg_iterations - ito), 2 * (ns + 1) * (6 if integ == "omf4" else 1))
 
 
 def test_hmc_nf2_mixed_matches_f64(q):
@@ -97,8 +97,8 @@ def test_hmc_nf2_mixed_matches_f64(q):
         info = q.HMC_(Ud, am0, 0.05, 10, [], 10000, 1e-24, prm, None)
         res[prec] = (info, to_host(Ud))
     q.set_precision("f64")
-    assert abs(res["f64"][0].dH - res["mixed"][0].dH) < 1e-7
-    assert rel(res["mixed"][1], res["f64"][1]) < 1e-8
+    bound("abs(res['f64'][0].dH - res['mixed'][0].dH)", abs(res["f64"][0].dH - res["mixed"][0].dH), 1e-7)
+    bound("rel err vs res['f64'][1]", rel(res["mixed"][1], res["f64"][1]), 1e-8)
     assert res["f64"][0].accepted == res["mixed"][0].accepted
 
 
@@ -118,10 +118,10 @@ def test_hmc_rhmc(q, prec):
     mom0, noise, u = draws(L, L, 31, info.counter, nf=2)
     st, Uo, acco, hi, hf, _ = o.hmc_rhmc(U0, am0, 0.1, 5, 10000, 1e-24, ro, mom0, noise, u)
     assert st == 0
-    assert abs(info.hini - hi) < 1e-9 * abs(hi)
-    assert abs(info.dH - (hf - hi)) < 1e-8
+    bound("abs(info.hini - hi)", abs(info.hini - hi), 1e-9 * abs(hi))
+    bound("abs(info.dH - (hf - hi))", abs(info.dH - (hf - hi)), 1e-8)
     assert info.accepted == acco
-    assert rel(to_host(Ud), Uo) < 1e-9
+    bound("rel err vs Uo", rel(to_host(Ud), Uo), 1e-9)
     q.set_precision("f64")
 
 

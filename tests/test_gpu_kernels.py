@@ -7,7 +7,7 @@ import os
 import numpy as np
 import pytest
 
-from helpers import cgauss, hot_links, rel, to_dev, to_host
+from helpers import bound, cgauss, hot_links, rel, to_dev, to_host
 from oracle.oracle import Oracle
 
 pytestmark = pytest.mark.gpu
@@ -35,33 +35,33 @@ def test_kernels_golden(q, tag):
     U, si, X = to_dev(g["U"]), to_dev(g["si"]), to_dev(g["X"])
     so = q.cfield(L1, L2)
     q.gamm5Dw(so, U, si, m0, prm)
-    assert rel(to_host(so), g["g5dw"]) < 1e-14
+    bound("rel err vs g5dw", rel(to_host(so), g["g5dw"]), 1e-14)
     q.Dw(so, U, si, m0, prm)
-    assert rel(to_host(so), g["dw"]) < 1e-14
+    bound("rel err vs dw", rel(to_host(so), g["dw"]), 1e-14)
     q.gamm5Dw_sqr(so, U, si, m0, prm)
-    assert rel(to_host(so), g["g5dw_sqr"]) < 1e-14
+    bound("rel err vs g5dw_sqr", rel(to_host(so), g["g5dw_sqr"]), 1e-14)
     q.gamm5Dw_sqr_musq(so, None, U, si, m0, mu, prm)
-    assert rel(to_host(so), g["g5dw_sqr_musq"]) < 1e-14
+    bound("rel err vs g5dw_sqr_musq", rel(to_host(so), g["g5dw_sqr_musq"]), 1e-14)
     G = q.cfield(L1, L2)
     q.gamm5Dw(G, U, X, m0, prm)
     frc = q.rfield(L1, L2)
     q.tr_dQwdU(frc, U, X, G, prm)
-    assert rel(to_host(frc), g["fermion_force"]) < 1e-13
+    bound("rel err vs fermion_force", rel(to_host(frc), g["fermion_force"]), 1e-13)
     Uu = to_dev(g["Uu"])
     plx = torch.zeros((L2, L1), dtype=torch.float64, device="cuda")
     q.plaquette_(plx, Uu, prm)
-    assert rel(to_host(plx), g["plaq_field"]) < 1e-14
+    bound("rel err vs plaq_field", rel(to_host(plx), g["plaq_field"]), 1e-14)
     q.qtop_(plx, Uu, prm)
-    assert rel(to_host(plx), g["qtop_field"]) < 1e-14
+    bound("rel err vs qtop_field", rel(to_host(plx), g["qtop_field"]), 1e-14)
     f1, f2 = q.rfield(L1, L2), q.rfield(L1, L2)
     q.krnl_force_(f1, f2, Uu, prm)
     assert rel(to_host(f1), g["frc1"]) < 1e-14 and rel(to_host(f2), g["frc2"]) < 1e-14
     U2 = Uu.clone()
     q.updt_fld_(U2, to_dev(g["mom"]), float(g["eps"]))
-    assert rel(to_host(U2), g["update_links"]) < 1e-14
+    bound("rel err vs update_links", rel(to_host(U2), g["update_links"]), 1e-14)
     assert np.array_equal(to_host(q.unfold_fld_(Uu, prm)), g["unfold"])
     assert np.array_equal(to_host(q.unfold_reflect_(Uu, prm)), g["reflect"])
-    assert abs(q.Action(Uu, prm) - float(g["action_unitary"])) < 1e-12 * abs(float(g["action_unitary"]))
+    bound("abs(q.Action(Uu, prm) - float(g['action_unitary']))", abs(q.Action(Uu, prm) - float(g["action_unitary"])), 1e-12 * abs(float(g["action_unitary"])))
 
 
 def test_free_field_eigenvalue(q):
@@ -77,7 +77,7 @@ def test_free_field_eigenvalue(q):
     q.Dw(Db, U, b, am0, prm)
     bh, Dh = to_host(b), to_host(Db)
     o = Oracle(L, L, 6.05)
-    assert rel(bh, o.plane_wave(k1, k2)) < 1e-14
+    bound("rel err vs o.plane_wave(k1, k2)", rel(bh, o.plane_wave(k1, k2)), 1e-14)
     lam = np.vdot(bh, Dh) / np.vdot(bh, bh)
     re = am0 + 2 * (np.sin(k1 / 2) ** 2 + np.sin(k2 / 2) ** 2)
     im = np.sqrt(np.sin(k1) ** 2 + np.sin(k2) ** 2)
@@ -94,15 +94,15 @@ def test_kernels_vs_oracle(q, L1, L2):
     Ud, sd = to_dev(U), to_dev(si)
     so = q.cfield(L1, L2)
     q.gamm5Dw(so, Ud, sd, 0.1, prm)
-    assert rel(to_host(so), o.g5dw(U, si, 0.1)) < 1e-14
+    bound("rel err vs o.g5dw(U, si, 0.1)", rel(to_host(so), o.g5dw(U, si, 0.1)), 1e-14)
     q.gamm5Dw_sqr_sqr(so, Ud, sd, 0.1, prm)
-    assert rel(to_host(so), o.g5dw_sqr_sqr(U, si, 0.1)) < 1e-13
+    bound("rel err vs o.g5dw_sqr_sqr(U, si, 0.1)", rel(to_host(so), o.g5dw_sqr_sqr(U, si, 0.1)), 1e-13)
     q.gamm5Dw_sqr_sqr_musq(so, None, Ud, sd, 0.1, 0.4, prm)
-    assert rel(to_host(so), o.g5dw_sqr_sqr_musq(U, si, 0.1, 0.4)) < 1e-13
+    bound("rel err vs o.g5dw_sqr_sqr_musq(U, si, 0.1, 0.4)", rel(to_host(so), o.g5dw_sqr_sqr_musq(U, si, 0.1, 0.4)), 1e-13)
     G = o.g5dw(U, si, 0.1)
     frc = q.rfield(L1, L2)
     q.tr_dQwdU(frc, Ud, sd, to_dev(G), prm)
-    assert rel(to_host(frc), o.fermion_force(U, si, G)) < 1e-13
+    bound("rel err vs o.fermion_force(U, si, G)", rel(to_host(frc), o.fermion_force(U, si, G)), 1e-13)
 
 
 @pytest.mark.parametrize("L1,L2", [(64, 64), (96, 40), (1024, 512)])
@@ -112,13 +112,13 @@ def test_observables_vs_oracle(q, L1, L2):
     U = hot_links(L1, L2, 3)
     Ud = to_dev(U)
     mom = np.random.default_rng(4).standard_normal((2, L2, L1))
-    assert abs(q.Action(Ud, prm) - o.action(U)) < 1e-12 * abs(o.action(U))
-    assert abs(q.Plaquette(Ud, prm) - o.plaquette(U)) < 1e-13
+    bound("abs(q.Action(Ud, prm) - o.action(U))", abs(q.Action(Ud, prm) - o.action(U)), 1e-12 * abs(o.action(U)))
+    bound("abs(q.Plaquette(Ud, prm) - o.plaquette(U))", abs(q.Plaquette(Ud, prm) - o.plaquette(U)), 1e-13)
     Qg, Qo = q.Qtop(Ud, prm), o.qtop(U)
-    assert abs(Qg - Qo) < 1e-9
+    bound("abs(Qg - Qo)", abs(Qg - Qo), 1e-9)
     assert q.Qtop_rounded(Ud, prm) == int(np.rint(Qo))
     H = q.Hamiltonian(to_dev(mom), Ud, prm)
-    assert abs(H - o.hamiltonian(mom, U)) < 1e-12 * abs(H)
+    bound("abs(H - o.hamiltonian(mom, U))", abs(H - o.hamiltonian(mom, U)), 1e-12 * abs(H))
 
 
 def test_random_streams_match_oracle(q):
@@ -151,6 +151,6 @@ def test_g5dw_complex64_vs_f64(q, L1, L2):
     q.gamm5Dw(so, U, si, 0.1, prm)
     ref = q.cfield(L1, L2)
     q.gamm5Dw(ref, U.to(torch.complex128), si.to(torch.complex128), 0.1, prm)
-    assert rel(to_host(so).astype(np.complex128), to_host(ref)) < 1e-6
+    bound("rel err vs to_host(ref)", rel(to_host(so).astype(np.complex128), to_host(ref)), 1e-6)
     with pytest.raises(ValueError):   # mixed precisions are rejected
         q.gamm5Dw(so, U.to(torch.complex128), si, 0.1, prm)

@@ -52,7 +52,9 @@ def test_noalloc_cg_matches_cg_twice(L1, L2, unitary):
         x_ref, it_ref = _cg_reference(qed2d, U, b, am0, L1, L2)
         x, it = _cg_noalloc(U, b, am0, L1, L2, torch)
         torch.cuda.synchronize()
-        assert it == it_ref
+        # qed2d_cg may run its tuned one-cluster schedule, whose sums are grouped
+        # differently from the cooperative grid this entry point always uses
+        assert abs(it - it_ref) <= 2
         assert rel(to_host(x), to_host(x_ref)) < 1e-9
 
 
@@ -70,3 +72,10 @@ def test_noalloc_cg_rejects_oversized_lattice():
                                      C.c_void_p(b.data_ptr()), 0.2, 100, 1e-24, None, C.byref(it))
     assert st == _lib.BAD_ARG
     assert b"exceeds the static scratch limit" in _lib.lib().qed2d_last_error()
+    # an output that overlaps the links is rejected before anything runs
+    L1 = 64
+    U = torch.ones((2, L2, L1), dtype=torch.complex128, device="cuda")
+    b = torch.ones_like(U)
+    st = _lib.lib().qed2d_cg_noalloc(L1, L2, C.c_void_p(U.data_ptr()), C.c_void_p(U.data_ptr()),
+                                     C.c_void_p(b.data_ptr()), 0.2, 100, 1e-24, None, C.byref(it))
+    assert st == _lib.BAD_ARG
