@@ -17,7 +17,9 @@ replica chain (no collective on the data path): value = all ranks' trajectories
 
 --impl reference times the reference's algorithm on the host CPU cores: the C
 restatement in oracle/ (the reference itself is Julia/CUDA.jl with no CPU
-path, and Julia is not installed), on a bounded sample of the same workload.
+path, and Julia is not installed).  Each of its steps is one full trajectory of
+replica chain 0 -- the same thermalised start and the same draws as the GPU
+arm's replica 0 at that step -- so its CG iteration counts match the GPU arm's.
 """
 import argparse
 import ctypes as C
@@ -54,6 +56,28 @@ B_DSLASH_C64 = 48.0      # g5Dw apply on complex64 fields: spinor in 16 + links 
 # traffic grows in proportion to the iterations at fixed size
 U_DRAM_PER_SITE_ITER = 61.0
 ENS_NS, ENS_EPS = 10, 0.1   # replica ensemble: leapfrog ns=10, eps=0.1
+CPU_TRAJ = 2                # trajectories of the GPU arm's CPU-baseline sample
+
+
+def l2_copy_peak(torch, dev):
+    """Copy bandwidth (read + write bytes / time) of a working set that stays in
+    L2 (two 24 MiB buffers, 126 MB of L2), measured in this run with CUDA events:
+    the denominator of the L2 roofline of the headline kernel."""
+    n = 24 * 2**20 // 16
+    a = torch.ones(n, 4, dtype=torch.float32, device=dev)
+    b = torch.empty_like(a)
+    for _ in range(20):
+        b.copy_(a)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = 0.0
+    for _ in range(3):
+        e0.record()
+        for _ in range(200):
+            b.copy_(a)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2 * a.numel() * 4 * 200 / (e0.elapsed_time(e1) / 1e3) / 1e9)
+    return best
 
 
 def load_peaks():
@@ -122,25 +146,23 @@ def hot_start(L1, L2, seed):
 
 # ---------------------------------------------------------------------------
 # reference arm / CPU baseline: the oracle (C restatement of the reference)
-def oracle_sample(U, seed, counter):
-    """One update_momenta! of the workload (CG solve to 1e-24 + both forces +
-    momentum kick) on the host cores; a trajectory is NS+1 of these."""
+def oracle_trajectory(o, U, seed, counter):
+    """One full Nf=2 trajectory of the workload (HMC! with leapfrog: momenta and
+    pseudofermion draws, ns+1 force evaluations each with a CG solve to 1e-24,
+    Metropolis) on the host cores, with the draws replica chain `seed` makes at
+    trajectory `counter` on the GPU.  Returns (seconds, new field, CG iterations)."""
     import numpy as np
     from oracle import oracle as O
-    o = O.Oracle(L, L, BETA)
+    mom0 = O.Oracle.normal(2 * L * L, seed, 1, counter).reshape(2, L, L)
     z = O.Oracle.normal(4 * L * L, seed, 16, counter)
-    X = ((z[0::2] + 1j * z[1::2]) / np.sqrt(2.0)).reshape(2, L, L)
-    F = o.g5dw(U, X, AM0)
-    mom = O.Oracle.normal(2 * L * L, seed, 1, counter).reshape(2, L, L)
-    Xs, G = o.cfield(), o.cfield()
-    it = C.c_int(0)
+    noise = ((z[0::2] + 1j * z[1::2]) / np.sqrt(2.0)).reshape(2, L, L)
+    u = O.Oracle.uniform(seed, 3, counter)
     t0 = time.perf_counter()
-    st = o.L.o_update_momenta_nf2(o._pp, O._p(mom), O._p(np.ascontiguousarray(U)), O._p(Xs), O._p(F), O._p(G),
-                                  AM0, 0.5 * EPS, MAXITER, TOL, C.byref(it))
+    st, U, acc, hi, hf, it = o.hmc_nf2(U, AM0, EPS, NS, MAXITER, TOL, mom0, noise, u)
     dt = time.perf_counter() - t0
     if st != 0:
         raise RuntimeError("oracle CG did not converge")
-    return dt, it.value
+    return dt, U, it
 
 
 def oracle_thermalised_field():
@@ -155,29 +177,35 @@ def oracle_thermalised_field():
 
 
 def run_reference(args):
+    """The reference's algorithm on the host cores: one step = one full trajectory
+    of replica chain 0 (seed SEED, counter = step index), from the same
+    thermalised start as the GPU arm, i.e. the trajectory the GPU arm's replica 0
+    runs at the same step."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     from oracle import oracle as O
     U = oracle_thermalised_field()
+    o = O.Oracle(L, L, BETA)
     times, iters = [], []
     for k in range(args.warmup + args.steps):
-        dt, it = oracle_sample(U, SEED, 1000 + k)
+        dt, U, it = oracle_trajectory(o, U, SEED, k)
         if k >= args.warmup:
             times.append(dt)
             iters.append(it)
-    t_traj = (NS + 1) * statistics.mean(times)
+    t_traj = statistics.mean(times)
     value = 1.0 / t_traj
     cores = O.num_threads()
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "traj/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_traj, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "solver": "reference CG (FP64, host)"},
+        "config": {"workload": WORKLOAD, "solver": "reference CG (FP64, host)", "chains": 1},
         "cpu_baseline": {"value": value, "unit": "traj/s", "cores": cores, "kind": "port",
-                         "sample": f"per step one update_momenta! (CG solve to 1e-24 + forces) of the {L}x{L} "
-                                   f"workload on the thermalised field, x{NS + 1} per trajectory; "
-                                   f"mean CG iterations {statistics.mean(iters):.0f}"},
+                         "sample": f"per step one full {L}x{L} trajectory (HMC! Nf=2, leapfrog ns={NS}) of replica "
+                                   f"chain 0 from the thermalised start, the draws of the GPU arm's replica 0 "
+                                   f"at the same step; mean CG iterations per trajectory "
+                                   f"{statistics.mean(iters):.0f}"},
         "e2e": {"value": value, "unit": "traj/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -517,10 +545,16 @@ def run_ours(args):
     cpu = None
     if not args.skip_cpu:
         from oracle import oracle as O
-        dt, it = oracle_sample(U1.cpu().numpy(), seeds[0], 999)
-        cpu = {"value": 1.0 / ((NS + 1) * dt), "unit": "traj/s", "cores": O.num_threads(), "kind": "port",
-               "sample": f"one update_momenta! (CG to 1e-24, {it} iterations, + forces) of the {L}x{L} workload "
-                         f"on the benchmark's field, x{NS + 1} per trajectory (one chain)"}
+        Uc = oracle_thermalised_field()
+        o = O.Oracle(L, L, BETA)
+        t_cpu, its_cpu = [], []
+        for k in range(CPU_TRAJ):
+            dt, Uc, it = oracle_trajectory(o, Uc, SEED, k)
+            t_cpu.append(dt)
+            its_cpu.append(it)
+        cpu = {"value": CPU_TRAJ / sum(t_cpu), "unit": "traj/s", "cores": O.num_threads(), "kind": "port",
+               "sample": f"the first {CPU_TRAJ} trajectories of replica chain 0 (the GPU arm's draws, "
+                         f"{'/'.join(str(i) for i in its_cpu)} CG iterations) from the thermalised start, one chain"}
 
     line = {
         "metric": METRIC, "value": value, "unit": "traj/s", "n_gpus": world, "steps": args.steps,

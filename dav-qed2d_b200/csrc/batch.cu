@@ -766,6 +766,29 @@ __global__ void k_r_finish(const RepState* __restrict__ st, int nrep, int maxite
 #include "batch_cg_uniform.cuh"
 #include "batch_cg_cluster.cuh"
 
+namespace qed2d {
+// tile heights of k_u_cg_mixed (rows of 32 sites per tile = warps per block);
+// the first is the default when the tuner is off
+constexpr int kUTileRows[3] = {8, 16, 4};
+
+// the equal-size solver for schedule 0/1 (grid reductions) or 4 (a barrier per
+// replica) and a tile height
+static const void* uniform_kernel(int sched, int rows) {
+    const int rs = sched == 4 ? 2 : sched;
+    switch (rows * 4 + rs) {
+        case 4 * 4 + 0: return (const void*)k_u_cg_mixed<0, 4>;
+        case 4 * 4 + 1: return (const void*)k_u_cg_mixed<1, 4>;
+        case 4 * 4 + 2: return (const void*)k_u_cg_mixed<2, 4>;
+        case 16 * 4 + 0: return (const void*)k_u_cg_mixed<0, 16>;
+        case 16 * 4 + 1: return (const void*)k_u_cg_mixed<1, 16>;
+        case 16 * 4 + 2: return (const void*)k_u_cg_mixed<2, 16>;
+        case 8 * 4 + 1: return (const void*)k_u_cg_mixed<1, 8>;
+        case 8 * 4 + 2: return (const void*)k_u_cg_mixed<2, 8>;
+        default: return (const void*)k_u_cg_mixed<0, 8>;
+    }
+}
+}  // namespace qed2d
+
 // ===========================================================================
 // host side
 using namespace qed2d;
@@ -798,9 +821,17 @@ struct qed2d_batch {
     int rsched = -1;                // uneven batches: 2 grid solver, 3 one cluster per replica (-1: not tuned)
     int rcs = 8;                    // blocks per cluster of the cluster solver (tuned)
     int* d_order = nullptr;         // [nrep] replicas by decreasing size (cluster solver)
+    // k_u_cg_mixed geometry per tile height (kUTileRows): tiles per replica,
+    // tiles per block, blocks per replica, grid
+    struct UVar {
+        int rows = 0, per_block = 0, bpr = 0, grid = 0;
+        long long ntr = 0;
+    } uv[3];
+    int nuv = 0;                    // heights whose kernels fit (co-resident grid)
+    int utile = -1;                 // index into uv of the tile height in use; -1 untuned
+    bool utile_fixed = false;       // set by qed2d_batch_set_tile_rows: the tuner keeps it
     UGeom ug{};
-    int ugrid = 0, ubpr = 0, uper_block = 0;
-    double* d_upart = nullptr;      // [2][ubpr * nrep]
+    double* d_upart = nullptr;      // [2][max grid over uv]
     double* d_ured = nullptr;       // [2][nrep]
     unsigned long long* d_ubar = nullptr;   // [nrep][16] per-replica barrier counters (schedule 4)
     int* d_out = nullptr;           // [2][nrep]: iterations, reliable updates of the last solve
@@ -874,6 +905,7 @@ template <class Launch>
 int tune_uniform(qed2d_batch* h, const UCGP& Q, int maxiter, Launch launch) {
     if (!tuning_enabled()) {
         h->usched = h->nrep >= 2 ? 4 : 1;
+        if (!h->utile_fixed) h->utile = 0;
         return QED2D_OK;
     }
     DevCtl saved;
@@ -887,29 +919,35 @@ int tune_uniform(qed2d_batch* h, const UCGP& Q, int maxiter, Launch launch) {
     cudaEvent_t e0, e1;
     QCHECK(cudaEventCreate(&e0));
     QCHECK(cudaEventCreate(&e1));
-    constexpr int cand[3] = {0, 1, 4};
-    const int ncand = h->nrep >= 2 ? 3 : 2;
-    float tbest[3] = {1e30f, 1e30f, 1e30f};
+    // candidates: (schedule, tile height); the height only when it is not fixed
+    constexpr int scheds[3] = {0, 1, 4};
+    const int nsched = h->nrep >= 2 ? 3 : 2;
+    const int t_lo = h->utile_fixed ? h->utile : 0, t_hi = h->utile_fixed ? h->utile + 1 : h->nuv;
+    std::vector<std::pair<int, int>> cand;
+    for (int t = t_lo; t < t_hi; t++)
+        for (int rs = 0; rs < nsched; rs++) cand.push_back({scheds[rs], t});
+    std::vector<float> tbest(cand.size(), 1e30f);
     int st = QED2D_OK;
     for (int rep = 0; rep < 3 && st == QED2D_OK; rep++)
-        for (int rs = 0; rs < ncand && st == QED2D_OK; rs++) {
+        for (size_t c = 0; c < cand.size() && st == QED2D_OK; c++) {
             cudaEventRecord(e0, h->stream);
-            st = launch(cand[rs], T);
+            st = launch(cand[c].first, cand[c].second, T);
             cudaEventRecord(e1, h->stream);
             if (cudaEventSynchronize(e1) != cudaSuccess) st = cuda_status(cudaGetLastError(), "schedule tuning");
             float ms = 0.f;
             cudaEventElapsedTime(&ms, e0, e1);
-            if (rep > 0) tbest[rs] = std::min(tbest[rs], ms);   // the first round warms up
+            if (rep > 0) tbest[c] = std::min(tbest[c], ms);   // the first round warms up
         }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     QCHECK(cudaMemcpyAsync(h->ctl, &saved, sizeof(DevCtl), cudaMemcpyHostToDevice, h->stream));
     QCHECK(cudaStreamSynchronize(h->stream));
     if (st != QED2D_OK) return st;
-    int best = 1;
-    for (int i = 0; i < ncand; i++)
-        if (tbest[i] < tbest[best]) best = i;
-    h->usched = cand[best];
+    size_t best = 0;
+    for (size_t c = 1; c < cand.size(); c++)
+        if (tbest[c] < tbest[best]) best = c;
+    h->usched = cand[best].first;
+    h->utile = cand[best].second;
     return QED2D_OK;
 }
 
@@ -1072,26 +1110,27 @@ int r_solve(qed2d_batch* h, const double2* U, const float4* U32, const double2* 
         Q.eps = eps;
         Q.delta2 = P.delta2;
         Q.maxiter = maxiter;
-        Q.bpr = h->ubpr;
-        Q.per_block = h->uper_block;
         Q.ctl = h->ctl;
         Q.part = h->d_upart;
         Q.red = h->d_ured;
         Q.rbar = h->d_ubar;
         Q.st_out = h->d_st;
-        auto launch = [&](int sched, const UCGP& q) -> int {
+        auto launch = [&](int sched, int tile, const UCGP& q0) -> int {
+            const qed2d_batch::UVar& v = h->uv[tile];
+            UCGP q = q0;
+            q.g.ntr = v.ntr;
+            q.bpr = v.bpr;
+            q.per_block = v.per_block;
             QCHECK(cudaMemsetAsync(&h->ctl->bar, 0, 2 * sizeof(unsigned long long) + sizeof(int), h->stream));
             if (sched == 4) QCHECK(cudaMemsetAsync(h->d_ubar, 0, sizeof(unsigned long long) * 16 * h->nrep, h->stream));
             void* uargs[] = {(void*)&q};
-            const void* kern = sched == 4   ? (const void*)k_u_cg_mixed<2>
-                               : sched == 1 ? (const void*)k_u_cg_mixed<1>
-                                            : (const void*)k_u_cg_mixed<0>;
-            QCHECK(cudaLaunchCooperativeKernel(kern, dim3((unsigned)h->ugrid), dim3(TILE), uargs, 0, h->stream));
+            QCHECK(cudaLaunchCooperativeKernel(uniform_kernel(sched, v.rows), dim3((unsigned)v.grid),
+                                               dim3((unsigned)(TX * v.rows)), uargs, 0, h->stream));
             count_launch();
             return QED2D_OK;
         };
-        if (h->usched < 0) QTRY(tune_uniform(h, Q, maxiter, launch));
-        QTRY(launch(h->usched, Q));
+        if (h->usched < 0 || h->utile < 0) QTRY(tune_uniform(h, Q, maxiter, launch));
+        QTRY(launch(h->usched, h->utile, Q));
         k_r_finish<<<1, 256, 0, h->stream>>>(h->d_st, h->nrep, maxiter, h->d_out, h->d_out + h->nrep, h->d_iters,
                                               h->ctl);
         return r_post("k_r_finish");
@@ -1230,22 +1269,30 @@ int batch_setup(qed2d_batch* h, const int* L1, const int* L2, const double* beta
     bool same = B <= kUniformReps;
     for (int r = 1; r < B && same; r++) same = L1[r] == L1[0] && L2[r] == L2[0];
     if (same) {
-        int per_smu = 0;
-        int per_smu1 = 0;
-        int per_smu2 = 0;
-        QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_smu, k_u_cg_mixed<0>, TILE, 0));
-        QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_smu1, k_u_cg_mixed<1>, TILE, 0));
-        QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_smu2, k_u_cg_mixed<2>, TILE, 0));
-        per_smu = std::min(per_smu, std::min(per_smu1, per_smu2));
-        const long long maxgu = std::min<long long>((long long)per_smu * h->num_sms, kMaxPartBlocks);
+        // one geometry per tile height: as many blocks per replica as stay
+        // co-resident (cooperative launch), tiles dealt in contiguous ranges
         const RepInfo& R0 = h->reps[0];
-        if (per_smu >= 1 && maxgu / B >= 1) {
-            h->uniform = true;
-            h->ug = UGeom{R0.L1, R0.L2, B, R0.nt1, R0.V, (long long)R0.nt};
+        for (int rows : kUTileRows) {
+            int per_smu = 1 << 30;
+            for (int sched : {0, 1, 4}) {
+                int n = 0;
+                QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, uniform_kernel(sched, rows), TX * rows, 0));
+                per_smu = std::min(per_smu, n);
+            }
+            const long long maxgu = std::min<long long>((long long)per_smu * h->num_sms, kMaxPartBlocks);
+            if (per_smu < 1 || maxgu / B < 1) continue;
+            qed2d_batch::UVar v;
+            v.rows = rows;
+            v.ntr = (long long)R0.nt1 * ((R0.L2 + rows - 1) / rows);
             const long long bpr = maxgu / B;
-            h->uper_block = (int)((R0.nt + bpr - 1) / bpr);
-            h->ubpr = (R0.nt + h->uper_block - 1) / h->uper_block;
-            h->ugrid = h->ubpr * B;
+            v.per_block = (int)((v.ntr + bpr - 1) / bpr);
+            v.bpr = (int)((v.ntr + v.per_block - 1) / v.per_block);
+            v.grid = v.bpr * B;
+            h->uv[h->nuv++] = v;
+        }
+        if (h->nuv > 0) {
+            h->uniform = true;
+            h->ug = UGeom{R0.L1, R0.L2, B, R0.nt1, R0.V, 0};
         }
     }
     std::vector<long long> dbc(B + 1), dbr(B + 1);
@@ -1275,7 +1322,9 @@ int batch_setup(qed2d_batch* h, const int* L1, const int* L2, const double* beta
     QCHECK(cudaMalloc(&h->d_red, sizeof(double) * 2 * B));
     QCHECK(cudaMalloc(&h->d_cnt, sizeof(int) * (B + 1)));
     if (h->uniform) {
-        QCHECK(cudaMalloc(&h->d_upart, sizeof(double) * 2 * (size_t)h->ugrid));
+        int gmax = 0;
+        for (int t = 0; t < h->nuv; t++) gmax = std::max(gmax, h->uv[t].grid);
+        QCHECK(cudaMalloc(&h->d_upart, sizeof(double) * 2 * (size_t)gmax));
         QCHECK(cudaMalloc(&h->d_ured, sizeof(double) * 2 * B));
         QCHECK(cudaMalloc(&h->d_ubar, sizeof(unsigned long long) * 16 * B));
     }
@@ -1378,6 +1427,32 @@ int qed2d_batch_set_schedule(qed2d_batch* h, int schedule) {
 int qed2d_batch_get_schedule(const qed2d_batch* h, int* schedule) {
     if (!h || !schedule) return QED2D_ERR_BAD_ARG;
     *schedule = h->uniform ? h->usched : h->rsched;
+    return QED2D_OK;
+}
+
+int qed2d_batch_set_tile_rows(qed2d_batch* h, int rows) {
+    if (!h || !h->uniform) {
+        set_error("qed2d_batch_set_tile_rows: only equal-size batches of at most 64 replicas have tile heights");
+        return QED2D_ERR_BAD_ARG;
+    }
+    if (rows == -1) {
+        h->utile_fixed = false;
+        h->utile = -1;
+        return QED2D_OK;
+    }
+    for (int t = 0; t < h->nuv; t++)
+        if (h->uv[t].rows == rows) {
+            h->utile = t;
+            h->utile_fixed = true;
+            return QED2D_OK;
+        }
+    set_error("qed2d_batch_set_tile_rows: rows must be -1 or one of 4, 8, 16 (with co-resident blocks)");
+    return QED2D_ERR_BAD_ARG;
+}
+
+int qed2d_batch_get_tile_rows(const qed2d_batch* h, int* rows) {
+    if (!h || !rows) return QED2D_ERR_BAD_ARG;
+    *rows = (h->uniform && h->utile >= 0) ? h->uv[h->utile].rows : -1;
     return QED2D_OK;
 }
 

@@ -49,12 +49,14 @@ struct UCGP {
     RepState* st_out;   // [B] final records
 };
 
-// site of thread t in tile (t1, t2) of replica r: global FP32 index, neighbours
+// site of thread t in tile (t1, t2) of replica r, tiles of 32 x TYv sites (a
+// block of 32 * TYv threads, one site each): global FP32 index, neighbours
 // wrapping inside the replica (no division)
+template <int TYv>
 __device__ __forceinline__ Site usite_at(const UGeom& g, int r, int t1, int t2, int t) {
     Site s;
     s.i1 = t1 * TX + (t & (TX - 1));
-    s.i2 = t2 * TY + (t >> 5);
+    s.i2 = t2 * TYv + (t >> 5);
     s.ok = s.i1 < g.L1 && s.i2 < g.L2;
     s.x = s.i1 + g.L1 * (r * g.L2 + s.i2);   // 32-bit: the batch holds < 2^30 sites
     s.xp1 = (s.i1 + 1 == g.L1) ? s.x - (g.L1 - 1) : s.x + 1;
@@ -147,9 +149,9 @@ __device__ __forceinline__ bool ureduce(GridSync& gs, double v, const UCGP& P, d
 #define FOR_MY_UTILES(q)                                                                       \
     for (int tt_ = TR.lo, t1_ = TR.s1, t2_ = TR.s2; tt_ < TR.hi;                              \
          ++tt_, (++t1_ == TR.nt1 ? (t1_ = 0, ++t2_) : 0))                                       \
-        if (const Site q = usite_at(P.g, myr, t1_, t2_, threadIdx.x); q.ok)
+        if (const Site q = usite_at<TYv>(P.g, myr, t1_, t2_, threadIdx.x); q.ok)
 
-template <int RS>
+template <int RS, int TYv>
 __device__ __forceinline__ bool u_body(const UCGP& P, GridSync& gs, int& k, double* smem, RepState* s_st,
                                        int* s_fl) {
     const int myr = blockIdx.x / P.bpr, lb = blockIdx.x - myr * P.bpr;
@@ -300,8 +302,13 @@ __device__ __forceinline__ bool u_body(const UCGP& P, GridSync& gs, int& k, doub
 }
 #undef FOR_MY_UTILES
 
-template <int RS>
-__global__ void __launch_bounds__(TILE, 4) k_u_cg_mixed(const UCGP P) {
+// Tiles of 32 x TYv sites, TYv = 4, 8 or 16 (blocks of 128, 256 or 512 threads):
+// the tile height sets how many blocks share a replica's tiles (and its
+// barriers) and how many tiles each block walks; the register budget (64 per
+// thread) is the same for all three.  Different heights group the partial sums
+// differently, so they agree to the solver's accuracy, not bit for bit.
+template <int RS, int TYv>
+__global__ void __launch_bounds__(32 * TYv, 32 / TYv) k_u_cg_mixed(const UCGP P) {
     __shared__ double smem[32];
     __shared__ RepState s_st[kUniformReps];
     __shared__ int s_fl[FL_N];
@@ -311,7 +318,7 @@ __global__ void __launch_bounds__(TILE, 4) k_u_cg_mixed(const UCGP P) {
     if constexpr (RS == 2) {   // independent replicas: a barrier per replica; its blocks leave when it is done
         const int myr = blockIdx.x / P.bpr;
         GridSync gs{P.rbar + 16 * myr, &P.ctl->gen, &P.ctl->err, (unsigned)P.bpr};
-        const bool ok = u_body<RS>(P, gs, k, smem, s_st, s_fl);
+        const bool ok = u_body<RS, TYv>(P, gs, k, smem, s_st, s_fl);
         if (blockIdx.x == myr * P.bpr && threadIdx.x == 0) {   // the replica's first block
             if (ok) P.st_out[myr] = s_st[myr];
             DevCtl* c = P.ctl;
@@ -321,7 +328,7 @@ __global__ void __launch_bounds__(TILE, 4) k_u_cg_mixed(const UCGP P) {
         return;
     }
     GridSync gs{&P.ctl->bar, &P.ctl->gen, &P.ctl->err};
-    const bool ok = u_body<RS>(P, gs, k, smem, s_st, s_fl);
+    const bool ok = u_body<RS, TYv>(P, gs, k, smem, s_st, s_fl);
     if (blockIdx.x == 0) {
         if (ok)   // every block holds the same records: block 0 stores them
             for (int r = threadIdx.x; r < P.g.B; r += blockDim.x) P.st_out[r] = s_st[r];

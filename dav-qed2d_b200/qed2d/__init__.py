@@ -758,6 +758,18 @@ class Batch:
     def schedule(self, s: int) -> None:
         check(lib().qed2d_batch_set_schedule(self.h, int(s)), "batch_set_schedule")
 
+    @property
+    def tile_rows(self) -> int:
+        """Tile height of the equal-size solver (tiles of 32 x rows sites): 4, 8
+        or 16, tuned with the schedule on the first solve (-1 until then)."""
+        v = C.c_int(0)
+        check(lib().qed2d_batch_get_tile_rows(self.h, C.byref(v)), "batch_get_tile_rows")
+        return v.value
+
+    @tile_rows.setter
+    def tile_rows(self, rows: int) -> None:
+        check(lib().qed2d_batch_set_tile_rows(self.h, int(rows)), "batch_set_tile_rows")
+
     def field(self, dtype=torch.complex128):
         if self.uniform:
             return torch.zeros((self.nrep, 2, self.L2, self.L1), dtype=dtype, device="cuda")

@@ -1,7 +1,9 @@
 """Batched replicas: each replica of a batch trajectory reproduces the
 single-lattice Nf=2 HMC step (mixed solver) with the same seed and counter, and
-the oracle replaying the same draws.  Tolerances as test_gpu_hmc.py: links 1e-9
-relative, Delta H 1e-8 absolute, identical accept/reject."""
+the oracle replaying the same draws.  Tolerances (each about 10x the error
+measured on a B200, recorded through helpers.bound): links 1e-12 (batch vs
+single lattice) and 5e-12 (vs the oracle) relative, Delta H 1e-10 / 5e-10
+absolute, identical accept/reject."""
 import numpy as np
 import pytest
 
@@ -33,9 +35,9 @@ def test_batch_matches_single_and_oracle(L1, L2):
         Ud = to_dev(U0[r])
         qed2d.seed(seeds[r])
         single = qed2d.HMC_(Ud, am0s[r], 0.1, 5, [], 10000, 1e-24, prm, None, counter=counter)
-        bound("abs(single.dH - infos[r].dH)", abs(single.dH - infos[r].dH), 1e-8)
+        bound("batch vs single-lattice dH abs", abs(single.dH - infos[r].dH), 1e-10)
         assert single.accepted == infos[r].accepted
-        bound("rel err vs to_host(Ud)", rel(to_host(Ub[r]), to_host(Ud)), 1e-9)
+        bound("batch vs single-lattice links", rel(to_host(Ub[r]), to_host(Ud)), 1e-12)
     qed2d.set_precision("f64")
     # replica 1 against the oracle replaying its draws
     r = 1
@@ -45,8 +47,8 @@ def test_batch_matches_single_and_oracle(L1, L2):
     st, Uo, acc, hi, hf, _ = o.hmc_nf2(U0[r], am0s[r], 0.1, 5, 10000, 1e-24, mom0, noise,
                                         Oracle.uniform(seeds[r], 3, counter))
     assert st == 0 and acc == infos[r].accepted
-    bound("abs(infos[r].dH - (hf - hi))", abs(infos[r].dH - (hf - hi)), 1e-8)
-    bound("rel err vs Uo", rel(to_host(Ub[r]), Uo), 1e-9)
+    bound("batch vs oracle dH abs", abs(infos[r].dH - (hf - hi)), 5e-10)
+    bound("batch vs oracle links", rel(to_host(Ub[r]), Uo), 5e-12)
 
 
 def test_batch_rejects_bad_shape():
@@ -77,7 +79,7 @@ def test_batch_cg_matches_single_cg():
         xs = qed2d.cfield(L1, L2)
         it = qed2d.CG(xs, U[r].contiguous(), src[r].contiguous(), am0s[r], 20000, 1e-24,
                       qed2d.gamm5Dw_sqr_msq, prm, None)
-        bound("rel err vs to_host(xs)", rel(to_host(x[r]), to_host(xs)), 1e-9)
+        bound("batched CG vs single-lattice CG", rel(to_host(x[r]), to_host(xs)), 1e-12)
         assert abs(its[r] - it) <= max(3, it // 20) and upd[r] >= 1
     qed2d.set_precision("f64")
 
@@ -107,9 +109,9 @@ def test_ragged_batch_matches_single_and_oracle():
         Ud = to_dev(U0[r])
         qed2d.seed(seeds[r])
         single = qed2d.HMC_(Ud, am0s[r], 0.1, 5, [], 10000, 1e-24, prm, None, counter=counter)
-        bound("abs(single.dH - infos[r].dH)", abs(single.dH - infos[r].dH), 1e-8)  # r
+        bound("ragged batch vs single-lattice dH abs", abs(single.dH - infos[r].dH), 1e-10)  # r
         assert single.accepted == infos[r].accepted, r
-        bound("rel err vs to_host(Ud)", rel(to_host(b.replica(Ub, r)), to_host(Ud)), 1e-9)  # r
+        bound("ragged batch vs single-lattice links", rel(to_host(b.replica(Ub, r)), to_host(Ud)), 1e-12)  # r
     qed2d.set_precision("f64")
     r = 5   # the odd-sized replica against the oracle replaying its draws
     l1, l2 = RAGGED[r]
@@ -119,8 +121,8 @@ def test_ragged_batch_matches_single_and_oracle():
     st, Uo, acc, hi, hf, _ = o.hmc_nf2(U0[r], am0s[r], 0.1, 5, 10000, 1e-24, mom0, noise,
                                         Oracle.uniform(seeds[r], 3, counter))
     assert st == 0 and acc == infos[r].accepted
-    bound("abs(infos[r].dH - (hf - hi))", abs(infos[r].dH - (hf - hi)), 1e-8)
-    bound("rel err vs Uo", rel(to_host(b.replica(Ub, r)), Uo), 1e-9)
+    bound("ragged batch vs oracle dH abs", abs(infos[r].dH - (hf - hi)), 1e-10)
+    bound("ragged batch vs oracle links", rel(to_host(b.replica(Ub, r)), Uo), 5e-12)
 
 
 def test_ragged_batch_cg_matches_single_and_is_deterministic():
@@ -141,7 +143,7 @@ def test_ragged_batch_cg_matches_single_and_is_deterministic():
         xs = qed2d.cfield(l1, l2)
         it = qed2d.CG(xs, b.replica(U, r).contiguous(), b.replica(src, r).contiguous(), am0s[r], 20000, 1e-24,
                       qed2d.gamm5Dw_sqr_msq, prm, None)
-        bound("rel err vs to_host(xs)", rel(to_host(b.replica(x, r)), to_host(xs)), 1e-9)  # r
+        bound("ragged batched CG vs single-lattice CG", rel(to_host(b.replica(x, r)), to_host(xs)), 1e-12)  # r
         assert abs(its[r] - it) <= max(3, it // 20) and upd[r] >= 1, r
     qed2d.set_precision("f64")
 
@@ -177,7 +179,7 @@ def test_many_replicas_global_state_cg():
         xs = qed2d.cfield(l1, l2)
         qed2d.CG(xs, b.replica(U, r).contiguous(), b.replica(src, r).contiguous(), am0s[r], 20000, 1e-24,
                  qed2d.gamm5Dw_sqr_msq, prm, None)
-        bound("rel err vs to_host(xs)", rel(to_host(b.replica(x, r)), to_host(xs)), 1e-9)  # r
+        bound("80-replica batched CG vs single-lattice CG", rel(to_host(b.replica(x, r)), to_host(xs)), 1e-12)  # r
     qed2d.set_precision("f64")
 
 
@@ -209,6 +211,46 @@ def test_batch_reduction_schedules_give_identical_bits():
     assert qed2d.Batch.ragged([(16, 16), (32, 8)], [4.0, 4.0]).schedule == -1
 
 
+@pytest.mark.parametrize("L1,L2", [(64, 48), (96, 40)])
+def test_batch_tile_heights(L1, L2):
+    """The equal-size solver's tile heights (tiles of 32 x 4, 8, 16 sites):
+    within a height the three schedules give identical bits; across heights the
+    block partials are grouped differently, so solutions agree to the solver's
+    accuracy (1e-9 relative) and iteration counts within 5%.  The first solve
+    tunes height and schedule together."""
+    import qed2d
+    nrep = 3
+    b = qed2d.Batch(nrep, L1, L2, 4.0)
+    assert b.tile_rows == -1
+    U, src = b.field(), b.field()
+    for r in range(nrep):
+        U[r] = to_dev(hot_links(L1, L2, 140 + r))
+        src[r] = to_dev(cgauss(L1, L2, 150 + r, 2))
+    am0 = [0.2, 0.3, 0.25]
+    b.cg(b.field(), U, src, am0, 20000, 1e-24)
+    assert b.tile_rows in (4, 8, 16) and b.schedule in (0, 1, 4)
+    res = {}
+    for rows in (8, 4, 16):
+        b.tile_rows = rows
+        per = []
+        for sched in (0, 1, 4):
+            b.schedule = sched
+            x = b.field()
+            its, _ = b.cg(x, U, src, am0, 20000, 1e-24)
+            per.append((list(its), to_host(x)))
+        for i in (1, 2):
+            assert per[0][0] == per[i][0] and np.array_equal(per[0][1], per[i][1]), (rows, i)
+        res[rows] = per[0]
+    for rows in (4, 16):
+        bound("tile height vs 32x8 solution rel", rel(res[rows][1], res[8][1]), 1e-9)
+        for r in range(nrep):
+            assert abs(res[rows][0][r] - res[8][0][r]) <= max(3, res[8][0][r] // 20), (rows, r)
+    b.tile_rows = -1
+    assert b.tile_rows == -1
+    with pytest.raises(qed2d.Qed2dError):
+        b.tile_rows = 12
+
+
 @pytest.mark.parametrize("nrep", [6, 80])
 def test_ragged_cluster_solver_matches_grid_solver(nrep):
     """Uneven batches have two solvers: one launch over all replicas with grid
@@ -236,9 +278,9 @@ def test_ragged_cluster_solver_matches_grid_solver(nrep):
         x2 = b.field()
         b.cg(x2, U, src, am0s, 20000, 1e-24)
         assert np.array_equal(to_host(x2), res[sched][1])   # each solver is deterministic
-    bound("rel err vs res[2][1]", rel(res[3][1], res[2][1]), 1e-9)
+    bound("cluster-per-replica vs grid solver", rel(res[3][1], res[2][1]), 2e-12)
     for r in range(nrep):
-        bound("abs(res[3][0][r] - res[2][0][r])", abs(res[3][0][r] - res[2][0][r]), max(3, res[2][0][r] // 20))  # r
+        bound("cluster-per-replica vs grid iterations", abs(res[3][0][r] - res[2][0][r]), 2)  # r
     qed2d.set_precision("mixed")
     for r in (0, nrep - 1):
         l1, l2 = sizes[r]
@@ -246,7 +288,7 @@ def test_ragged_cluster_solver_matches_grid_solver(nrep):
         xs = qed2d.cfield(l1, l2)
         qed2d.CG(xs, b.replica(U, r).contiguous(), b.replica(src, r).contiguous(), am0s[r], 20000, 1e-24,
                  qed2d.gamm5Dw_sqr_msq, prm, None)
-        bound("rel err vs to_host(xs)", rel(to_host(b.replica(x2, r)), to_host(xs)), 1e-9)  # r
+        bound("cluster-per-replica vs single-lattice CG", rel(to_host(b.replica(x2, r)), to_host(xs)), 1e-12)  # r
     qed2d.set_precision("f64")
 
 
@@ -303,7 +345,7 @@ def test_capped_solves_agree_across_solvers(maxiter):
         qed2d.set_schedule(prm, -1, "mixed")
         qed2d.set_precision("f64")
     assert np.abs(ref[2]).max() > 0
-    bound("rel err vs ref[2]", rel(ref[1], ref[2]), 1e-4)
+    bound("capped solve, x paired vs one update per iteration", rel(ref[1], ref[2]), 1e-6)
     bt = qed2d.Batch(2, L, L, 4.0)
     Ub, bb = bt.field(), bt.field()
     for r in range(2):
@@ -313,7 +355,7 @@ def test_capped_solves_agree_across_solvers(maxiter):
         x = bt.field()
         capped(lambda: bt.cg(x, Ub, bb, [am0, am0], maxiter, 1e-24))
         for r in range(2):
-            bound("rel err vs ref[2]", rel(to_host(x[r]), ref[2]), 1e-4)  # (sched, r)
+            bound("capped batched solve vs single-lattice", rel(to_host(x[r]), ref[2]), 1e-6)  # (sched, r)
     rb = qed2d.Batch.ragged([(L, L), (32, 32)], [4.0, 4.0])
     Ur, br = rb.field(), rb.field()
     rb.replica(Ur, 0).copy_(U)
@@ -324,4 +366,4 @@ def test_capped_solves_agree_across_solvers(maxiter):
         rb.schedule = sched
         x = rb.field()
         capped(lambda: rb.cg(x, Ur, br, [am0, am0], maxiter, 1e-24))
-        bound("rel err vs ref[2]", rel(to_host(rb.replica(x, 0)), ref[2]), 1e-4)  # sched
+        bound("capped ragged solve vs single-lattice", rel(to_host(rb.replica(x, 0)), ref[2]), 1e-6)  # sched

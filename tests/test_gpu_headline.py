@@ -66,13 +66,13 @@ def test_headline_batched_trajectories_vs_oracle(thermalised):
             i = infos[r]
             assert i.accepted == acc, (counter, r, i.dH, hf - hi)
             accepted += acc
-            bound("H_ini rel (4x512^2 batched)", abs(i.hini - hi) / abs(hi), 1e-13)
-            bound("H_fin rel (4x512^2 batched)", abs(i.hfin - hf) / abs(hf), 1e-11)
-            bound("dH abs (4x512^2 batched)", abs(i.dH - (hf - hi)), 1e-5)
-            bound("final links rel (4x512^2 batched)", rel(to_host(U[r]), Uo), 1e-9)
-            # 21 solves per trajectory; FP32 inner iterations may differ from FP64 by a few per solve
+            bound("H_ini rel (4x512^2 batched)", abs(i.hini - hi) / abs(hi), 5e-15)
+            bound("H_fin rel (4x512^2 batched)", abs(i.hfin - hf) / abs(hf), 1e-14)
+            bound("dH abs (4x512^2 batched)", abs(i.dH - (hf - hi)), 1e-8)
+            bound("final links rel (4x512^2 batched)", rel(to_host(U[r]), Uo), 1e-11)
+            # 21 solves per trajectory; the FP32 inner iterations may differ from FP64 by one here and there
             bound("CG iterations rel diff (4x512^2 batched mixed vs oracle FP64)",
-                  abs(i.cg_iterations - ito) / ito, 0.05)
+                  abs(i.cg_iterations - ito) / ito, 2e-3)
             note("dH (4x512^2 batched)", i.dH)
     note("accepted of 8 (4x512^2 batched)", accepted)
 
@@ -115,13 +115,13 @@ def test_cg_large_vs_oracle(thermalised, prec, L):
         # the residual the reference's stop rule asks for, evaluated by the oracle in FP64
         bound(f"CG {prec} {L}^2 oracle-evaluated |b-Ax|/|b|", res_g, 1.0e-12)
         # solution difference, L2-relative; the amplification err / (res_g + res_o) is at most kappa
-        bound(f"CG {prec} {L}^2 |x-x_o|/|x_o|", err, 1e-9)
+        bound(f"CG {prec} {L}^2 |x-x_o|/|x_o|", err, 1e-14 if prec == "f64" else 1e-13)
         note(f"CG {prec} {L}^2 amplification err/(res_g+res_o)", err / (res_g + res_o))
         note(f"CG {prec} {L}^2 max-abs rel", rel(xg, xo))
         if prec == "f64":
-            bound(f"CG f64 {L}^2 iterations |it-it_o|", abs(it - ito), 2)
+            bound(f"CG f64 {L}^2 iterations |it-it_o|", abs(it - ito), 1)
         else:
-            bound(f"CG mixed {L}^2 iterations rel diff", abs(it - ito) / ito, 0.05)
+            bound(f"CG mixed {L}^2 iterations rel diff", abs(it - ito) / ito, 0.01)
         note(f"CG {prec} {L}^2 iterations (gpu, oracle)", [it, ito])
     finally:
         qed2d.set_precision("f64")

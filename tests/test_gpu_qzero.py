@@ -39,8 +39,8 @@ def test_qzero_pure_gauge_chain():
         _, Uq, aq, hi, hf = o.hmc_gauge(Uo, EPS, NS, mom0, u, integrator=O_OMF4, qzero=True)
         _, Un, an, _, _ = o.hmc_gauge(Uo, EPS, NS, mom0, u, integrator=O_OMF4, qzero=False)
         assert info.accepted == aq == acc[0], t
-        bound("qzero gauge dH abs", abs(info.dH - (hf - hi)), 1e-10)
-        bound("qzero gauge links rel", rel(to_host(Ud), Uq), 1e-12)
+        bound("qzero gauge dH abs", abs(info.dH - (hf - hi)), 5e-12)
+        bound("qzero gauge links rel", rel(to_host(Ud), Uq), 5e-13)
         if an and not aq:
             vetoed += 1
             assert abs(o.qtop(Un)) > 0.1
@@ -73,8 +73,8 @@ def test_qzero_nf2_chain(prec):
             _, Uq, aq, hi, hf, _ = o.hmc_nf2(Uo, am0, EPS, NS, 10000, 1e-24, mom0, noise, u, qzero=True)
             _, Un, an, _, _, _ = o.hmc_nf2(Uo, am0, EPS, NS, 10000, 1e-24, mom0, noise, u, qzero=False)
             assert info.accepted == aq, t
-            bound(f"qzero nf2 {prec} dH abs", abs(info.dH - (hf - hi)), 1e-9)
-            bound(f"qzero nf2 {prec} links rel", rel(to_host(Ud), Uq), 1e-10)
+            bound(f"qzero nf2 {prec} dH abs", abs(info.dH - (hf - hi)), 1e-9 if prec == "mixed" else 2e-10)
+            bound(f"qzero nf2 {prec} links rel", rel(to_host(Ud), Uq), 5e-11 if prec == "mixed" else 2e-12)
             if an and not aq:
                 vetoed += 1
                 assert np.array_equal(Uq, Uo)
@@ -108,7 +108,7 @@ def test_qzero_batched_replicas():
             _, _, an, _, _, _ = o.hmc_nf2(Uo[r], am0, EPS, NS, 10000, 1e-24, mom0, noise, u, qzero=False)
             assert infos[r].accepted == aq, (t, r)
             bound("qzero batched dH abs", abs(infos[r].dH - (hf - hi)), 1e-9)
-            bound("qzero batched links rel", rel(to_host(U[r]), Uq), 1e-10)
+            bound("qzero batched links rel", rel(to_host(U[r]), Uq), 5e-11)
             vetoed += int(an and not aq)
             accepted += aq
             Uo[r] = Uq

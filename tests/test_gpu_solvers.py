@@ -2,13 +2,15 @@
 pseudofermion generation, power method, LuscherZ, reweighting factor) against
 the CPU oracle on identical seeded inputs.
 
-Tolerances (the solution error of a CG stopped at |r|^2 < eps |b|^2 is bounded by
-the condition number times the residual, so solutions are compared through
-their residual and against the oracle's solution):
-  * FP64 and reference-structured paths: |x_gpu - x_oracle| / |x_oracle| < 1e-9
-    at eps = 1e-24 (relative residual 1e-12);
-  * mixed FP32/FP64 path: the same bound -- the final solve meets the FP64
-    residual, only its iteration count differs."""
+Tolerances (each about 10x the error measured on a B200, recorded through
+helpers.bound; the solution error of a CG stopped at |r|^2 < eps |b|^2 is at most
+the condition number times the residual, but two solvers that follow the same
+Krylov recurrences agree far closer than that):
+  * FP64 and reference-structured paths, eps = 1e-24 (relative residual 1e-12):
+    max|x_gpu - x_oracle| / max|x_oracle| < 1e-13 (the north star asks 1e-12),
+    iteration counts within 1;
+  * mixed FP32/FP64 path: 5e-12 -- the final solve meets the same FP64 residual
+    along a different (FP32) Krylov path."""
 import numpy as np
 import pytest
 
@@ -45,12 +47,14 @@ def test_cg_method1(q, prec, L1, L2, unitary):
     assert st == 0
     x = q.cfield(L1, L2)
     it = q.CG(x, to_dev(U), to_dev(b), am0, 20000, 1e-24, q.gamm5Dw_sqr_msq, prm, None)
-    bound("rel err vs xo", rel(to_host(x), xo), 1e-9)
+    # FP64 paths: the north star asks 1e-12; measured <= 2e-15.  Mixed: the same
+    # FP64 stop rule through a different Krylov path; measured <= 6e-13
+    bound(f"CG method 1 {prec} vs oracle", rel(to_host(x), xo), 1e-13 if prec != "mixed" else 5e-12)
     # residual of the GPU solution, evaluated by the oracle
     r = b - o.g5dw_sqr(U, to_host(x), am0)
     assert np.linalg.norm(r) ** 2 < 1e-23 * np.linalg.norm(b) ** 2
     if prec in ("f64", "plain"):
-        bound("abs(it - ito)", abs(it - ito), 2)
+        bound("CG method 1 iterations |it - it_oracle|", abs(it - ito), 1)
     else:
         assert it <= 2 * ito
 
@@ -66,15 +70,15 @@ def test_cg_method2_shift_and_guess(q, prec):
     st, xo, ito, _ = o.cg(U, b, am0, 20000, 1e-24, mu=mu)
     x = q.cfield(L1, L2)
     q.CG(x, to_dev(U), to_dev(b), am0, mu, 20000, 1e-24, q.gamm5Dw_sqr_musq, prm, None)
-    bound("rel err vs xo", rel(to_host(x), xo), 1e-10)
+    bound(f"CG method 2 {prec} vs oracle", rel(to_host(x), xo), 5e-12)
     # warm start from a perturbed solution (src/QED2dSolver.jl:263-271)
     g0 = xo + 1e-3 * cgauss(L1, L2, 9, 3)
     st, xo2, ito2, _ = o.cg(U, b, am0, 20000, 1e-24, mu=mu, guess=g0)
     x = to_dev(g0)
     it = q.CG(x, to_dev(U), to_dev(b), am0, mu, 20000, 1e-24, q.gamm5Dw_sqr_musq, prm, None, so_as_guess=True)
-    bound("rel err vs xo2", rel(to_host(x), xo2), 1e-10)
+    bound(f"CG method 2 warm start {prec} vs oracle", rel(to_host(x), xo2), 1e-13 if prec != "mixed" else 5e-12)
     if prec != "mixed":
-        bound("abs(it - ito2)", abs(it - ito2), 2)
+        bound("CG method 2 warm start iterations |it - it_oracle|", abs(it - ito2), 1)
     # a guess that already solves the system returns after 0 iterations
     it = q.CG(x, to_dev(U), to_dev(b), am0, mu, 20000, 1e-20, q.gamm5Dw_sqr_musq, prm, None, so_as_guess=True)
     assert it == 0
@@ -92,7 +96,7 @@ def test_multishift_vs_sequential_oracle(q):
     q.multishift_CG(xs, to_dev(U), to_dev(b), am0, mus, 20000, 1e-24, prm)
     for mu, x in zip(mus, xs):
         st, xo, _, _ = o.cg(U, b, am0, 20000, 1e-24, mu=mu)
-        bound("rel err vs xo", rel(to_host(x), xo), 1e-9)  # mu
+        bound("multishift vs sequential oracle CG", rel(to_host(x), xo), 5e-12)  # mu
 
 
 @pytest.mark.parametrize("prec", ["f64", "plain"])
@@ -112,12 +116,12 @@ def test_multicg_rational_pf(q, prec):
     Ud, Xd = to_dev(U), to_dev(X)
     so = q.cfield(L, L)
     q.MultiCG(so, Ud, Xd, am0, 10000, 1e-25, q.gamm5Dw_sqr_musq, rp, prm)
-    bound("rel err vs o.multi_cg(U, X, am0, 10000, 1e-25, r)[1]", rel(to_host(so), o.multi_cg(U, X, am0, 10000, 1e-25, r)[1]), 1e-10)
+    bound("MultiCG vs oracle", rel(to_host(so), o.multi_cg(U, X, am0, 10000, 1e-25, r)[1]), 1e-14)
     q.R(so, Ud, Xd, am0, 10000, 1e-25, q.gamm5Dw_sqr_musq, rp, prm)
-    bound("rel err vs o.rational(U, X, am0, 10000, 1e-25, r)[1]", rel(to_host(so), o.rational(U, X, am0, 10000, 1e-25, r)[1]), 1e-10)
+    bound("R vs oracle", rel(to_host(so), o.rational(U, X, am0, 10000, 1e-25, r)[1]), 1e-14)
     F = q.cfield(L, L)
     q.generate_pseudofermion_(F, Ud, Xd, am0, 10000, 1e-25, prm, None, rp)
-    bound("rel err vs o.pf_generate(U, X, am0, 10000, 1e-25, r)[1]", rel(to_host(F), o.pf_generate(U, X, am0, 10000, 1e-25, r)[1]), 1e-10)
+    bound("generate_pseudofermion! vs oracle", rel(to_host(F), o.pf_generate(U, X, am0, 10000, 1e-25, r)[1]), 1e-14)
     Z = q.cfield(L, L)
     q.LuscherZ(Z, Ud, Xd, am0, 10000, 1e-25, rp, prm)
     st, Zo = o.luscher_z(U, X, am0, 10000, 1e-25, r)
@@ -145,9 +149,9 @@ def test_power_method(q, tag):
     b0 = cgauss(L1, L2, 77, 4, counter=0)   # stream QED2D_STREAM_POWER, first counter
     omin, omax = o.power_method(U, m0, 4000, b0)
     emin, emax = float(g["eig_min_unitary"]), float(g["eig_max_unitary"])
-    bound("abs(lmax - omax)", abs(lmax - omax), 1e-10 * omax)
-    bound("abs(lmax - emax)", abs(lmax - emax), 1e-6 * emax)
-    bound("abs(lmin - emin)", abs(lmin - emin), 1e-3 * emax)
+    bound("power_method lambda_max rel vs oracle", abs(lmax - omax) / omax, 1e-14)
+    bound("power_method lambda_max rel vs dense spectrum", abs(lmax - emax) / emax, 1e-13)
+    bound("power_method lambda_min vs dense spectrum (rel to lambda_max)", abs(lmin - emin) / emax, 1e-10)
 
 
 def test_reweighting_factor_vs_oracle(q):
@@ -162,7 +166,7 @@ def test_reweighting_factor_vs_oracle(q):
     W = q.reweighting_factor(to_dev(U), 0.3, 10000, 1e-25, prm, None, rp)
     noise = cgauss(L, L, 2024, 64, counter=0)[None]
     st, Wo = o.reweighting_factor(U, 0.3, 10000, 1e-25, r, noise)
-    bound("abs(W - Wo)", abs(W - Wo), 1e-10 * abs(Wo))
+    bound("reweighting_factor rel vs oracle", abs(W - Wo) / abs(Wo), 1e-13)
 
 
 def test_zero_source_and_errors(q):
@@ -262,8 +266,8 @@ def test_cluster_schedule_matches_grid_schedule(L1, L2, prec):
             x = qed2d.cfield(L1, L2)
             it = qed2d.CG(x, U, src, 0.15, 20000, 1e-24, qed2d.gamm5Dw_sqr_msq, prm, None)
             out.append((it, to_host(x)))
-        bound("rel err vs out[0][1]", rel(out[1][1], out[0][1]), 1e-9)
-        bound("abs(out[0][0] - out[1][0])", abs(out[0][0] - out[1][0]), max(2, out[0][0] // 20))
+        bound(f"CG {prec} one-cluster vs grid schedule", rel(out[1][1], out[0][1]), 2e-12)
+        bound("CG one-cluster vs grid schedule iterations", abs(out[0][0] - out[1][0]), 2)
         x2 = qed2d.cfield(L1, L2)   # repeated cluster solves are bitwise identical
         qed2d.CG(x2, U, src, 0.15, 20000, 1e-24, qed2d.gamm5Dw_sqr_msq, prm, None)
         assert np.array_equal(to_host(x2), out[1][1])
@@ -297,12 +301,12 @@ def test_multishift_schedules(L1, L2):
         assert out[0][0] == out[1][0]
         for a, b in zip(out[0][1], out[1][1]):
             assert np.array_equal(a, b)
-        bound("abs(out[2][0] - out[1][0])", abs(out[2][0] - out[1][0]), 2)
+        bound("multishift one-cluster vs grid iterations", abs(out[2][0] - out[1][0]), 1)
         for a, b in zip(out[2][1], out[1][1]):
-            bound("rel err vs b", rel(a, b), 1e-9)
+            bound("multishift one-cluster vs grid solution", rel(a, b), 1e-13)
         y, b = qed2d.cfield(L1, L2), to_host(src)
         for mu, x in zip(mus, out[1][1]):   # (A + mu^2) x = src
             qed2d.gamm5Dw_sqr_musq(y, None, U, to_dev(x), am0, mu, prm)
-            bound("rel err vs b", rel(to_host(y), b), 1e-9)  # mu
+            bound("multishift residual |(A + mu^2) x - b| / |b|", rel(to_host(y), b), 1e-11)  # mu
     finally:
         qed2d.set_schedule(prm, -1, "multishift")
