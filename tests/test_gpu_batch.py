@@ -215,9 +215,9 @@ def test_batch_reduction_schedules_give_identical_bits():
 def test_batch_tile_heights(L1, L2):
     """The equal-size solver's tile heights (tiles of 32 x 4, 8, 16 sites):
     within a height the three schedules give identical bits; across heights the
-    block partials are grouped differently, so solutions agree to the solver's
-    accuracy (1e-9 relative) and iteration counts within 5%.  The first solve
-    tunes height and schedule together."""
+    block partials are grouped differently, so the bits differ: solutions agree
+    to 1e-13 relative (measured on a B200: 2.6e-16) and iteration counts within
+    5%.  The first solve tunes height and schedule together."""
     import qed2d
     nrep = 3
     b = qed2d.Batch(nrep, L1, L2, 4.0)
@@ -242,7 +242,7 @@ def test_batch_tile_heights(L1, L2):
             assert per[0][0] == per[i][0] and np.array_equal(per[0][1], per[i][1]), (rows, i)
         res[rows] = per[0]
     for rows in (4, 16):
-        bound("tile height vs 32x8 solution rel", rel(res[rows][1], res[8][1]), 1e-9)
+        bound("tile height vs 32x8 solution rel", rel(res[rows][1], res[8][1]), 1e-13)
         for r in range(nrep):
             assert abs(res[rows][0][r] - res[8][0][r]) <= max(3, res[8][0][r] // 20), (rows, r)
     b.tile_rows = -1

@@ -44,7 +44,7 @@ def test_hmc_gauge(q, integ):
         st, Uo, acco, hi, hf = o.hmc_gauge(Uo, 0.05, 10, mom0, u,
                                             integrator=O_OMF4 if integ == "omf4" else O_LEAPFROG)
         bound("HMC! gauge H_ini rel vs oracle", abs(info.hini - hi) / abs(hi), 1e-14)
-        bound("HMC! gauge dH abs vs oracle", abs(info.dH - (hf - hi)), 1e-10)
+        bound("HMC! gauge dH abs vs oracle", abs(info.dH - (hf - hi)), 2e-9)
         assert info.accepted == acco == acc[0]
         bound("HMC! gauge links vs oracle", rel(to_host(Ud), Uo), 1e-12)
         bound("HMC! gauge Qtop abs vs oracle", abs(info.qtop - o.qtop(Uo)), 1e-12)
