@@ -51,10 +51,19 @@ B_MIXED_SETUP = 112.0    # |b|^2, x=0, r32 = b/|b|, x32 = 0
 B_F64_ITER = 384.0       # FP64 fused iteration: phase A 160 B + phase B 224 B
 B_DSLASH_F64 = 96.0      # g5Dw apply, FP64: spinor in 32 + links 32 + out 32
 B_DSLASH_C64 = 48.0      # g5Dw apply on complex64 fields: spinor in 16 + links 16 + out 16
-# DRAM bytes (read + write) per site-iteration of k_u_cg_mixed at 4 x 512^2, from an
-# ncu capture of one 100-iteration launch (6.400 GB over 1,048,576 sites x 100);
-# traffic grows in proportion to the iterations at fixed size
-U_DRAM_PER_SITE_ITER = 61.0
+# Roofline units of the headline kernel.  Algorithmic bytes per site of one CG
+# iteration on (g5Dw)^2: 256 B in FP32 (two applies at 48 B + ten vector passes
+# at 16 B), 512 B in FP64 -- an FP64 reliable update is counted as one FP64
+# iteration.  (The fused solver moves 176 B per FP32 iteration by design; that
+# figure is reported beside.)
+B_ITER_F32 = 256.0
+B_ITER_F64 = 512.0
+# Measured traffic per site-iteration of k_u_cg_mixed at 4 x 512^2, from one ncu
+# capture of a 100-iteration launch of the current kernel: DRAM read + write
+# (6.529 GB over 1,048,576 sites x 100) and L1 <-> L2 (18.19 GB read + 6.60 GB
+# written); both grow in proportion to the iterations at fixed size
+U_DRAM_PER_SITE_ITER = 62.3
+U_L2_PER_SITE_ITER = 236.0
 ENS_NS, ENS_EPS = 10, 0.1   # replica ensemble: leapfrog ns=10, eps=0.1
 CPU_TRAJ = 2                # trajectories of the GPU arm's CPU-baseline sample
 
@@ -435,20 +444,29 @@ def run_ours(args):
         kern.append((a0.elapsed_time(a1) / 1e3, its, upd))
     t_k, its, upd = min(kern[1:], key=lambda z: z[0])
     V = L * L
-    bytes_k = V * sum(B_MIXED_SETUP + i * B_MIXED_ITER + u * B_MIXED_UPDATE for i, u in zip(its, upd))
+    bytes_k = V * sum(i * B_ITER_F32 + u * B_ITER_F64 for i, u in zip(its, upd))
+    fused_k = V * sum(B_MIXED_SETUP + i * B_MIXED_ITER + u * B_MIXED_UPDATE for i, u in zip(its, upd))
     achieved = bytes_k / t_k / 1e9
     traffic = V * sum(its) * U_DRAM_PER_SITE_ITER
+    l2_bytes = V * sum(its) * U_L2_PER_SITE_ITER
+    l2_peak = l2_copy_peak(torch, dev)
     roofline = {"kernel": "k_u_cg_mixed", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                 "dram_achieved": traffic / t_k / 1e9, "dram_frac": traffic / t_k / 1e9 / peak,
+                "fused_model_achieved": fused_k / t_k / 1e9,
+                "l2": {"achieved": l2_bytes / t_k / 1e9, "peak": l2_peak, "unit": "GB/s",
+                       "frac": l2_bytes / t_k / 1e9 / l2_peak, "peak_kind": "measured in this run (L2-resident copy)"},
+                "launch_us": t_k * 1e6,
                 "schedule": {0: "last block publishes the sums", 1: "every block sums",
                              4: "independent replicas (a barrier per replica)"}.get(batch.schedule, "untuned"),
+                "tiling": {"rows": batch.tiling[0], "walk": batch.tiling[1]},
                 "note": f"one launch = one solve of all {B} replicas: per replica iterations {min(its)}-{max(its)} "
-                        f"x {B_MIXED_ITER:.0f} B/site + reliable updates {min(upd)}-{max(upd)} x "
-                        f"{B_MIXED_UPDATE:.0f} B/site; {B} x {L}^2 working set partly L2-resident, so achieved "
-                        f"(algorithmic bytes) can exceed the copy bandwidth; traffic = ncu DRAM bytes per "
-                        f"site-iteration at this size x the solve's site-iterations, dram_achieved = traffic / time "
-                        f"(the kernel is latency-bound)"}
+                        f"x {B_ITER_F32:.0f} B/site + reliable updates {min(upd)}-{max(upd)} x {B_ITER_F64:.0f} "
+                        f"B/site (algorithmic); the {B} x {L}^2 FP32 working set is mostly L2-resident, so the "
+                        f"algorithmic rate exceeds the DRAM copy bandwidth; traffic = ncu DRAM bytes per "
+                        f"site-iteration x the solve's site-iterations (dram_achieved = traffic / time); l2 = "
+                        f"ncu L1<->L2 bytes per site-iteration x site-iterations against an L2-resident copy "
+                        f"measured in this run; neither is saturated: the kernel is latency- and barrier-bound"}
 
     # --- single-chain baselines on the same field and draws as replica 0's first
     # timed step: mixed (no batching), fused FP64, and the plain FP64 GPU path

@@ -81,10 +81,57 @@ __device__ __forceinline__ bool ureduce(GridSync& gs, double v, const UCGP& P, d
                                         int* s_fl, int kind, int k) {
     __shared__ int s_last, s_bits, s_ok;
     __shared__ double s_red[kUniformReps];
-    const int myr = RS == 2 ? blockIdx.x / P.bpr : 0;
+    const int myr = RS >= 2 ? blockIdx.x / P.bpr : 0;
     const int buf = gs.nred++ & 1;
     double* part = P.part + (size_t)buf * P.bpr * P.g.B;
     double* red = P.red + (size_t)buf * P.g.B;
+    if constexpr (RS == 3) {
+        // Independent replicas, lean: the same additions in the same order as
+        // RS = 2 (so the same bits), with two block barriers instead of seven.
+        // Every warp reduces its value by shuffles; after one __syncthreads
+        // (which orders the block's stores before thread 0's release-add) warp 0
+        // sums the warp values, publishes the block partial and arrives, polls,
+        // sums the replica's partials, and thread 0 steps the replica's
+        // recurrences and sets the flags; one more __syncthreads releases the
+        // block.
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) smem[warp] = v;
+        __syncthreads();
+        gs.target += gs.n();
+        if (warp == 0) {
+            double s = lane < nw ? smem[lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            int ok = 1;
+            if (lane == 0) {
+                part[blockIdx.x] = s;
+                red_release_add_u64(gs.arrivals, 1ULL);
+                gs.poll(gs.arrivals);
+                ok = ld_volatile_int(gs.err) == 0;
+            }
+            __syncwarp();   // orders lane 0's acquire before the other lanes' partial loads
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            double t = 0.0;
+            for (int i = lane; i < P.bpr; i += 32) t += __ldcg(part + (size_t)myr * P.bpr + i);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+            if (lane == 0) {
+                int fl[FL_N] = {0, 0, 0};
+                RepState st = s_st[myr];
+                rep_step(st, kind, t, k, P.eps, P.delta2, P.maxiter, fl);
+                s_st[myr] = st;
+                clear_flags(kind, s_fl);
+                s_fl[FL_ACT] |= fl[FL_ACT];
+                s_fl[FL_UPD] |= fl[FL_UPD];
+                s_fl[FL_R4] |= fl[FL_R4];
+                s_ok = ok;
+            }
+        }
+        __syncthreads();
+        return s_ok != 0;
+    }
     double vv[1] = {v};
     block_sum<1>(vv, smem);
     if (threadIdx.x == 0) {
@@ -302,23 +349,34 @@ __device__ __forceinline__ bool u_body(const UCGP& P, GridSync& gs, int& k, doub
 }
 #undef FOR_MY_UTILES
 
-// Tiles of 32 x TYv sites, TYv = 4, 8 or 16 (blocks of 128, 256 or 512 threads):
-// the tile height sets how many blocks share a replica's tiles (and its
-// barriers) and how many tiles each block walks; the register budget (64 per
-// thread) is the same for all three.  Different heights group the partial sums
-// differently, so they agree to the solver's accuracy, not bit for bit.
-template <int RS, int TYv>
-__global__ void __launch_bounds__(32 * TYv, 32 / TYv) k_u_cg_mixed(const UCGP P) {
+}  // namespace qed2d
+
+#include "batch_cg_walk.cuh"
+
+namespace qed2d {
+
+// Tiles of 32 x TYv sites, TYv = 4, 8 or 16.  WALK = false: blocks of 32 * TYv
+// threads (128, 256 or 512), one site per thread per tile (u_body); WALK = true:
+// blocks of 8 warps, each warp walking whole tiles down their rows (w_body,
+// batch_cg_walk.cuh).  The tile height sets how many blocks share a replica's
+// tiles (and its barriers) and how many tiles each block walks; the register
+// budget (64 per thread) is the same for all.  Different heights and mappings
+// group the partial sums differently, so they agree to rounding, not bit for bit.
+template <int RS, int TYv, bool WALK = false>
+__global__ void __launch_bounds__(WALK ? 32 * kWalkWarps : 32 * TYv, WALK ? 3 : 32 / TYv)
+    k_u_cg_mixed(const UCGP P) {
     __shared__ double smem[32];
     __shared__ RepState s_st[kUniformReps];
     __shared__ int s_fl[FL_N];
     if (threadIdx.x < FL_N) s_fl[threadIdx.x] = 0;
     __syncthreads();
     int k = 0;
-    if constexpr (RS == 2) {   // independent replicas: a barrier per replica; its blocks leave when it is done
+    if constexpr (RS >= 2) {   // independent replicas: a barrier per replica; its blocks leave when it is done
         const int myr = blockIdx.x / P.bpr;
         GridSync gs{P.rbar + 16 * myr, &P.ctl->gen, &P.ctl->err, (unsigned)P.bpr};
-        const bool ok = u_body<RS, TYv>(P, gs, k, smem, s_st, s_fl);
+        bool ok;
+        if constexpr (WALK) ok = w_body<RS, TYv>(P, gs, k, smem, s_st, s_fl);
+        else ok = u_body<RS, TYv>(P, gs, k, smem, s_st, s_fl);
         if (blockIdx.x == myr * P.bpr && threadIdx.x == 0) {   // the replica's first block
             if (ok) P.st_out[myr] = s_st[myr];
             DevCtl* c = P.ctl;
@@ -328,7 +386,9 @@ __global__ void __launch_bounds__(32 * TYv, 32 / TYv) k_u_cg_mixed(const UCGP P)
         return;
     }
     GridSync gs{&P.ctl->bar, &P.ctl->gen, &P.ctl->err};
-    const bool ok = u_body<RS, TYv>(P, gs, k, smem, s_st, s_fl);
+    bool ok;
+    if constexpr (WALK) ok = w_body<RS, TYv>(P, gs, k, smem, s_st, s_fl);
+    else ok = u_body<RS, TYv>(P, gs, k, smem, s_st, s_fl);
     if (blockIdx.x == 0) {
         if (ok)   // every block holds the same records: block 0 stores them
             for (int r = threadIdx.x; r < P.g.B; r += blockDim.x) P.st_out[r] = s_st[r];

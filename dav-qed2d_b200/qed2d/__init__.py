@@ -747,9 +747,10 @@ class Batch:
     @property
     def schedule(self) -> int:
         """Schedule of the batched solver: -1 untuned; equal-size batches of at
-        most 64 replicas 0/1 (reduction schedules) or 4 (independent replicas,
-        a barrier per replica), all three with the same bits; other batches 2
-        (one launch with grid barriers) or 3 (one thread-block cluster per replica)."""
+        most 64 replicas 0/1 (reduction schedules), 4 (independent replicas, a
+        barrier per replica) or 5 (the same with a leaner reduction), all four
+        with the same bits; other batches 2 (one launch with grid barriers) or 3
+        (one thread-block cluster per replica)."""
         v = C.c_int(0)
         check(lib().qed2d_batch_get_schedule(self.h, C.byref(v)), "batch_get_schedule")
         return v.value
@@ -759,16 +760,24 @@ class Batch:
         check(lib().qed2d_batch_set_schedule(self.h, int(s)), "batch_set_schedule")
 
     @property
-    def tile_rows(self) -> int:
-        """Tile height of the equal-size solver (tiles of 32 x rows sites): 4, 8
-        or 16, tuned with the schedule on the first solve (-1 until then)."""
-        v = C.c_int(0)
-        check(lib().qed2d_batch_get_tile_rows(self.h, C.byref(v)), "batch_get_tile_rows")
-        return v.value
+    def tiling(self):
+        """(rows, walk) of the equal-size solver: tiles of 32 x rows sites (4, 8
+        or 16), walk = False for one site per thread per tile, True for warps
+        walking whole tiles down their rows; tuned with the schedule on the first
+        solve ((-1, -1) until then).  Set a pair to fix it, or -1 to tune again."""
+        r, w = C.c_int(0), C.c_int(0)
+        check(lib().qed2d_batch_get_tiling(self.h, C.byref(r), C.byref(w)), "batch_get_tiling")
+        return (r.value, w.value if w.value < 0 else bool(w.value))
 
-    @tile_rows.setter
-    def tile_rows(self, rows: int) -> None:
-        check(lib().qed2d_batch_set_tile_rows(self.h, int(rows)), "batch_set_tile_rows")
+    @tiling.setter
+    def tiling(self, value) -> None:
+        rows, walk = (value, False) if isinstance(value, int) else value
+        check(lib().qed2d_batch_set_tiling(self.h, int(rows), int(bool(walk))), "batch_set_tiling")
+
+    @property
+    def tile_rows(self) -> int:
+        """Tile height of the tiling in use (-1 until tuned)."""
+        return self.tiling[0]
 
     def field(self, dtype=torch.complex128):
         if self.uniform:
