@@ -1135,7 +1135,8 @@ int r_solve(qed2d_batch* h, const double2* U, const float4* U32, const double2* 
             if (sched >= 4) QCHECK(cudaMemsetAsync(h->d_ubar, 0, sizeof(unsigned long long) * 16 * h->nrep, h->stream));
             void* uargs[] = {(void*)&q};
             QCHECK(cudaLaunchCooperativeKernel(uniform_kernel(sched, v.rows, v.walk), dim3((unsigned)v.grid),
-                                               dim3((unsigned)v.threads), uargs, 0, h->stream));
+                                               dim3((unsigned)v.threads), uargs, v.walk ? kWalkSmem : 0,
+                                               h->stream));
             count_launch();
             return QED2D_OK;
         };
@@ -1284,11 +1285,13 @@ int batch_setup(qed2d_batch* h, const int* L1, const int* L2, const double* beta
         const RepInfo& R0 = h->reps[0];
         for (const UShape sh : kUShapes) {
             const int threads = sh.walk ? TX * kWalkWarps : TX * sh.rows;
+            const size_t dsmem = sh.walk ? kWalkSmem : 0;
             int per_smu = 1 << 30;
             for (int sched : {0, 1, 4, 5}) {
+                const void* kern = uniform_kernel(sched, sh.rows, sh.walk);
+                if (dsmem) QCHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem));
                 int n = 0;
-                QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, uniform_kernel(sched, sh.rows, sh.walk),
-                                                                     threads, 0));
+                QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, threads, dsmem));
                 per_smu = std::min(per_smu, n);
             }
             const long long maxgu = std::min<long long>((long long)per_smu * h->num_sms, kMaxPartBlocks);

@@ -12,7 +12,7 @@
 // p = r + beta p_old is formed once per site instead of five times, and the
 // links of x - 1 come from the lane to the left.  Lanes 0 and 31 (and the lane
 // whose right neighbour wraps around the lattice) load their missing
-// neighbour.  The data of the next steps is requested one step ahead.
+// neighbour.  Rows are prefetched through a per-warp ring in shared memory.
 //
 // Every site's FP32 values (p, g5Dw p, the r and x updates) are computed by the
 // same operations as in u_body, so they are bitwise the same for the same
@@ -62,12 +62,37 @@ __device__ __forceinline__ int wx(const UGeom& g, const WalkCol& w, int c, int i
     return c + g.L1 * (w.rowbase + i2);
 }
 
+// Row prefetch: each warp streams its tile's rows (the row above the tile, its
+// rows, the row below) through a ring of kWalkDepth stages in shared memory with
+// cp.async (16 bytes per lane per array, through L2), so rows are requested
+// kWalkDepth - 1 steps before they are used without holding registers.  A lane
+// reads back only the slots it copied itself, so the ring needs no barrier: the
+// lane's cp.async.wait_group is enough.  A stage is refilled one step after it
+// was read, once every value taken from it has been used.  Per stage and warp:
+// three 32-lane arrays (phase A: r, p_old, links; phase B: t, r, links) and five
+// edge slots (lane 0: the spinor arrays and links of column x - 1; the lane
+// whose right neighbour is not lane + 1: the spinor arrays of column x + 1).
+constexpr int kWalkDepth = 4;
+constexpr int kRingStage = 3 * 32 + 5;   // float4 slots per stage and warp
+constexpr size_t kWalkSmem = sizeof(float4) * kWalkWarps * kWalkDepth * kRingStage;
+
+__device__ __forceinline__ void cp16(float4* dst, const float4* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // Phase A: p = r + beta p_old, t = g5Dw p; returns this thread's sum of |t|^2.
 template <int TYv>
 __device__ __forceinline__ float walk_phase_a(const UCGP& P, int myr, const TileRange& TR, float4* qn,
-                                              const float4* qo, float beta, bool use_p, float m2f) {
+                                              const float4* qo, float beta, bool use_p, float m2f, float4* ring) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const UGeom& g = P.g;
+    float4* wr = ring + warp * (kWalkDepth * kRingStage);
     float f = 0.f;
     auto form = [&](float4 r, float4 po) -> Pair<float> {   // as SpAxpy::ld
         Pair<float> v = upk(r);
@@ -78,52 +103,81 @@ __device__ __forceinline__ float walk_phase_a(const UCGP& P, int myr, const Tile
         }
         return v;
     };
-    auto ldp = [&](int x) -> Pair<float> { return form(P.r32[x], use_p ? qo[x] : make_float4(0, 0, 0, 0)); };
     for (int tt = TR.lo + warp; tt < TR.hi; tt += kWalkWarps) {
         const int t2 = tt / TR.nt1, t1 = tt - t2 * TR.nt1;
         const WalkCol w = walk_col(g, myr, t1, t2, TYv, lane);
-        const int im = w.r0 == 0 ? g.L2 - 1 : w.r0 - 1;
-        Pair<float> pm = ldp(wx(g, w, w.c1, im));
-        Pair<float> pc = ldp(wx(g, w, w.c1, w.r0));
-        float2 u2m = LkF{P.U32}.u2(wx(g, w, w.c1, im));
-        float4 uc = __ldg(P.U32 + wx(g, w, w.c1, w.r0));
-        // the next row's raw spinor data, requested one step ahead
-        int in = (w.r0 + 1 == g.L2) ? 0 : w.r0 + 1;
-        float4 nr = P.r32[wx(g, w, w.c1, in)];
-        float4 np = use_p ? qo[wx(g, w, w.c1, in)] : make_float4(0, 0, 0, 0);
-        for (int j = 0; j < w.nrow; j++) {
-            const int i2 = w.r0 + j;
-            const int x = wx(g, w, w.c1, i2);
-            const Pair<float> pn = form(nr, np);   // row i2 + 1
-            float4 un = uc;
-            if (j + 1 < w.nrow) {   // the links of row i2 + 1, the spinors of row i2 + 2
-                un = __ldg(P.U32 + wx(g, w, w.c1, in));
-                const int i3 = (in + 1 == g.L2) ? 0 : in + 1;
-                const int x3 = wx(g, w, w.c1, i3);
-                nr = P.r32[x3];
-                if (use_p) np = qo[x3];
-                in = i3;
+        const int nstream = w.nrow + 2;   // the row above, the tile's rows, the row below
+        const bool iss_p = w.edge_p && w.ok;
+        auto row_of = [&](int k) {   // stream position k -> lattice row (periodic)
+            int i2 = w.r0 - 1 + k;
+            return i2 < 0 ? i2 + g.L2 : (i2 >= g.L2 ? i2 - g.L2 : i2);
+        };
+        auto issue = [&](int k) {
+            if (k < nstream) {
+                float4* st = wr + (k % kWalkDepth) * kRingStage;
+                const int xr = wx(g, w, 0, row_of(k));
+                cp16(st + lane, P.r32 + xr + w.c1);
+                if (use_p) cp16(st + 32 + lane, qo + xr + w.c1);
+                cp16(st + 64 + lane, P.U32 + xr + w.c1);
+                if (w.edge_m) {
+                    cp16(st + 96, P.r32 + xr + w.m1c);
+                    if (use_p) cp16(st + 97, qo + xr + w.m1c);
+                    cp16(st + 98, P.U32 + xr + w.m1c);
+                }
+                if (iss_p) {
+                    cp16(st + 99, P.r32 + xr + w.p1c);
+                    if (use_p) cp16(st + 100, qo + xr + w.p1c);
+                }
             }
-            Pair<float> p1 = upk(shfl_down4(pk(pc))), m1 = upk(shfl_up4(pk(pc)));
-            float2 u1m = make_float2(__shfl_up_sync(0xffffffffu, uc.x, 1), __shfl_up_sync(0xffffffffu, uc.y, 1));
-            if (w.edge_p) p1 = ldp(x - w.c1 + w.p1c);
+            cp_commit();
+        };
+        for (int k = 0; k < kWalkDepth; k++) issue(k);
+        Pair<float> pm{}, pc{};
+        float2 u2m{};
+        float4 uc{};
+        Pair<float> em{}, ep{};
+        float2 eu{};
+        for (int k = 0; k < nstream; k++) {
+            cp_wait<kWalkDepth - 2>();
+            const float4* st = wr + (k % kWalkDepth) * kRingStage;
+            const Pair<float> pk_ = form(st[lane], use_p ? st[32 + lane] : make_float4(0, 0, 0, 0));
+            const float4 uk = st[64 + lane];
+            Pair<float> emk{}, epk{};
+            float2 euk{};
             if (w.edge_m) {
-                m1 = ldp(x - w.c1 + w.m1c);
-                u1m = LkF{P.U32}.u1(x - w.c1 + w.m1c);
+                emk = form(st[96], use_p ? st[97] : make_float4(0, 0, 0, 0));
+                const float4 q = st[98];
+                euk = make_float2(q.x, q.y);
             }
-            Pair<float> t;
-            g5dw_site<float>(pc.a, pc.b, p1.a, p1.b, m1.a, m1.b, pn.a, pn.b, pm.a, pm.b, make_float2(uc.x, uc.y),
-                             make_float2(uc.z, uc.w), u1m, u2m, m2f, t.a, t.b);
-            if (w.ok) {
-                st_f(qn, x, pc);
-                st_f(P.t32, x, t);
-                f += norm2(t.a) + norm2(t.b);
+            if (w.edge_p) epk = form(st[99], use_p ? st[100] : make_float4(0, 0, 0, 0));
+            if (k >= 2) {   // row k - 1 of the stream = tile row k - 2
+                const int x = wx(g, w, w.c1, w.r0 + k - 2);
+                Pair<float> p1 = upk(shfl_down4(pk(pc))), m1 = upk(shfl_up4(pk(pc)));
+                float2 u1m = make_float2(__shfl_up_sync(0xffffffffu, uc.x, 1), __shfl_up_sync(0xffffffffu, uc.y, 1));
+                if (w.edge_p) p1 = ep;
+                if (w.edge_m) {
+                    m1 = em;
+                    u1m = eu;
+                }
+                Pair<float> t;
+                g5dw_site<float>(pc.a, pc.b, p1.a, p1.b, m1.a, m1.b, pk_.a, pk_.b, pm.a, pm.b,
+                                 make_float2(uc.x, uc.y), make_float2(uc.z, uc.w), u1m, u2m, m2f, t.a, t.b);
+                if (w.ok) {
+                    st_f(qn, x, pc);
+                    st_f(P.t32, x, t);
+                    f += norm2(t.a) + norm2(t.b);
+                }
             }
+            if (k >= 1) issue(k - 1 + kWalkDepth);   // stage of row k - 1: all its values are used
+            if (k >= 1) u2m = make_float2(uc.z, uc.w);
             pm = pc;
-            pc = pn;
-            u2m = make_float2(uc.z, uc.w);
-            uc = un;
+            pc = pk_;
+            uc = uk;
+            em = emk;
+            ep = epk;
+            eu = euk;
         }
+        cp_wait<0>();
     }
     return f;
 }
@@ -132,68 +186,96 @@ __device__ __forceinline__ float walk_phase_a(const UCGP& P, int myr, const Tile
 // returns this thread's sum of |r|^2.
 template <int TYv, bool PEND>
 __device__ __forceinline__ float walk_phase_b(const UCGP& P, int myr, const TileRange& TR, const float4* qn,
-                                              const float4* qo, float alpha, float apend, float m2f) {
+                                              const float4* qo, float alpha, float apend, float m2f, float4* ring) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const UGeom& g = P.g;
+    float4* wr = ring + warp * (kWalkDepth * kRingStage);
     float f = 0.f;
     for (int tt = TR.lo + warp; tt < TR.hi; tt += kWalkWarps) {
         const int t2 = tt / TR.nt1, t1 = tt - t2 * TR.nt1;
         const WalkCol w = walk_col(g, myr, t1, t2, TYv, lane);
-        const int im = w.r0 == 0 ? g.L2 - 1 : w.r0 - 1;
-        float4 tm = P.t32[wx(g, w, w.c1, im)];
-        float4 tc = P.t32[wx(g, w, w.c1, w.r0)];
-        float2 u2m = LkF{P.U32}.u2(wx(g, w, w.c1, im));
-        float4 uc = __ldg(P.U32 + wx(g, w, w.c1, w.r0));
-        int in = (w.r0 + 1 == g.L2) ? 0 : w.r0 + 1;
-        float4 nt = P.t32[wx(g, w, w.c1, in)];
-        for (int j = 0; j < w.nrow; j++) {
-            const int i2 = w.r0 + j;
-            const int x = wx(g, w, w.c1, i2);
-            // this row's vectors
-            Pair<float> r = SpF{P.r32}.ld(x);
-            Pair<float> xv, pc, po;
-            if constexpr (PEND) {
-                xv = SpF{P.x32}.ld(x);
-                pc = SpF{qn}.ld(x);
-                po = SpF{qo}.ld(x);
-            }
-            const float4 tn = nt;
-            float4 un = uc;
-            if (j + 1 < w.nrow) {   // the links of row i2 + 1, t of row i2 + 2
-                un = __ldg(P.U32 + wx(g, w, w.c1, in));
-                const int i3 = (in + 1 == g.L2) ? 0 : in + 1;
-                nt = P.t32[wx(g, w, w.c1, i3)];
-                in = i3;
-            }
-            Pair<float> t1p = upk(shfl_down4(tc)), t1m = upk(shfl_up4(tc));
-            float2 u1m = make_float2(__shfl_up_sync(0xffffffffu, uc.x, 1), __shfl_up_sync(0xffffffffu, uc.y, 1));
-            if (w.edge_p) t1p = SpF{P.t32}.ld(x - w.c1 + w.p1c);
-            if (w.edge_m) {
-                t1m = SpF{P.t32}.ld(x - w.c1 + w.m1c);
-                u1m = LkF{P.U32}.u1(x - w.c1 + w.m1c);
-            }
-            const Pair<float> c = upk(tc), tpn = upk(tn), tmm = upk(tm);
-            Pair<float> a;
-            g5dw_site<float>(c.a, c.b, t1p.a, t1p.b, t1m.a, t1m.b, tpn.a, tpn.b, tmm.a, tmm.b, make_float2(uc.x, uc.y),
-                             make_float2(uc.z, uc.w), u1m, u2m, m2f, a.a, a.b);
-            if (w.ok) {
-                if constexpr (PEND) {   // x += apend p_old, then x += alpha p
-                    xv.a = xv.a + apend * po.a;
-                    xv.b = xv.b + apend * po.b;
-                    xv.a = xv.a + alpha * pc.a;
-                    xv.b = xv.b + alpha * pc.b;
-                    st_f(P.x32, x, xv);
+        const int nstream = w.nrow + 2;
+        const bool iss_p = w.edge_p && w.ok;
+        auto row_of = [&](int k) {
+            int i2 = w.r0 - 1 + k;
+            return i2 < 0 ? i2 + g.L2 : (i2 >= g.L2 ? i2 - g.L2 : i2);
+        };
+        auto issue = [&](int k) {
+            if (k < nstream) {
+                float4* st = wr + (k % kWalkDepth) * kRingStage;
+                const int xr = wx(g, w, 0, row_of(k));
+                cp16(st + lane, P.t32 + xr + w.c1);
+                cp16(st + 32 + lane, P.r32 + xr + w.c1);
+                cp16(st + 64 + lane, P.U32 + xr + w.c1);
+                if (w.edge_m) {
+                    cp16(st + 96, P.t32 + xr + w.m1c);
+                    cp16(st + 98, P.U32 + xr + w.m1c);
                 }
-                r.a = r.a - alpha * a.a;
-                r.b = r.b - alpha * a.b;
-                st_f(P.r32, x, r);
-                f += norm2(r.a) + norm2(r.b);
+                if (iss_p) cp16(st + 99, P.t32 + xr + w.p1c);
             }
+            cp_commit();
+        };
+        for (int k = 0; k < kWalkDepth; k++) issue(k);
+        float4 tm{}, tc{}, uc{}, rc{};
+        float2 u2m{}, eu{};
+        Pair<float> em{}, ep{};
+        for (int k = 0; k < nstream; k++) {
+            cp_wait<kWalkDepth - 2>();
+            const float4* st = wr + (k % kWalkDepth) * kRingStage;
+            const float4 tk = st[lane], rk = st[32 + lane], uk = st[64 + lane];
+            Pair<float> emk{}, epk{};
+            float2 euk{};
+            if (w.edge_m) {
+                emk = upk(st[96]);
+                const float4 q = st[98];
+                euk = make_float2(q.x, q.y);
+            }
+            if (w.edge_p) epk = upk(st[99]);
+            if (k >= 2) {   // tile row k - 2
+                const int x = wx(g, w, w.c1, w.r0 + k - 2);
+                Pair<float> xv, pc, po;
+                if constexpr (PEND) {
+                    xv = SpF{P.x32}.ld(x);
+                    pc = SpF{qn}.ld(x);
+                    po = SpF{qo}.ld(x);
+                }
+                Pair<float> t1p = upk(shfl_down4(tc)), t1m = upk(shfl_up4(tc));
+                float2 u1m = make_float2(__shfl_up_sync(0xffffffffu, uc.x, 1), __shfl_up_sync(0xffffffffu, uc.y, 1));
+                if (w.edge_p) t1p = ep;
+                if (w.edge_m) {
+                    t1m = em;
+                    u1m = eu;
+                }
+                const Pair<float> c = upk(tc), tpn = upk(tk), tmm = upk(tm);
+                Pair<float> a;
+                g5dw_site<float>(c.a, c.b, t1p.a, t1p.b, t1m.a, t1m.b, tpn.a, tpn.b, tmm.a, tmm.b,
+                                 make_float2(uc.x, uc.y), make_float2(uc.z, uc.w), u1m, u2m, m2f, a.a, a.b);
+                if (w.ok) {
+                    if constexpr (PEND) {   // x += apend p_old, then x += alpha p
+                        xv.a = xv.a + apend * po.a;
+                        xv.b = xv.b + apend * po.b;
+                        xv.a = xv.a + alpha * pc.a;
+                        xv.b = xv.b + alpha * pc.b;
+                        st_f(P.x32, x, xv);
+                    }
+                    Pair<float> r = upk(rc);
+                    r.a = r.a - alpha * a.a;
+                    r.b = r.b - alpha * a.b;
+                    st_f(P.r32, x, r);
+                    f += norm2(r.a) + norm2(r.b);
+                }
+            }
+            if (k >= 1) issue(k - 1 + kWalkDepth);
+            if (k >= 1) u2m = make_float2(uc.z, uc.w);
             tm = tc;
-            tc = tn;
-            u2m = make_float2(uc.z, uc.w);
-            uc = un;
+            tc = tk;
+            rc = rk;
+            uc = uk;
+            em = emk;
+            ep = epk;
+            eu = euk;
         }
+        cp_wait<0>();
     }
     return f;
 }
@@ -208,6 +290,7 @@ __device__ __forceinline__ float walk_phase_b(const UCGP& P, int myr, const Tile
 template <int RS, int TYv>
 __device__ __forceinline__ bool w_body(const UCGP& P, GridSync& gs, int& k, double* smem, RepState* s_st,
                                        int* s_fl) {
+    extern __shared__ float4 ring[];   // kWalkSmem bytes: the warps' row rings
     const int myr = blockIdx.x / P.bpr, lb = blockIdx.x - myr * P.bpr;
     const TileRange TR = tile_range(P.g.ntr, P.g.nt1, P.per_block, lb);
     const long long V = P.g.V, sh = (long long)myr * V;
@@ -255,7 +338,7 @@ __device__ __forceinline__ bool w_body(const UCGP& P, GridSync& gs, int& k, doub
         {   // p = r + beta p_old, t = g5Dw p, <p, A p> = |t|^2
             float f = 0.f;
             const RepState st = s_st[myr];
-            if (st.act) f = walk_phase_a<TYv>(P, myr, TR, qn, qo, (float)st.beta, !st.first, m2f);
+            if (st.act) f = walk_phase_a<TYv>(P, myr, TR, qn, qo, (float)st.beta, !st.first, m2f, ring);
             if (!ureduce<RS>(gs, (double)f, P, smem, s_st, s_fl, RED_PAP, k)) return false;
         }
         {   // x += alpha p, r -= alpha g5Dw t
@@ -263,8 +346,8 @@ __device__ __forceinline__ bool w_body(const UCGP& P, GridSync& gs, int& k, doub
             const RepState st = s_st[myr];
             if (st.act) {
                 const float alpha = (float)st.alpha;
-                f = pend ? walk_phase_b<TYv, true>(P, myr, TR, qn, qo, alpha, apend, m2f)
-                         : walk_phase_b<TYv, false>(P, myr, TR, qn, qo, alpha, apend, m2f);
+                f = pend ? walk_phase_b<TYv, true>(P, myr, TR, qn, qo, alpha, apend, m2f, ring)
+                         : walk_phase_b<TYv, false>(P, myr, TR, qn, qo, alpha, apend, m2f, ring);
                 apend = alpha;
                 pend = !pend;
             }
