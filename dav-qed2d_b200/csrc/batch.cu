@@ -767,33 +767,25 @@ __global__ void k_r_finish(const RepState* __restrict__ st, int nrep, int maxite
 #include "batch_cg_cluster.cuh"
 
 namespace qed2d {
-// Geometries of k_u_cg_mixed: tile height (rows of 32 sites) and site mapping
-// (false: one site per thread per tile; true: warps walking whole tiles).  The
-// first is the default when the tuner is off.
-struct UShape {
-    int rows;
-    bool walk;
-};
-constexpr UShape kUShapes[6] = {{8, false}, {16, false}, {4, false}, {8, true}, {4, true}, {16, true}};
+// tile heights of k_u_cg_mixed (rows of 32 sites per tile = warps per block);
+// the first is the default when the tuner is off
+constexpr int kUTileRows[3] = {8, 16, 4};
 
 template <int RS>
-static const void* uniform_kernel_rs(int rows, bool walk) {
-    if (walk) return rows == 4    ? (const void*)k_u_cg_mixed<RS, 4, true>
-                     : rows == 16 ? (const void*)k_u_cg_mixed<RS, 16, true>
-                                  : (const void*)k_u_cg_mixed<RS, 8, true>;
+static const void* uniform_kernel_rs(int rows) {
     return rows == 4    ? (const void*)k_u_cg_mixed<RS, 4>
            : rows == 16 ? (const void*)k_u_cg_mixed<RS, 16>
                         : (const void*)k_u_cg_mixed<RS, 8>;
 }
 
 // the equal-size solver for schedule 0/1 (grid reductions), 4 (a barrier per
-// replica) or 5 (the same, lean reduction) and a geometry
-static const void* uniform_kernel(int sched, int rows, bool walk) {
+// replica) or 5 (the same, lean reduction) and a tile height
+static const void* uniform_kernel(int sched, int rows) {
     switch (sched) {
-        case 0: return uniform_kernel_rs<0>(rows, walk);
-        case 1: return uniform_kernel_rs<1>(rows, walk);
-        case 4: return uniform_kernel_rs<2>(rows, walk);
-        default: return uniform_kernel_rs<3>(rows, walk);
+        case 0: return uniform_kernel_rs<0>(rows);
+        case 1: return uniform_kernel_rs<1>(rows);
+        case 4: return uniform_kernel_rs<2>(rows);
+        default: return uniform_kernel_rs<3>(rows);
     }
 }
 }  // namespace qed2d
@@ -830,16 +822,15 @@ struct qed2d_batch {
     int rsched = -1;                // uneven batches: 2 grid solver, 3 one cluster per replica (-1: not tuned)
     int rcs = 8;                    // blocks per cluster of the cluster solver (tuned)
     int* d_order = nullptr;         // [nrep] replicas by decreasing size (cluster solver)
-    // k_u_cg_mixed geometry per tiling (kUShapes): tile height, site mapping,
-    // threads per block, tiles per replica, tiles per block, blocks per replica, grid
+    // k_u_cg_mixed geometry per tile height (kUTileRows): tiles per replica,
+    // tiles per block, blocks per replica, grid
     struct UVar {
-        int rows = 0, per_block = 0, bpr = 0, grid = 0, threads = 0;
-        bool walk = false;
+        int rows = 0, per_block = 0, bpr = 0, grid = 0;
         long long ntr = 0;
-    } uv[6];
+    } uv[3];
     int nuv = 0;                    // heights whose kernels fit (co-resident grid)
-    int utile = -1;                 // index into uv of the tiling in use; -1 untuned
-    bool utile_fixed = false;       // set by qed2d_batch_set_tiling: the tuner keeps it
+    int utile = -1;                 // index into uv of the tile height in use; -1 untuned
+    bool utile_fixed = false;       // set by qed2d_batch_set_tile_rows: the tuner keeps it
     UGeom ug{};
     double* d_upart = nullptr;      // [2][max grid over uv]
     double* d_ured = nullptr;       // [2][nrep]
@@ -1134,9 +1125,8 @@ int r_solve(qed2d_batch* h, const double2* U, const float4* U32, const double2* 
             QCHECK(cudaMemsetAsync(&h->ctl->bar, 0, 2 * sizeof(unsigned long long) + sizeof(int), h->stream));
             if (sched >= 4) QCHECK(cudaMemsetAsync(h->d_ubar, 0, sizeof(unsigned long long) * 16 * h->nrep, h->stream));
             void* uargs[] = {(void*)&q};
-            QCHECK(cudaLaunchCooperativeKernel(uniform_kernel(sched, v.rows, v.walk), dim3((unsigned)v.grid),
-                                               dim3((unsigned)v.threads), uargs, v.walk ? kWalkSmem : 0,
-                                               h->stream));
+            QCHECK(cudaLaunchCooperativeKernel(uniform_kernel(sched, v.rows), dim3((unsigned)v.grid),
+                                               dim3((unsigned)(TX * v.rows)), uargs, 0, h->stream));
             count_launch();
             return QED2D_OK;
         };
@@ -1283,29 +1273,20 @@ int batch_setup(qed2d_batch* h, const int* L1, const int* L2, const double* beta
         // one geometry per tile height: as many blocks per replica as stay
         // co-resident (cooperative launch), tiles dealt in contiguous ranges
         const RepInfo& R0 = h->reps[0];
-        for (const UShape sh : kUShapes) {
-            const int threads = sh.walk ? TX * kWalkWarps : TX * sh.rows;
-            const size_t dsmem = sh.walk ? kWalkSmem : 0;
+        for (int rows : kUTileRows) {
             int per_smu = 1 << 30;
             for (int sched : {0, 1, 4, 5}) {
-                const void* kern = uniform_kernel(sched, sh.rows, sh.walk);
-                if (dsmem) QCHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem));
                 int n = 0;
-                QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, threads, dsmem));
+                QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, uniform_kernel(sched, rows), TX * rows, 0));
                 per_smu = std::min(per_smu, n);
             }
             const long long maxgu = std::min<long long>((long long)per_smu * h->num_sms, kMaxPartBlocks);
             if (per_smu < 1 || maxgu / B < 1) continue;
             qed2d_batch::UVar v;
-            v.rows = sh.rows;
-            v.walk = sh.walk;
-            v.threads = threads;
-            v.ntr = (long long)R0.nt1 * ((R0.L2 + sh.rows - 1) / sh.rows);
+            v.rows = rows;
+            v.ntr = (long long)R0.nt1 * ((R0.L2 + rows - 1) / rows);
             const long long bpr = maxgu / B;
-            // tiles per block: as few as keep the grid co-resident; with the walk
-            // mapping a multiple of the 8 warps (one tile per warp per round)
-            const int unit = sh.walk ? kWalkWarps : 1;
-            v.per_block = unit * (int)((v.ntr + (long long)unit * bpr - 1) / ((long long)unit * bpr));
+            v.per_block = (int)((v.ntr + bpr - 1) / bpr);
             v.bpr = (int)((v.ntr + v.per_block - 1) / v.per_block);
             v.grid = v.bpr * B;
             h->uv[h->nuv++] = v;
@@ -1451,9 +1432,9 @@ int qed2d_batch_get_schedule(const qed2d_batch* h, int* schedule) {
     return QED2D_OK;
 }
 
-int qed2d_batch_set_tiling(qed2d_batch* h, int rows, int walk) {
+int qed2d_batch_set_tile_rows(qed2d_batch* h, int rows) {
     if (!h || !h->uniform) {
-        set_error("qed2d_batch_set_tiling: only equal-size batches of at most 64 replicas have tilings");
+        set_error("qed2d_batch_set_tile_rows: only equal-size batches of at most 64 replicas have tile heights");
         return QED2D_ERR_BAD_ARG;
     }
     if (rows == -1) {
@@ -1462,20 +1443,18 @@ int qed2d_batch_set_tiling(qed2d_batch* h, int rows, int walk) {
         return QED2D_OK;
     }
     for (int t = 0; t < h->nuv; t++)
-        if (h->uv[t].rows == rows && h->uv[t].walk == (walk != 0)) {
+        if (h->uv[t].rows == rows) {
             h->utile = t;
             h->utile_fixed = true;
             return QED2D_OK;
         }
-    set_error("qed2d_batch_set_tiling: rows must be -1 or one of 4, 8, 16 (with co-resident blocks), walk 0 or 1");
+    set_error("qed2d_batch_set_tile_rows: rows must be -1 or one of 4, 8, 16 (with co-resident blocks)");
     return QED2D_ERR_BAD_ARG;
 }
 
-int qed2d_batch_get_tiling(const qed2d_batch* h, int* rows, int* walk) {
-    if (!h || !rows || !walk) return QED2D_ERR_BAD_ARG;
-    const bool set = h->uniform && h->utile >= 0;
-    *rows = set ? h->uv[h->utile].rows : -1;
-    *walk = set ? (int)h->uv[h->utile].walk : -1;
+int qed2d_batch_get_tile_rows(const qed2d_batch* h, int* rows) {
+    if (!h || !rows) return QED2D_ERR_BAD_ARG;
+    *rows = (h->uniform && h->utile >= 0) ? h->uv[h->utile].rows : -1;
     return QED2D_OK;
 }
 

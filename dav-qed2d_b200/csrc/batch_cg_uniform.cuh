@@ -349,22 +349,13 @@ __device__ __forceinline__ bool u_body(const UCGP& P, GridSync& gs, int& k, doub
 }
 #undef FOR_MY_UTILES
 
-}  // namespace qed2d
-
-#include "batch_cg_walk.cuh"
-
-namespace qed2d {
-
-// Tiles of 32 x TYv sites, TYv = 4, 8 or 16.  WALK = false: blocks of 32 * TYv
-// threads (128, 256 or 512), one site per thread per tile (u_body); WALK = true:
-// blocks of 8 warps, each warp walking whole tiles down their rows (w_body,
-// batch_cg_walk.cuh).  The tile height sets how many blocks share a replica's
-// tiles (and its barriers) and how many tiles each block walks; the register
-// budget (64 per thread) is the same for all.  Different heights and mappings
-// group the partial sums differently, so they agree to rounding, not bit for bit.
-template <int RS, int TYv, bool WALK = false>
-__global__ void __launch_bounds__(WALK ? 32 * kWalkWarps : 32 * TYv, WALK ? 3 : 32 / TYv)
-    k_u_cg_mixed(const UCGP P) {
+// Tiles of 32 x TYv sites, TYv = 4, 8 or 16 (blocks of 128, 256 or 512 threads):
+// the tile height sets how many blocks share a replica's tiles (and its
+// barriers) and how many tiles each block walks; the register budget (64 per
+// thread) is the same for all three.  Different heights group the partial sums
+// differently, so they agree to rounding, not bit for bit.
+template <int RS, int TYv>
+__global__ void __launch_bounds__(32 * TYv, 32 / TYv) k_u_cg_mixed(const UCGP P) {
     __shared__ double smem[32];
     __shared__ RepState s_st[kUniformReps];
     __shared__ int s_fl[FL_N];
@@ -374,9 +365,7 @@ __global__ void __launch_bounds__(WALK ? 32 * kWalkWarps : 32 * TYv, WALK ? 3 : 
     if constexpr (RS >= 2) {   // independent replicas: a barrier per replica; its blocks leave when it is done
         const int myr = blockIdx.x / P.bpr;
         GridSync gs{P.rbar + 16 * myr, &P.ctl->gen, &P.ctl->err, (unsigned)P.bpr};
-        bool ok;
-        if constexpr (WALK) ok = w_body<RS, TYv>(P, gs, k, smem, s_st, s_fl);
-        else ok = u_body<RS, TYv>(P, gs, k, smem, s_st, s_fl);
+        const bool ok = u_body<RS, TYv>(P, gs, k, smem, s_st, s_fl);
         if (blockIdx.x == myr * P.bpr && threadIdx.x == 0) {   // the replica's first block
             if (ok) P.st_out[myr] = s_st[myr];
             DevCtl* c = P.ctl;
@@ -386,9 +375,7 @@ __global__ void __launch_bounds__(WALK ? 32 * kWalkWarps : 32 * TYv, WALK ? 3 : 
         return;
     }
     GridSync gs{&P.ctl->bar, &P.ctl->gen, &P.ctl->err};
-    bool ok;
-    if constexpr (WALK) ok = w_body<RS, TYv>(P, gs, k, smem, s_st, s_fl);
-    else ok = u_body<RS, TYv>(P, gs, k, smem, s_st, s_fl);
+    const bool ok = u_body<RS, TYv>(P, gs, k, smem, s_st, s_fl);
     if (blockIdx.x == 0) {
         if (ok)   // every block holds the same records: block 0 stores them
             for (int r = threadIdx.x; r < P.g.B; r += blockDim.x) P.st_out[r] = s_st[r];

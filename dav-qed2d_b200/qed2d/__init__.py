@@ -760,24 +760,16 @@ class Batch:
         check(lib().qed2d_batch_set_schedule(self.h, int(s)), "batch_set_schedule")
 
     @property
-    def tiling(self):
-        """(rows, walk) of the equal-size solver: tiles of 32 x rows sites (4, 8
-        or 16), walk = False for one site per thread per tile, True for warps
-        walking whole tiles down their rows; tuned with the schedule on the first
-        solve ((-1, -1) until then).  Set a pair to fix it, or -1 to tune again."""
-        r, w = C.c_int(0), C.c_int(0)
-        check(lib().qed2d_batch_get_tiling(self.h, C.byref(r), C.byref(w)), "batch_get_tiling")
-        return (r.value, w.value if w.value < 0 else bool(w.value))
-
-    @tiling.setter
-    def tiling(self, value) -> None:
-        rows, walk = (value, False) if isinstance(value, int) else value
-        check(lib().qed2d_batch_set_tiling(self.h, int(rows), int(bool(walk))), "batch_set_tiling")
-
-    @property
     def tile_rows(self) -> int:
-        """Tile height of the tiling in use (-1 until tuned)."""
-        return self.tiling[0]
+        """Tile height of the equal-size solver (tiles of 32 x rows sites): 4, 8
+        or 16, tuned with the schedule on the first solve (-1 until then)."""
+        v = C.c_int(0)
+        check(lib().qed2d_batch_get_tile_rows(self.h, C.byref(v)), "batch_get_tile_rows")
+        return v.value
+
+    @tile_rows.setter
+    def tile_rows(self, rows: int) -> None:
+        check(lib().qed2d_batch_set_tile_rows(self.h, int(rows)), "batch_set_tile_rows")
 
     def field(self, dtype=torch.complex128):
         if self.uniform:

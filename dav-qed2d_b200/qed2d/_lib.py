@@ -102,8 +102,8 @@ SIGNATURES = {
     "qed2d_batch_layout": (I, [P, C.POINTER(C.c_int64)]),
     "qed2d_batch_set_schedule": (I, [P, I]),
     "qed2d_batch_get_schedule": (I, [P, PI]),
-    "qed2d_batch_set_tiling": (I, [P, I, I]),
-    "qed2d_batch_get_tiling": (I, [P, PI, PI]),
+    "qed2d_batch_set_tile_rows": (I, [P, I]),
+    "qed2d_batch_get_tile_rows": (I, [P, PI]),
     "qed2d_batch_destroy": (I, [P]),
     "qed2d_batch_set_stream": (I, [P, P]),
     "qed2d_batch_cg": (I, [P, P, P, P, PD, I, D, PI, PI]),

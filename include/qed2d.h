@@ -300,18 +300,15 @@ int qed2d_batch_set_stream(qed2d_batch* batch, void* cuda_stream);
  * on the next solve (get: -1 while untuned). */
 int qed2d_batch_set_schedule(qed2d_batch* batch, int schedule);
 int qed2d_batch_get_schedule(const qed2d_batch* batch, int* schedule);
-/* Tiling of the equal-size batched solver: tiles of 32 x rows sites, rows = 4, 8
- * or 16, and the mapping of sites to threads: walk = 0, one site per thread per
- * tile (blocks of 32*rows threads); walk = 1, each warp of a 256-thread block
- * walks whole tiles down their rows, taking the rows above and below from its
- * previous and next steps and the columns left and right from the neighbouring
- * lanes.  It takes the role of the reference's KernelParm launch geometry
- * (src/QED2d.jl:10-13), which the library chooses: the first solve tunes it
- * together with the schedule; set: fix it (rows = -1: tune again); get: -1 while
- * untuned.  Tilings group the sums differently: results agree to rounding, not
- * bit for bit.  Other batches: BAD_ARG. */
-int qed2d_batch_set_tiling(qed2d_batch* batch, int rows, int walk);
-int qed2d_batch_get_tiling(const qed2d_batch* batch, int* rows, int* walk);
+/* Tile height of the equal-size batched solver: tiles of 32 x rows sites, rows =
+ * 4, 8 or 16 (blocks of 128, 256 or 512 threads, so more or fewer blocks share a
+ * replica's tiles and barriers).  It takes the role of the reference's
+ * KernelParm launch geometry (src/QED2d.jl:10-13), which the library chooses:
+ * the first solve tunes it together with the schedule; set: fix it (-1 = tune
+ * again); get: -1 while untuned.  Heights group the sums differently: results
+ * agree to rounding, not bit for bit.  Other batches: BAD_ARG. */
+int qed2d_batch_set_tile_rows(qed2d_batch* batch, int rows);
+int qed2d_batch_get_tile_rows(const qed2d_batch* batch, int* rows);
 /* every replica's CG method 1 (src/QED2dSolver.jl:3-46) in one launch:
  * x_r = ((g5Dw)^2)^-1 b_r with mass am0[r]; iterations[nrep] and updates[nrep]
  * (FP64 reliable updates) may be NULL */

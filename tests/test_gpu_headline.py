@@ -56,7 +56,7 @@ def test_headline_batched_trajectories_vs_oracle(thermalised):
         U_start = [to_host(U[r]) for r in range(NREP)]
         infos = b.hmc_nf2(U, bench.AM0, bench.EPS, bench.NS, bench.MAXITER, bench.TOL, seeds, counter)
         assert b.schedule in (0, 1, 4, 5)
-        note("batched solver schedule, tiling", [b.schedule, list(b.tiling)])
+        note("batched solver schedule, tile rows", [b.schedule, b.tile_rows])
         for r in range(NREP):
             mom0 = Oracle.normal(2 * V, seeds[r], 1, counter).reshape(2, L, L)
             noise = cgauss(L, L, seeds[r], 16, counter)
