@@ -723,6 +723,190 @@ done:
 }
 
 // ---------------------------------------------------------------------------
+// FP32-inner multi-shift CG: the recurrences of k_cg_multishift (same shift
+// scalars, computed in FP64) on FP32 vectors -- r, p, t, every shift's x and p
+// packed as float4 per site, links in FP32 -- for a source normalised to unit
+// norm.  It stops when |r|^2 < eps32 (relative to |b|^2), a residual FP32 can
+// reach, and writes every shift's solution in FP64 planes, scaled back by |b|;
+// the host then refines each shift with the mixed CG (warm start) to the
+// caller's FP64 stop rule, so every shift meets the same bound as with the FP64
+// multi-shift.
+struct MSP32 {
+    Lat g;
+    const float4* U32;
+    const double2* b;
+    float4* r;
+    float4* p0;
+    float4* p1;
+    float4* t;
+    float4* x[kMaxShifts];
+    float4* ps[kMaxShifts];
+    double2* x64[kMaxShifts];
+    double d[kMaxShifts];
+    int n;
+    int base;
+    double m2;
+    double mu2b;
+    double eps32;
+    int maxiter;
+    int per_block;
+    DevCtl* ctl;
+    double* part;
+};
+
+template <int RS>
+__global__ void __launch_bounds__(TILE, 3) k_cg_multishift32(const MSP32 P) {
+    __shared__ double smem[32 * 2];
+    __shared__ double z[kMaxShifts], zp[kMaxShifts], ai[kMaxShifts], bi[kMaxShifts];
+    __shared__ int upd[kMaxShifts], act[kMaxShifts];
+    auto gs = make_sync<RS>(P.ctl);
+    const long long ntiles = num_tiles(P.g), V = P.g.V;
+    const TileRange TR = tile_range(ntiles, (P.g.L1 + TX - 1) / TX, P.per_block, blockIdx.x);
+    const LkF Lf{P.U32};
+    const float m2f = (float)P.m2, mu2f = (float)P.mu2b;
+    const Pair<float> zf{make_float2(0, 0), make_float2(0, 0)};
+    int k = 0;
+    bool conv = false;
+    double rr = 0.0, bb = 0.0, scale = 1.0;
+    if (threadIdx.x < kMaxShifts) {
+        z[threadIdx.x] = 1.0; zp[threadIdx.x] = 1.0; ai[threadIdx.x] = 0.0; bi[threadIdx.x] = 0.0;
+        upd[threadIdx.x] = 0; act[threadIdx.x] = threadIdx.x < P.n;
+    }
+    {   // |b|^2
+        double v[1] = {0.0};
+        FOR_TILES(q) {
+            const Pair<double> bv{__ldg(P.b + q.x), __ldg(P.b + q.x + V)};
+            v[0] += norm2(bv.a) + norm2(bv.b);
+        }
+        if (!reduce_sync<1, RS>(gs, v, P.part, P.ctl->red, smem)) goto done;
+        bb = v[0];
+    }
+    if (bb == 0.0) {   // zero source: zero solutions
+        FOR_TILES(q) for (int i = 0; i < P.n; i++) st_d(P.x64[i], V, q.x, Pair<double>{make_double2(0, 0), make_double2(0, 0)});
+        conv = true;
+        goto done;
+    }
+    {   // r = b / |b|, x_i = 0
+        scale = 1.0 / sqrt(bb);
+        double v[1] = {0.0};
+        FOR_TILES(q) {
+            const Pair<float> r{to_f(scale * __ldg(P.b + q.x)), to_f(scale * __ldg(P.b + q.x + V))};
+            st_f(P.r, q.x, r);
+            v[0] += (double)(norm2(r.a) + norm2(r.b));
+            for (int i = 0; i < P.n; i++) st_f(P.x[i], q.x, zf);
+        }
+        if (!reduce_sync<1, RS>(gs, v, P.part, P.ctl->red, smem)) goto done;
+        rr = v[0];
+    }
+    {
+        const double tol = P.eps32 * rr;
+        double beta = 0.0, alpha_prev = 1.0;
+        for (k = 1; k <= P.maxiter; k++) {
+            float4* pn = (k & 1) ? P.p0 : P.p1;
+            const float4* po = (k & 1) ? P.p1 : P.p0;
+            const SpAxpy<float, SpF> Q{SpF{P.r}, SpF{po}, (float)beta, k > 1};
+            double v[1] = {0.0};
+            FOR_TILES(q) {
+                const Pair<float> c = Q.ld(q.x);
+                const Pair<float> tt = g5dw_at_c<float>(Q, c, Lf, q, m2f);
+                st_f(pn, q.x, c);
+                st_f(P.t, q.x, tt);
+                v[0] += (double)(norm2(tt.a) + norm2(tt.b) + mu2f * (norm2(c.a) + norm2(c.b)));
+                const Pair<float> rc = SpF{P.r}.ld(q.x);
+                for (int i = 0; i < P.n; i++) {
+                    if (i == P.base) continue;
+                    if (upd[i]) {   // x_i += a^i_{k-1} p_i^{k-1}
+                        const Pair<float> pi = SpF{P.ps[i]}.ld(q.x);
+                        Pair<float> xi = SpF{P.x[i]}.ld(q.x);
+                        const float a = (float)ai[i];
+                        xi.a = xi.a + a * pi.a;
+                        xi.b = xi.b + a * pi.b;
+                        st_f(P.x[i], q.x, xi);
+                        if (act[i]) {
+                            const float zi = (float)z[i], bs = (float)bi[i];
+                            Pair<float> pnew;
+                            pnew.a = zi * rc.a + bs * pi.a;
+                            pnew.b = zi * rc.b + bs * pi.b;
+                            st_f(P.ps[i], q.x, pnew);
+                        }
+                    } else if (k == 1) {
+                        st_f(P.ps[i], q.x, rc);
+                    }
+                }
+            }
+            if (!reduce_sync<1, RS>(gs, v, P.part, P.ctl->red, smem)) goto done;
+            const double alpha = rr / v[0];
+            const float af = (float)alpha;
+            v[0] = 0.0;
+            FOR_TILES(q) {
+                const Pair<float> pc = SpF{pn}.ld(q.x);
+                const Pair<float> a = g5dw_at<float>(SpF{P.t}, Lf, q, m2f);
+                Pair<float> xb = SpF{P.x[P.base]}.ld(q.x), r = SpF{P.r}.ld(q.x);
+                xb.a = xb.a + af * pc.a;
+                xb.b = xb.b + af * pc.b;
+                r.a = r.a - af * (a.a + mu2f * pc.a);
+                r.b = r.b - af * (a.b + mu2f * pc.b);
+                st_f(P.x[P.base], q.x, xb);
+                st_f(P.r, q.x, r);
+                v[0] += (double)(norm2(r.a) + norm2(r.b));
+            }
+            if (!reduce_sync<1, RS>(gs, v, P.part, P.ctl->red, smem)) goto done;
+            const double rn = v[0];
+            const double beta_new = rn / rr;
+            if (threadIdx.x < P.n && threadIdx.x != P.base) {
+                const int i = threadIdx.x;
+                if (act[i]) {
+                    const double zk = z[i], zkm = zp[i];
+                    const double znew = zk * zkm * alpha_prev /
+                                        (alpha * beta * (zkm - zk) + zkm * alpha_prev * (1.0 + P.d[i] * alpha));
+                    ai[i] = alpha * znew / zk;
+                    bi[i] = beta_new * (znew / zk) * (znew / zk);
+                    zp[i] = zk;
+                    z[i] = znew;
+                    upd[i] = 1;
+                    if (znew * znew * rn < tol) act[i] = 0;
+                } else {
+                    upd[i] = 0;
+                }
+            }
+            __syncthreads();
+            alpha_prev = alpha;
+            beta = beta_new;
+            rr = rn;
+            if (rn < tol) { conv = true; break; }
+        }
+        if (!conv) k = P.maxiter;
+        if (!gs.sync()) goto done;
+        // the last x_i updates, then every solution to FP64, scaled back by |b|
+        const double inv = 1.0 / scale;
+        FOR_TILES(q) {
+            for (int i = 0; i < P.n; i++) {
+                Pair<float> xi = SpF{P.x[i]}.ld(q.x);
+                if (i != P.base && upd[i]) {
+                    const Pair<float> pi = SpF{P.ps[i]}.ld(q.x);
+                    const float a = (float)ai[i];
+                    xi.a = xi.a + a * pi.a;
+                    xi.b = xi.b + a * pi.b;
+                }
+                st_d(P.x64[i], V, q.x, Pair<double>{make_double2(inv * xi.a.x, inv * xi.a.y),
+                                                     make_double2(inv * xi.b.x, inv * xi.b.y)});
+            }
+        }
+    }
+done:
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        DevCtl* c = P.ctl;
+        const int err = ld_volatile_int(&c->err);
+        c->last_iters = k;
+        c->last_updates = 0;
+        c->last_conv = conv && !err;
+        c->last_relres = rr;
+        c->iters_total += k;
+        if (c->status == 0 && err) c->status = QED2D_ERR_TIMEOUT;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // host side
 static_assert(offsetof(DevCtl, gen) == sizeof(unsigned long long) &&
                   offsetof(DevCtl, err) == 2 * sizeof(unsigned long long),
@@ -1022,9 +1206,66 @@ static int tune_multishift(Ctx& c, const MSP& P) {
     return QED2D_OK;
 }
 
+// Multishift schedule 3: the FP32 shared Krylov space (k_cg_multishift32, grid
+// reductions) to the relative residual sqrt(kMs32Eps), then every shift refined
+// by the mixed CG from that start to the caller's eps.  The refinement of a
+// shift stops on the FP64 true residual of that shift's system, as every solve
+// of the library does.
+constexpr double kMs32Eps = 1e-12;
+
+static int multishift32_solve(Ctx& c, const double2* U, const double2* b, double2* const* x, const double* mu2,
+                              int n, double am0, int maxiter, double eps) {
+    MSP32 P{};
+    P.g = c.g;
+    float4* u32 = c.spinor32("ms32_u");
+    if (!u32) return QED2D_ERR_NO_MEMORY;
+    QTRY(launch_pack_links(c, u32, U));
+    P.U32 = u32;
+    P.b = b;
+    P.r = c.spinor32("ms32_r");
+    P.p0 = c.spinor32("ms32_p0");
+    P.p1 = c.spinor32("ms32_p1");
+    P.t = c.spinor32("ms32_t");
+    int base = 0;
+    for (int i = 1; i < n; i++)
+        if (mu2[i] < mu2[base]) base = i;
+    for (int i = 0; i < n; i++) {
+        P.x[i] = c.spinor32("ms32_x_" + std::to_string(i));
+        P.ps[i] = i == base ? nullptr : c.spinor32("ms32_ps_" + std::to_string(i));
+        P.x64[i] = x[i];
+        P.d[i] = mu2[i] - mu2[base];
+        if (!P.x[i] || (i != base && !P.ps[i])) return QED2D_ERR_NO_MEMORY;
+    }
+    if (!P.r || !P.p0 || !P.p1 || !P.t) return QED2D_ERR_NO_MEMORY;
+    P.n = n;
+    P.base = base;
+    P.m2 = 2.0 + am0;
+    P.mu2b = mu2[base];
+    P.eps32 = std::max(eps, kMs32Eps);
+    P.maxiter = maxiter;
+    P.ctl = c.ctl;
+    P.part = c.part;
+    QTRY(launch_coop(c, k_cg_multishift32<1>, P));
+    for (int i = 0; i < n; i++) {   // refine each shift to the FP64 stop rule
+        SolveArgs a;
+        a.U = U;
+        a.U32 = u32;
+        a.b = b;
+        a.x = x[i];
+        a.am0 = am0;
+        a.mu2 = mu2[i];
+        a.maxiter = maxiter;
+        a.eps = eps;
+        a.guess = true;
+        QTRY(cg_solve(c, a, QED2D_PREC_MIXED));
+    }
+    return QED2D_OK;
+}
+
 int multishift_solve(Ctx& c, const double2* U, const double2* b, double2* const* x, const double* mu2, int n,
                      double am0, int maxiter, double eps) {
     if (n < 1 || n > kMaxShifts) return QED2D_ERR_BAD_ARG;
+    if (c.sched[2] == 3) return multishift32_solve(c, U, b, x, mu2, n, am0, maxiter, eps);
     MSP P{};
     P.g = c.g;
     P.U = U;

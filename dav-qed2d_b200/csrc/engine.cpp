@@ -417,7 +417,9 @@ int qed2d_ctx_set_schedule(qed2d_ctx* ctx, int precision, int schedule) {
     QCTX(ctx);
     const int slot = sched_slot(precision);
     if (slot < 0) return bad_arg("schedule: QED2D_PREC_F64, QED2D_PREC_MIXED or QED2D_MULTISHIFT only");
-    if (schedule < -1 || schedule > 2) return bad_arg("schedule must be -1, 0, 1 or 2");
+    const int top = slot == 2 ? 3 : 2;   // the multishift solver also has its FP32-inner form (3)
+    if (schedule < -1 || schedule > top)
+        return bad_arg(slot == 2 ? "multishift schedule must be -1, 0, 1, 2 or 3" : "schedule must be -1, 0, 1 or 2");
     c.sched[slot] = schedule;
     return QED2D_OK;
 }

@@ -310,3 +310,58 @@ def test_multishift_schedules(L1, L2):
             bound("multishift residual |(A + mu^2) x - b| / |b|", rel(to_host(y), b), 1e-11)  # mu
     finally:
         qed2d.set_schedule(prm, -1, "multishift")
+
+
+@pytest.mark.parametrize("L1,L2", [(64, 64), (128, 96)])
+def test_multishift_fp32_inner_form(L1, L2):
+    """Multishift schedule 3: the shared Krylov space in FP32, then every shift
+    refined by the mixed CG to the FP64 stop rule.  Each shift's solution
+    satisfies its own system to the same bound as the FP64 multi-shift, and the
+    two agree (1e-11 relative; different Krylov paths)."""
+    import qed2d
+    prm = qed2d.LattParm((L1, L2), 4.0)
+    U, src = to_dev(hot_links(L1, L2, 35)), to_dev(cgauss(L1, L2, 36, 2))
+    am0, mus = 0.15, [0.02, 0.1, 0.4, 1.5, 6.0, 20.0]
+    out = {}
+    try:
+        for sched in (1, 3):
+            qed2d.set_schedule(prm, sched, "multishift")
+            xs = [qed2d.cfield(L1, L2) for _ in mus]
+            qed2d.multishift_CG(xs, U, src, am0, mus, 20000, 1e-24, prm)
+            out[sched] = [to_host(x) for x in xs]
+        y, b = qed2d.cfield(L1, L2), to_host(src)
+        for mu, x3, x1 in zip(mus, out[3], out[1]):
+            bound("multishift FP32-inner vs FP64 multishift", rel(x3, x1), 1e-11)
+            qed2d.gamm5Dw_sqr_musq(y, None, U, to_dev(x3), am0, mu, prm)
+            bound("multishift FP32-inner residual |(A + mu^2) x - b| / |b|", rel(to_host(y), b), 1e-11)  # mu
+    finally:
+        qed2d.set_schedule(prm, -1, "multishift")
+
+
+def test_rhmc_trajectory_fp32_inner_multishift_vs_oracle():
+    """One RHMC trajectory (2 flavours, 12^2) with the FP32-inner multishift form,
+    against the oracle replaying the same draws."""
+    import qed2d
+    from oracle.oracle import zolotarev
+    L, beta = 12, 6.05
+    am0 = [0.6, 1.2]
+    prm = qed2d.LattParm((L, L), beta)
+    o = Oracle(L, L, beta)
+    U0 = hot_links(L, L, 6)
+    rp = [qed2d.get_rhmc_params(4, np.sqrt(0.1), np.sqrt(26.0)) for _ in am0]
+    ro = [zolotarev(4, np.sqrt(0.1), np.sqrt(26.0)) for _ in am0]
+    Ud = to_dev(U0)
+    qed2d.set_precision("f64")
+    qed2d.set_schedule(prm, 3, "multishift")
+    try:
+        qed2d.seed(31)
+        info = qed2d.HMC_(Ud, am0, 0.1, 5, [], 10000, 1e-24, prm, None, rp)
+    finally:
+        qed2d.set_schedule(prm, -1, "multishift")
+    mom0 = Oracle.normal(2 * L * L, 31, 1, info.counter).reshape(2, L, L)
+    noise = [cgauss(L, L, 31, 16 + j, info.counter) for j in range(2)]
+    st, Uo, acco, hi, hf, _ = o.hmc_rhmc(U0, am0, 0.1, 5, 10000, 1e-24, ro, mom0, noise,
+                                         Oracle.uniform(31, 3, info.counter))
+    assert st == 0 and info.accepted == acco
+    bound("RHMC FP32-inner multishift dH abs vs oracle", abs(info.dH - (hf - hi)), 1e-9)
+    bound("RHMC FP32-inner multishift links vs oracle", rel(to_host(Ud), Uo), 1e-11)
