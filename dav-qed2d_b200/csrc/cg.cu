@@ -1057,6 +1057,7 @@ static bool cluster_possible(Ctx& c, int slot) {
 // environment the choice is the size rule measured on B200 instead: every
 // block sums (RS = 1) up to 2^20 sites, the last block publishes beyond.
 constexpr int kTuneIters = 24;
+constexpr long long kMs32Sites = 1LL << 22;   // lattices from 2048^2 on: FP32-inner multishift (schedule 3)
 
 bool tuning_enabled() {
     const char* e = std::getenv("QED2D_TUNE");
@@ -1183,6 +1184,10 @@ static bool multishift_cluster_possible(Ctx& c) {
 // per block); the grid wins once a cluster's blocks walk many tiles each, the
 // shift updates growing with them.
 static int tune_multishift(Ctx& c, const MSP& P) {
+    if (c.g.V >= kMs32Sites) {   // the FP32-inner form, measured faster from 2048^2 on
+        c.sched[2] = 3;
+        return QED2D_OK;
+    }
     if (!tuning_enabled()) {
         c.sched[2] = 1;
         return QED2D_OK;
@@ -1210,7 +1215,11 @@ static int tune_multishift(Ctx& c, const MSP& P) {
 // reductions) to the relative residual sqrt(kMs32Eps), then every shift refined
 // by the mixed CG from that start to the caller's eps.  The refinement of a
 // shift stops on the FP64 true residual of that shift's system, as every solve
-// of the library does.
+// of the library does.  Measured on B200, 12 Zolotarev poles, eps = 1e-24 (the
+// FP64 multi-shift first): 128^2 2.32 -> 5.16 ms, 512^2 9.68 -> 11.53 ms,
+// 2048^2 157.7 -> 141.5 ms.  Below 2048^2 the twelve refinement solves cost more
+// than the halved bytes of the shared Krylov space save (the solver is
+// latency-bound there); the untuned choice is this form from kMs32Sites on.
 constexpr double kMs32Eps = 1e-12;
 
 static int multishift32_solve(Ctx& c, const double2* U, const double2* b, double2* const* x, const double* mu2,

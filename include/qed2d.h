@@ -111,10 +111,11 @@ int qed2d_ctx_get_dims(const qed2d_ctx* ctx, int* L1, int* L2);
  * and keeps the fastest (a host synchronisation; QED2D_TUNE=0 in the
  * environment selects a fixed size rule instead).  set: 0, 1 or 2 to fix it
  * (2 falls back to 1 where no cluster fits), -1 to tune again on the next
- * solve; get: -1 while untuned.  The multishift solver has a fourth form, never
- * chosen by the tuner: 3 = the shared Krylov space in FP32 (to a relative
- * residual of 1e-6), then every shift refined by the mixed CG from that start to
- * the FP64 stop rule. */
+ * solve; get: -1 while untuned.  The multishift solver has a fourth form, 3 =
+ * the shared Krylov space in FP32 (to a relative residual of 1e-6), then every
+ * shift refined by the mixed CG from that start to the FP64 stop rule; it is the
+ * first solve's choice on lattices of 2^22 sites and more (measured faster there,
+ * slower below), and is otherwise chosen only when set. */
 #define QED2D_MULTISHIFT 3   /* schedule selector of the multishift solver (FP64) */
 int qed2d_ctx_set_schedule(qed2d_ctx* ctx, int precision, int schedule);
 int qed2d_ctx_get_schedule(const qed2d_ctx* ctx, int precision, int* schedule);
