@@ -899,14 +899,22 @@ int r_pack(qed2d_batch* h, double2* U, const double* mom, double eps, float4* U3
 // into scratch outputs, and keep the fastest; the device control block is saved
 // and restored around it.  Independent replicas (4) are a candidate from two
 // replicas up (with one they are schedule 1).  QED2D_TUNE=0: the size rule
-// measured on B200 instead -- independent replicas from two replicas up
-// (schedule 1 -> 4 per iteration: 2 x 512^2 23.1 -> 20.2 us, 4 x 512^2 39.1 ->
-// 30.8 us, 32 x 64^2 28.8 -> 9.8 us), every block sums for one.
+// measured on B200 instead -- independent replicas with the lean reduction from
+// two replicas up (schedule 1 -> 4 per iteration: 2 x 512^2 23.1 -> 20.2 us,
+// 4 x 512^2 39.1 -> 30.8 us, 32 x 64^2 28.8 -> 9.8 us; 4 -> 5: 16 x 128^2
+// 11.9 -> 11.3 us, 8 x 256^2 16.9 -> 16.6 us, 4 x 512^2 within 4% either way
+// over runs), every block sums for one; tiles of 16 rows for replicas of 2^18
+// sites and more (the tuner's choice at 4 x 512^2), else 8.
 template <class Launch>
 int tune_uniform(qed2d_batch* h, const UCGP& Q, int maxiter, Launch launch) {
     if (!tuning_enabled()) {
-        h->usched = h->nrep >= 2 ? 4 : 1;
-        if (!h->utile_fixed) h->utile = 0;
+        h->usched = h->nrep >= 2 ? 5 : 1;
+        if (!h->utile_fixed) {
+            h->utile = 0;
+            if (h->Vtot / h->nrep >= (1LL << 18))
+                for (int t = 0; t < h->nuv; t++)
+                    if (h->uv[t].rows == 16) h->utile = t;
+        }
         return QED2D_OK;
     }
     DevCtl saved;

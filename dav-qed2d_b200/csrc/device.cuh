@@ -151,6 +151,17 @@ __device__ __forceinline__ unsigned long long atom_acq_rel_add_u64(unsigned long
     asm volatile("atom.acq_rel.gpu.global.add.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
     return old;
 }
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" : : "l"(p), "l"(v) : "memory");
+}
+// after relaxed loads that observed release stores: orders every later access
+// of this thread after them (the acquire half of the release/acquire pattern)
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" : : : "memory"); }
 __device__ __forceinline__ int ld_volatile_int(const int* p) {
     return *reinterpret_cast<const volatile int*>(p);
 }
@@ -165,15 +176,19 @@ struct GridSync {
 
     __device__ __forceinline__ unsigned n() const { return members ? members : gridDim.x; }
 
-    // Poll *c (acquire) until it reaches target, at most `limit` times.  False
-    // when the wait ended on the error flag or timed out.
+    // Poll *c (acquire) until it reaches target, about `limit` times at most
+    // (checked every 8th poll).  False when the wait ended on the error flag or
+    // timed out.  The error flag is read every 8th poll only: each read is an
+    // L2 round trip that would otherwise sit between two polls of the counter.
     __device__ __forceinline__ bool poll(const unsigned long long* c, unsigned long long limit = 1ULL << 26) {
         unsigned long long polls = 0;
         while (ld_acquire_u64(c) < target) {
-            if (ld_volatile_int(err) != 0) return false;
-            if (++polls > limit) {
-                atomicExch(err, 2 /* QED2D_ERR_TIMEOUT */);
-                return false;
+            if ((++polls & 7) == 0) {
+                if (ld_volatile_int(err) != 0) return false;
+                if (polls > limit) {
+                    atomicExch(err, 2 /* QED2D_ERR_TIMEOUT */);
+                    return false;
+                }
             }
             __nanosleep(32);
         }

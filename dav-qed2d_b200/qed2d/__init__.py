@@ -300,7 +300,9 @@ def set_schedule(prm: LattParm, schedule: int, precision="mixed") -> None:
     0 (last block publishes the sums), 1 (every block sums), 2 (one
     thread-block cluster, small lattices), or -1 to tune again on the next
     solve.  0 and 1 give the same bits.  `precision` selects the solver:
-    "f64" or "mixed" (CG), "multishift" (the RHMC shifted solves)."""
+    "f64" or "mixed" (CG), "multishift" (the RHMC shifted solves; its schedule
+    3 is the FP32 shared Krylov space with every shift refined by the mixed CG,
+    the untuned choice from 2^22 sites on)."""
     check(lib().qed2d_ctx_set_schedule(_c(prm), _PRECS[precision], int(schedule)), "set_schedule")
 
 

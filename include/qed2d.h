@@ -121,7 +121,8 @@ int qed2d_ctx_set_schedule(qed2d_ctx* ctx, int precision, int schedule);
 int qed2d_ctx_get_schedule(const qed2d_ctx* ctx, int precision, int* schedule);
 /* Self-test of failure detection (no counterpart in the reference): runs one
  * kernel whose grid-barrier wait can never complete, with the wait bounded to
- * `polls` polls (1..2^26) instead of the solvers' 2^26.  The wait gives up as a
+ * `polls` polls (1..2^26, rounded up to a multiple of 8: the limit is checked
+ * every 8th poll) instead of the solvers' 2^26.  The wait gives up as a
  * solver's barrier does when a block never arrives, and the call returns
  * QED2D_ERR_TIMEOUT; the context stays usable for the next call. */
 int qed2d_selftest_barrier_timeout(qed2d_ctx* ctx, int64_t polls);
