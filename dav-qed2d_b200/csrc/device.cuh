@@ -151,17 +151,6 @@ __device__ __forceinline__ unsigned long long atom_acq_rel_add_u64(unsigned long
     asm volatile("atom.acq_rel.gpu.global.add.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
     return old;
 }
-__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
-    unsigned long long v;
-    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
-    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" : : "l"(p), "l"(v) : "memory");
-}
-// after relaxed loads that observed release stores: orders every later access
-// of this thread after them (the acquire half of the release/acquire pattern)
-__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" : : : "memory"); }
 __device__ __forceinline__ int ld_volatile_int(const int* p) {
     return *reinterpret_cast<const volatile int*>(p);
 }
