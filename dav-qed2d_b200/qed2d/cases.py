@@ -8,7 +8,8 @@ bcg (one batched mixed CG launch over --batch replicas of L x L), ens (one
 batched mixed CG over the 512-replica ensemble of uneven sizes), ms (MultiCG
 with 12 Zolotarev poles on [0.9 lambda_min, 1.1 lambda_max] from 300 power
 iterations, as the RHMC 128^2 configuration; --schedule 3 for the FP32-inner
-form).  Seeded
+form), rhmc (--repeat one-flavour RHMC trajectories of that configuration, ns
+20, eps 0.05, after 10 pure-gauge thermalisation trajectories).  Seeded
 hot-start links and Gaussian sources; prints the per-launch time of the last
 repeat.
 """
@@ -43,7 +44,7 @@ def hot_batch_field(batch, seed):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["g5dw", "cg_mixed", "cg_f64", "force", "updt", "bcg", "ens", "ms"])
+    ap.add_argument("case", choices=["g5dw", "cg_mixed", "cg_f64", "force", "updt", "bcg", "ens", "ms", "rhmc"])
     ap.add_argument("--schedule", type=int, default=-1, help="ms: multishift schedule (-1 tuned)")
     ap.add_argument("--batch", type=int, default=4)
     ap.add_argument("--L", type=int, default=2048)
@@ -70,7 +71,10 @@ def main(argv=None):
         Ub = hot_batch_field(bt, 2024)
         bb = torch.randn(2 * bt.sites, dtype=torch.complex128, device="cuda", generator=g)
         xb = torch.zeros_like(bb)
-    if a.case == "ms":
+    if a.case == "rhmc":
+        for _ in range(10):
+            qed2d.HMC_(U, 0.1, 10, [], prm, None)
+    if a.case in ("ms", "rhmc"):
         lmin, lmax = qed2d.power_method(U, 0.1, prm, None, iter=300)
         rp = qed2d.get_rhmc_params(12, np.sqrt(0.9 * lmin), np.sqrt(1.1 * lmax))
         qed2d.set_schedule(prm, a.schedule, "multishift")
@@ -99,12 +103,14 @@ def main(argv=None):
                 it = qed2d.MultiCG(so, U, si, 0.1, a.maxiter, 1e-24, qed2d.gamm5Dw_sqr_msq, rp, prm)
             except qed2d.Qed2dError:
                 it = "capped"
+        elif a.case == "rhmc":
+            it = qed2d.HMC_(U, [0.1], 0.05, 20, [], 10000, 1e-24, prm, None, [rp])
         elif a.case == "updt":
             mom = torch.randn(2, L, L, dtype=torch.float64, device="cuda", generator=g)
             qed2d.updt_fld_(U, mom, 0.01)
         ev1.record()
         torch.cuda.synchronize()
-    it = qed2d.last_solve(prm) if a.case.startswith("cg") else (it if a.case in ("bcg", "ens", "ms") else None)
+    it = qed2d.last_solve(prm) if a.case.startswith("cg") else (it if a.case in ("bcg", "ens", "ms", "rhmc") else None)
     print(f"{a.case} L={L}: {ev0.elapsed_time(ev1):.3f} ms  solve={it}")
     return 0
 
