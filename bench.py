@@ -292,6 +292,10 @@ def run_configs(qed2d, torch, dev):
     st3()
     out["C3_rhmc_128_12_poles"] = {"value": timed(st3, 10), "unit": "traj/s", "solver": "FP64 multi-shift, one launch for all poles",
                                    "solver_schedule": names.get(qed2d.get_schedule(p3, "multishift"), "untuned"),
+                                   "solver_layout": {0: "32x8 tiles, one thread per site", 1: "32x8 tiles, two threads per site",
+                                                     2: "32x4 tiles, four threads per site",
+                                                     3: "32x4 tiles, two threads per site"}.get(
+                                       qed2d.get_multishift_layout(p3), "untuned"),
                                    "trajectories": 10}
     del U, U2, U3
     # C5

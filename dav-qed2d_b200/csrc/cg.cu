@@ -587,30 +587,54 @@ struct MSP {
 };
 
 // RS: the reduction schedules of reduce_sync (tuned per context as for cg_solve).
-template <int RS>
-__global__ void __launch_bounds__(TILE, 3) k_cg_multishift(const MSP P) {
+// Layout: tiles of 32 x TYv sites, S threads per site.  Group 0 of a block (its
+// first 32 * TYv threads, one per site) runs the stencil phases and the base
+// system; the shift updates of phase A, which read and write only the site's
+// own values, are dealt over the S groups (non-base shift j goes to group
+// (j + 1) % S, so group 0, which also runs the stencil, gets the fewest).  With
+// S = 1 and TYv = 8 this is one thread per site of a 32 x 8 tile.  Layouts that
+// split the lattice into the same blocks give the same bits (the extra groups
+// add zeros to the block sums); otherwise the partial sums group differently.
+template <int RS, int TYv, int S>
+__global__ void __launch_bounds__(32 * TYv * S, TYv * S <= 8 ? 3 : 1) k_cg_multishift(const MSP P) {
+    constexpr int TPB = 32 * TYv;   // threads of one group: one per site of a tile
     __shared__ double smem[32 * 2];
     __shared__ double z[kMaxShifts], zp[kMaxShifts], ai[kMaxShifts], bi[kMaxShifts];
     __shared__ int upd[kMaxShifts], act[kMaxShifts];
     auto gs = make_sync<RS>(P.ctl);
-    const long long ntiles = num_tiles(P.g), V = P.g.V;
-    const TileRange TR = tile_range(ntiles, (P.g.L1 + TX - 1) / TX, P.per_block, blockIdx.x);
+    const int nt1 = (P.g.L1 + TX - 1) / TX;
+    const long long ntiles = (long long)nt1 * ((P.g.L2 + TYv - 1) / TYv), V = P.g.V;
+    const TileRange TR = tile_range(ntiles, nt1, P.per_block, blockIdx.x);
+    const int st = S == 1 ? (int)threadIdx.x : (int)threadIdx.x % TPB;
+    const int grp = S == 1 ? 0 : (int)threadIdx.x / TPB;
+    const int j0 = (grp + S - 1) % S;   // this group's first non-base shift
     const LkD L{P.U, V};
     const double m2 = P.m2, mu2 = P.mu2b;
     int k = 0;
     bool conv = false;
     double rr = 0.0, bb = 0.0;
+#define FOR_MS_TILES(q)                                                                       \
+    for (int tt_ = TR.lo, t1_ = TR.s1, t2_ = TR.s2; tt_ < TR.hi;                              \
+         ++tt_, (++t1_ == TR.nt1 ? (t1_ = 0, ++t2_) : 0))                                       \
+        if (const Site q = site_at_t<TYv>(P.g, t1_, t2_, st); q.ok)
+#define FOR_MY_SHIFTS(i)                                                                      \
+    for (int j_ = j0, i = j0 < P.base ? j0 : j0 + 1; j_ < P.n - 1;                            \
+         j_ += S, i = j_ < P.base ? j_ : j_ + 1)
     if (threadIdx.x < kMaxShifts) {
         z[threadIdx.x] = 1.0; zp[threadIdx.x] = 1.0; ai[threadIdx.x] = 0.0; bi[threadIdx.x] = 0.0;
         upd[threadIdx.x] = 0; act[threadIdx.x] = threadIdx.x < P.n;
     }
     {
         double v[1] = {0.0};
-        FOR_TILES(q) {
-            const Pair<double> bv{__ldg(P.b + q.x), __ldg(P.b + q.x + V)};
-            v[0] += norm2(bv.a) + norm2(bv.b);
-            st_d(P.r, V, q.x, bv);
-            for (int i = 0; i < P.n; i++) st_d(P.x[i], V, q.x, Pair<double>{make_double2(0, 0), make_double2(0, 0)});
+        const Pair<double> zz{make_double2(0, 0), make_double2(0, 0)};
+        FOR_MS_TILES(q) {
+            if (grp == 0) {
+                const Pair<double> bv{__ldg(P.b + q.x), __ldg(P.b + q.x + V)};
+                v[0] += norm2(bv.a) + norm2(bv.b);
+                st_d(P.r, V, q.x, bv);
+                st_d(P.x[P.base], V, q.x, zz);
+            }
+            FOR_MY_SHIFTS(i) st_d(P.x[i], V, q.x, zz);
         }
         if (!reduce_sync<1, RS>(gs, v, P.part, P.ctl->red, smem)) goto done;
         bb = v[0];
@@ -625,15 +649,16 @@ __global__ void __launch_bounds__(TILE, 3) k_cg_multishift(const MSP P) {
             const double2* po = (k & 1) ? P.p1 : P.p0;
             const SpAxpy<double, SpD> Q{SpD{P.r, V}, SpD{po, V}, beta, k > 1};
             double v[1] = {0.0};
-            FOR_TILES(q) {
-                const Pair<double> c = Q.ld(q.x);
-                const Pair<double> tt = g5dw_at_c<double>(Q, c, L, q, m2);
-                st_d(pn, V, q.x, c);
-                st_d(P.t, V, q.x, tt);
-                v[0] += norm2(tt.a) + norm2(tt.b) + mu2 * (norm2(c.a) + norm2(c.b));
+            FOR_MS_TILES(q) {
+                if (grp == 0) {
+                    const Pair<double> c = Q.ld(q.x);
+                    const Pair<double> tt = g5dw_at_c<double>(Q, c, L, q, m2);
+                    st_d(pn, V, q.x, c);
+                    st_d(P.t, V, q.x, tt);
+                    v[0] += norm2(tt.a) + norm2(tt.b) + mu2 * (norm2(c.a) + norm2(c.b));
+                }
                 const Pair<double> rc = SpD{P.r, V}.ld(q.x);
-                for (int i = 0; i < P.n; i++) {
-                    if (i == P.base) continue;
+                FOR_MY_SHIFTS(i) {
                     if (upd[i]) {   // x_i += a^i_{k-1} p_i^{k-1}
                         const Pair<double> pi = SpD{P.ps[i], V}.ld(q.x);
                         Pair<double> xi = SpD{P.x[i], V}.ld(q.x);
@@ -654,18 +679,18 @@ __global__ void __launch_bounds__(TILE, 3) k_cg_multishift(const MSP P) {
             if (!reduce_sync<1, RS>(gs, v, P.part, P.ctl->red, smem)) goto done;
             const double alpha = rr / v[0];
             v[0] = 0.0;
-            FOR_TILES(q) {
-                const Pair<double> pc = SpD{pn, V}.ld(q.x);
-                const Pair<double> a = g5dw_at<double>(SpD{P.t, V}, L, q, m2);
-                Pair<double> xb = SpD{P.x[P.base], V}.ld(q.x), r = SpD{P.r, V}.ld(q.x);
-                xb.a = xb.a + alpha * pc.a;
-                xb.b = xb.b + alpha * pc.b;
-                r.a = r.a - alpha * (a.a + mu2 * pc.a);
-                r.b = r.b - alpha * (a.b + mu2 * pc.b);
-                st_d(P.x[P.base], V, q.x, xb);
-                st_d(P.r, V, q.x, r);
-                v[0] += norm2(r.a) + norm2(r.b);
-            }
+            if (grp == 0) FOR_MS_TILES(q) {
+                    const Pair<double> pc = SpD{pn, V}.ld(q.x);
+                    const Pair<double> a = g5dw_at<double>(SpD{P.t, V}, L, q, m2);
+                    Pair<double> xb = SpD{P.x[P.base], V}.ld(q.x), r = SpD{P.r, V}.ld(q.x);
+                    xb.a = xb.a + alpha * pc.a;
+                    xb.b = xb.b + alpha * pc.b;
+                    r.a = r.a - alpha * (a.a + mu2 * pc.a);
+                    r.b = r.b - alpha * (a.b + mu2 * pc.b);
+                    st_d(P.x[P.base], V, q.x, xb);
+                    st_d(P.r, V, q.x, r);
+                    v[0] += norm2(r.a) + norm2(r.b);
+                }
             if (!reduce_sync<1, RS>(gs, v, P.part, P.ctl->red, smem)) goto done;
             const double rn = v[0];
             const double beta_new = rn / rr;
@@ -695,9 +720,9 @@ __global__ void __launch_bounds__(TILE, 3) k_cg_multishift(const MSP P) {
         if (!conv) k = P.maxiter;
         // final x_i updates of the last step
         if (!gs.sync()) goto done;
-        FOR_TILES(q) {
-            for (int i = 0; i < P.n; i++) {
-                if (i == P.base || !upd[i]) continue;
+        FOR_MS_TILES(q) {
+            FOR_MY_SHIFTS(i) {
+                if (!upd[i]) continue;
                 const Pair<double> pi = SpD{P.ps[i], V}.ld(q.x);
                 Pair<double> xi = SpD{P.x[i], V}.ld(q.x);
                 xi.a = xi.a + ai[i] * pi.a;
@@ -706,6 +731,8 @@ __global__ void __launch_bounds__(TILE, 3) k_cg_multishift(const MSP P) {
             }
         }
     }
+#undef FOR_MS_TILES
+#undef FOR_MY_SHIFTS
 done:
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         DevCtl* c = P.ctl;
@@ -915,13 +942,13 @@ static_assert(offsetof(DevCtl, gen) == sizeof(unsigned long long) &&
 // Cooperative grid: at most the co-resident limit, then as few blocks as give
 // every block the same number of tiles (fewer arrivals per barrier, no tail).
 template <class K>
-static int coop_grid(Ctx& c, K kernel, int* grid) {
+static int coop_grid(Ctx& c, K kernel, int* grid, int threads = TILE, long long nt = -1) {
+    if (nt < 0) nt = num_tiles(c.g);
     int per_sm = 0;
-    QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, TILE, 0));
+    QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0));
     if (per_sm < 1) return QED2D_ERR_UNSUPPORTED;
     long long g = (long long)per_sm * c.num_sms;
     if (g > kMaxPartBlocks) g = kMaxPartBlocks;
-    const long long nt = num_tiles(c.g);
     const long long per_block = (nt + g - 1) / g;
     g = (nt + per_block - 1) / per_block;
     *grid = (int)g;
@@ -955,14 +982,14 @@ int barrier_timeout_probe(Ctx& c, long long polls) {
 }
 
 template <class K, class Par>
-static int launch_coop(Ctx& c, K kernel, Par P) {
+static int launch_coop(Ctx& c, K kernel, Par P, int threads = TILE, long long nt = -1) {
+    if (nt < 0) nt = num_tiles(c.g);
     int grid = 0;
-    QTRY(coop_grid(c, kernel, &grid));
-    const long long nt = num_tiles(c.g);
+    QTRY(coop_grid(c, kernel, &grid, threads, nt));
     P.per_block = (int)((nt + grid - 1) / grid);
     QTRY(reset_barrier(c));
     void* args[] = {(void*)&P};
-    QCHECK(cudaLaunchCooperativeKernel((const void*)kernel, dim3(grid), dim3(TILE), args, 0, c.stream));
+    QCHECK(cudaLaunchCooperativeKernel((const void*)kernel, dim3(grid), dim3(threads), args, 0, c.stream));
     count_launch();
     return QED2D_OK;
 }
@@ -974,9 +1001,10 @@ static int solve_plain(Ctx& c, const SolveArgs& a);
 // returns QED2D_ERR_UNSUPPORTED when no such cluster fits on the device.
 constexpr int kClusterTiles = 128;
 
+// (threads: block size; nt: the lattice's tiles in the kernel's tile shape)
 template <class K>
-static int cluster_grid(Ctx& c, K kernel, int* grid) {
-    const long long nt = num_tiles(c.g);
+static int cluster_grid(Ctx& c, K kernel, int* grid, int threads = TILE, long long nt = -1) {
+    if (nt < 0) nt = num_tiles(c.g);
     if (nt > kClusterTiles) return QED2D_ERR_UNSUPPORTED;
     int g = (int)std::min<long long>(nt, 16);
     if (g > 8 && cudaFuncSetAttribute((const void*)kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
@@ -987,7 +1015,7 @@ static int cluster_grid(Ctx& c, K kernel, int* grid) {
     for (; g >= 1; g /= 2) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(g);
-        cfg.blockDim = dim3(TILE);
+        cfg.blockDim = dim3(threads);
         cudaLaunchAttribute at[1];
         at[0].id = cudaLaunchAttributeClusterDimension;
         at[0].val.clusterDim.x = g;
@@ -1007,16 +1035,16 @@ static int cluster_grid(Ctx& c, K kernel, int* grid) {
 }
 
 template <class Par>
-static int launch_cluster(Ctx& c, void (*kernel)(Par), Par P) {
+static int launch_cluster(Ctx& c, void (*kernel)(Par), Par P, int threads = TILE, long long nt = -1) {
+    if (nt < 0) nt = num_tiles(c.g);
     int grid = 0;
-    QTRY(cluster_grid(c, kernel, &grid));
-    const long long nt = num_tiles(c.g);
+    QTRY(cluster_grid(c, kernel, &grid, threads, nt));
     P.per_block = (int)((nt + grid - 1) / grid);
     grid = (int)((nt + P.per_block - 1) / P.per_block);   // no block without tiles
     QTRY(reset_barrier(c));   // no barrier here, but the epilogue reads err: clear one a timeout left
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(TILE);
+    cfg.blockDim = dim3(threads);
     cfg.stream = c.stream;
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;
@@ -1167,29 +1195,55 @@ int cg_solve(Ctx& c, const SolveArgs& a, int precision) {
     return launch_cg(c, P, 1, c.sched[1]);
 }
 
-static int launch_multishift(Ctx& c, const MSP& P, int rs) {
-    if (rs == 2) return launch_cluster(c, k_cg_multishift<2>, P);
-    return launch_coop(c, rs ? k_cg_multishift<1> : k_cg_multishift<0>, P);
+// layouts of k_cg_multishift: tile rows and threads per site (shift groups)
+struct MsLayout {
+    int ty, s;
+};
+constexpr MsLayout kMsLayouts[kMsLayoutCount] = {{8, 1}, {8, 2}, {4, 4}, {4, 2}};
+
+template <int RS>
+static void (*ms_kernel(int layout))(MSP) {
+    switch (layout) {
+        case 1: return k_cg_multishift<RS, 8, 2>;
+        case 2: return k_cg_multishift<RS, 4, 4>;
+        case 3: return k_cg_multishift<RS, 4, 2>;
+        default: return k_cg_multishift<RS, 8, 1>;
+    }
 }
 
-static bool multishift_cluster_possible(Ctx& c) {
+static long long ms_tiles(const Ctx& c, int ty) {
+    return (long long)((c.g.L1 + TX - 1) / TX) * ((c.g.L2 + ty - 1) / ty);
+}
+
+static int launch_multishift(Ctx& c, const MSP& P, int rs, int layout) {
+    const MsLayout& l = kMsLayouts[layout];
+    const int threads = TX * l.ty * l.s;
+    const long long nt = ms_tiles(c, l.ty);
+    if (rs == 2) return launch_cluster(c, ms_kernel<2>(layout), P, threads, nt);
+    return launch_coop(c, rs ? ms_kernel<1>(layout) : ms_kernel<0>(layout), P, threads, nt);
+}
+
+static bool multishift_cluster_possible(Ctx& c, int layout) {
     int g = 0;
-    return cluster_grid(c, k_cg_multishift<2>, &g) == QED2D_OK;
+    const MsLayout& l = kMsLayouts[layout];
+    return cluster_grid(c, ms_kernel<2>(layout), &g, TX * l.ty * l.s, ms_tiles(c, l.ty)) == QED2D_OK;
 }
 
-// As tune_cg: the first multishift solve of a context times the schedules on the
-// caller's operator and source, capped at kTuneIters iterations, into scratch
-// solutions (one per shift), and keeps the fastest.  The single cluster wins on
-// the smallest lattices (one barrier round trip less than the grid, a few tiles
-// per block); the grid wins once a cluster's blocks walk many tiles each, the
-// shift updates growing with them.
+// As tune_cg: the first multishift solve of a context times the schedules and
+// layouts on the caller's operator and source, capped at kTuneIters
+// iterations, into scratch solutions (one per shift), and keeps the fastest.
+// The single cluster wins on the smallest lattices (one barrier round trip less
+// than the grid, a few tiles per block); the grid wins once a cluster's blocks
+// walk many tiles each, the shift updates growing with them.  A layout fixed by
+// the caller is kept.
 static int tune_multishift(Ctx& c, const MSP& P) {
     if (c.g.V >= kMs32Sites) {   // the FP32-inner form, measured faster from 2048^2 on
         c.sched[2] = 3;
         return QED2D_OK;
     }
-    if (!tuning_enabled()) {
+    if (!tuning_enabled()) {   // measured: 32 x 4 tiles with four threads per site up to 128^2
         c.sched[2] = 1;
+        if (c.ms_layout < 0) c.ms_layout = c.g.V <= (1LL << 14) ? 2 : 0;
         return QED2D_OK;
     }
     DevCtl saved;
@@ -1201,13 +1255,38 @@ static int tune_multishift(Ctx& c, const MSP& P) {
         if (!T.x[i]) return QED2D_ERR_NO_MEMORY;
     }
     T.maxiter = std::min(P.maxiter, kTuneIters);
-    const int ncand = multishift_cluster_possible(c) ? 3 : 2;
-    int best = 1;
-    const int st = time_schedules(c, [&](int rs) -> int { return launch_multishift(c, T, rs); }, ncand, &best);
+    std::vector<std::pair<int, int>> cand;   // (schedule, layout)
+    const int l_lo = c.ms_layout >= 0 ? c.ms_layout : 0, l_hi = c.ms_layout >= 0 ? c.ms_layout + 1 : kMsLayoutCount;
+    for (int l = l_lo; l < l_hi; l++) {
+        cand.push_back({0, l});
+        cand.push_back({1, l});
+        if (multishift_cluster_possible(c, l)) cand.push_back({2, l});
+    }
+    cudaEvent_t e0, e1;
+    QCHECK(cudaEventCreate(&e0));
+    QCHECK(cudaEventCreate(&e1));
+    std::vector<float> tbest(cand.size(), 1e30f);
+    int st = QED2D_OK;
+    for (int rep = 0; rep < 3 && st == QED2D_OK; rep++)
+        for (size_t i = 0; i < cand.size() && st == QED2D_OK; i++) {
+            cudaEventRecord(e0, c.stream);
+            st = launch_multishift(c, T, cand[i].first, cand[i].second);
+            cudaEventRecord(e1, c.stream);
+            if (cudaEventSynchronize(e1) != cudaSuccess) st = cuda_status(cudaGetLastError(), "schedule tuning");
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep > 0) tbest[i] = std::min(tbest[i], ms);   // the first repetition warms up
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
     QCHECK(cudaMemcpyAsync(c.ctl, &saved, sizeof(DevCtl), cudaMemcpyHostToDevice, c.stream));
     QCHECK(cudaStreamSynchronize(c.stream));
     if (st != QED2D_OK) return st;
-    c.sched[2] = best;
+    size_t best = 0;
+    for (size_t i = 1; i < cand.size(); i++)
+        if (tbest[i] < tbest[best]) best = i;
+    c.sched[2] = cand[best].first;
+    c.ms_layout = cand[best].second;
     return QED2D_OK;
 }
 
@@ -1300,8 +1379,9 @@ int multishift_solve(Ctx& c, const double2* U, const double2* b, double2* const*
     P.ctl = c.ctl;
     P.part = c.part;
     if (c.sched[2] < 0) QTRY(tune_multishift(c, P));
-    if (c.sched[2] == 2 && !multishift_cluster_possible(c)) c.sched[2] = 1;
-    return launch_multishift(c, P, c.sched[2]);
+    const int layout = c.ms_layout < 0 ? 0 : c.ms_layout;
+    if (c.sched[2] == 2 && !multishift_cluster_possible(c, layout)) c.sched[2] = 1;
+    return launch_multishift(c, P, c.sched[2], layout);
 }
 
 // ---------------------------------------------------------------------------

@@ -432,6 +432,20 @@ int qed2d_ctx_get_schedule(const qed2d_ctx* ctx, int precision, int* schedule) {
     return QED2D_OK;
 }
 
+int qed2d_ctx_set_multishift_layout(qed2d_ctx* ctx, int layout) {
+    QCTX(ctx);
+    if (layout < -1 || layout >= kMsLayoutCount) return bad_arg("multishift layout must be -1, 0, 1, 2 or 3");
+    c.ms_layout = layout;
+    if (layout < 0 && c.sched[2] >= 0 && c.sched[2] != 3) c.sched[2] = -1;   // tune both on the next solve
+    return QED2D_OK;
+}
+
+int qed2d_ctx_get_multishift_layout(const qed2d_ctx* ctx, int* layout) {
+    if (!ctx || !layout) return bad_arg("context or layout is NULL");
+    *layout = ctx->c.ms_layout;
+    return QED2D_OK;
+}
+
 int qed2d_selftest_barrier_timeout(qed2d_ctx* ctx, int64_t polls) {
     QCTX(ctx);
     if (polls < 1 || polls > (1LL << 26)) return bad_arg("polls must be in [1, 2^26]");

@@ -36,6 +36,7 @@ struct DevCtl {
 };
 
 constexpr int kMaxPartBlocks = 2048;   // partial-sum slots per reduced quantity
+constexpr int kMsLayoutCount = 4;      // layouts of the multishift kernel (tile rows, threads per site)
 constexpr int kMaxPartVals = 8;        // quantities reduced together
 
 struct Ctx {
@@ -53,6 +54,7 @@ struct Ctx {
     int64_t last_updates = 0;
     double last_relres = 0.0;
     int sched[3] = {-1, -1, -1};   // reduction schedule of the F64 / MIXED / multishift solvers (-1: not tuned yet)
+    int ms_layout = -1;            // layout of the multishift kernel (kMsLayouts; -1: tuned with the schedule)
 
     void* buf(const std::string& name, size_t bytes);   // grow-only named workspace
     double2* spinor(const std::string& name) { return (double2*)buf(name, sizeof(double2) * 2 * g.V); }

@@ -42,8 +42,22 @@ __host__ __device__ __forceinline__ long long num_tiles(const Lat& g) {
     return (long long)((g.L1 + TX - 1) / TX) * ((g.L2 + TY - 1) / TY);
 }
 
-// site of thread t in tile (t1, t2) -- no division; the persistent solvers walk
-// a block's contiguous tile range and advance (t1, t2) incrementally
+// site of thread t in tile (t1, t2) of 32 x TYv sites -- no division; the
+// persistent solvers walk a block's contiguous tile range and advance (t1, t2)
+// incrementally
+template <int TYv>
+__device__ __forceinline__ Site site_at_t(const Lat& g, int t1, int t2, int t) {
+    Site s;
+    s.i1 = t1 * TX + (t & (TX - 1));
+    s.i2 = t2 * TYv + (t >> 5);
+    s.ok = s.i1 < g.L1 && s.i2 < g.L2;
+    s.x = s.i1 + g.L1 * s.i2;   // 32-bit arithmetic: 2*V < 2^31 is checked at context creation
+    s.xp1 = (s.i1 + 1 == g.L1) ? s.x - (g.L1 - 1) : s.x + 1;
+    s.xm1 = (s.i1 == 0) ? s.x + (g.L1 - 1) : s.x - 1;
+    s.xp2 = (s.i2 + 1 == g.L2) ? (long long)s.i1 : s.x + g.L1;
+    s.xm2 = (s.i2 == 0) ? s.x + (g.V - g.L1) : s.x - g.L1;
+    return s;
+}
 __device__ __forceinline__ Site site_at(const Lat& g, int t1, int t2, int t) {
     Site s;
     s.i1 = t1 * TX + (t & (TX - 1));

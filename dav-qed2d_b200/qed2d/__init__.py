@@ -39,7 +39,7 @@ __all__ = [
     "gamm5Dw_sqr_sqr", "gamm5", "Dw", "CG", "save_gauge", "load_gauge", "get_rhmc_params", "power_method",
     "reweighting_factor", "R", "MultiCG", "generate_pseudofermion_", "plwv", "LuscherZ", "LuscherZp",
     "k", "v", "a_r", "c_r", "mu", "nu", "rho_mu", "rho_nu", "P", "d", "A", "delta", "error",
-    "seed", "set_precision", "set_schedule", "get_schedule", "Qed2dError", "cfield", "rfield", "context",
+    "seed", "set_precision", "set_schedule", "get_schedule", "set_multishift_layout", "get_multishift_layout", "Qed2dError", "cfield", "rfield", "context",
 ]
 
 
@@ -304,6 +304,22 @@ def set_schedule(prm: LattParm, schedule: int, precision="mixed") -> None:
     3 is the FP32 shared Krylov space with every shift refined by the mixed CG,
     the untuned choice from 2^22 sites on)."""
     check(lib().qed2d_ctx_set_schedule(_c(prm), _PRECS[precision], int(schedule)), "set_schedule")
+
+
+def set_multishift_layout(prm: LattParm, layout: int) -> None:
+    """Fix the layout of the FP64 multishift kernel on this lattice's context:
+    0 (32 x 8 tiles, one thread per site), 1 (32 x 8 tiles, two threads per
+    site), 2 (32 x 4 tiles, four threads per site), 3 (32 x 4 tiles, two
+    threads per site), or -1 to tune it with the schedule on the next solve.
+    Layouts that split the lattice into the same blocks give the same bits."""
+    check(lib().qed2d_ctx_set_multishift_layout(_c(prm), int(layout)), "set_multishift_layout")
+
+
+def get_multishift_layout(prm: LattParm) -> int:
+    """The multishift kernel's layout on this lattice (-1 until tuned)."""
+    v = C.c_int(0)
+    check(lib().qed2d_ctx_get_multishift_layout(_c(prm), C.byref(v)), "get_multishift_layout")
+    return v.value
 
 
 def get_schedule(prm: LattParm, precision="mixed") -> int:

@@ -49,6 +49,8 @@ SIGNATURES = {
     "qed2d_ctx_get_dims": (I, [P, PI, PI]),
     "qed2d_ctx_set_schedule": (I, [P, I, I]),
     "qed2d_ctx_get_schedule": (I, [P, I, PI]),
+    "qed2d_ctx_set_multishift_layout": (I, [P, I]),
+    "qed2d_ctx_get_multishift_layout": (I, [P, PI]),
     "qed2d_last_solve": (I, [P, PI64, PD, PI64]),
     "qed2d_selftest_barrier_timeout": (I, [P, I64]),
     "qed2d_status_string": (C.c_char_p, [I]),

@@ -119,6 +119,21 @@ int qed2d_ctx_get_dims(const qed2d_ctx* ctx, int* L1, int* L2);
 #define QED2D_MULTISHIFT 3   /* schedule selector of the multishift solver (FP64) */
 int qed2d_ctx_set_schedule(qed2d_ctx* ctx, int precision, int schedule);
 int qed2d_ctx_get_schedule(const qed2d_ctx* ctx, int precision, int* schedule);
+/* Layout of the FP64 multishift kernel (schedules 0-2; no reference
+ * counterpart: it takes the role of KernelParm's launch geometry for the RHMC
+ * solves).  0 = tiles of 32 x 8 sites, one thread per site; 1 = 32 x 8 tiles,
+ * two threads per site; 2 = 32 x 4 tiles, four threads per site; 3 = 32 x 4
+ * tiles, two threads per site.  The extra threads of a site take a share of the
+ * shift updates (each shift's x and p), the first runs the stencil and the base
+ * system as well, so the lattice spreads over more SMs and warps.  Layouts
+ * that split the lattice into the same blocks (same tile height, as many
+ * blocks as tiles) give the same bits; the others agree to rounding.  -1 =
+ * tune it with the schedule on the next multishift solve (get: -1 while
+ * untuned).  Measured per iteration with 12 poles, grid schedule 1: 64^2 9.50
+ * (layout 0) -> 7.85 us (layout 2); 128^2 9.54 -> 8.30 us (layout 2); 256^2
+ * and 512^2 layout 0 fastest (12.7 and 42.9 us). */
+int qed2d_ctx_set_multishift_layout(qed2d_ctx* ctx, int layout);
+int qed2d_ctx_get_multishift_layout(const qed2d_ctx* ctx, int* layout);
 /* Self-test of failure detection (no counterpart in the reference): runs one
  * kernel whose grid-barrier wait can never complete, with the wait bounded to
  * `polls` polls (1..2^26, rounded up to a multiple of 8: the limit is checked

@@ -99,6 +99,41 @@ def test_multishift_vs_sequential_oracle(q):
         bound("multishift vs sequential oracle CG", rel(to_host(x), xo), 5e-12)  # mu
 
 
+@pytest.mark.parametrize("L1,L2", [(64, 64), (128, 128), (100, 37), (256, 96)])
+def test_multishift_layouts_vs_sequential_oracle(q, L1, L2):
+    """Every layout of the FP64 multishift kernel (tiles of 32 x 8 or 32 x 4
+    sites, one to four threads per site sharing the shift updates) under the
+    grid schedules and, where the lattice fits one cluster, the cluster schedule:
+    each shift against the oracle's sequential CG with that shift, and the grid
+    schedules 0 and 1 bit-identical within a layout."""
+    L = q._lib.lib()
+    q.set_precision("f64")
+    prm = q.LattParm((L1, L2), 4.0)
+    o = Oracle(L1, L2, 4.0)
+    U, b = setup(L1, L2, unitary=True, seed=L1 + L2)
+    am0 = 0.2
+    mus = [0.05, 0.3, 1.1, 2.5, 7.0]
+    ref = [o.cg(U, b, am0, 20000, 1e-24, mu=mu)[1] for mu in mus]
+    try:
+        for layout in range(4):
+            q.set_multishift_layout(prm, layout)
+            got = {}
+            for sched in (0, 1, 2):
+                q.set_schedule(prm, sched, "multishift")
+                xs = [q.cfield(L1, L2) for _ in mus]
+                q.multishift_CG(xs, to_dev(U), to_dev(b), am0, mus, 20000, 1e-24, prm)
+                got[sched] = [to_host(x) for x in xs]
+                for x, xo in zip(got[sched], ref):
+                    bound("multishift layout vs sequential oracle CG", rel(x, xo), 1e-14)  # (layout, sched)
+            for a, c in zip(got[0], got[1]):
+                assert np.array_equal(a, c), layout
+            assert q.get_multishift_layout(prm) == layout
+    finally:
+        q.set_multishift_layout(prm, -1)
+        q.set_schedule(prm, -1, "multishift")
+    assert L.qed2d_ctx_set_multishift_layout(q.context(L1, L2, 4.0), 4) == q._lib.BAD_ARG
+
+
 @pytest.mark.parametrize("prec", ["f64", "plain"])
 def test_multicg_rational_pf(q, prec):
     q.set_precision(prec)
