@@ -586,22 +586,16 @@ struct MSP {
     double* part;
 };
 
-// The group that updates non-base shift j in a layout of S threads per site:
-// (j + 1) % S, so group 0, which also runs the stencil, gets the fewest.  (With
-// four groups, leaving group 0 no shift measured slower: 128^2 8.30 -> 8.50 us
-// per iteration.)
-template <int S>
-__device__ __forceinline__ int ms_owner(int j) {
-    return S == 1 ? 0 : (j + 1) % S;
-}
 
 // RS: the reduction schedules of reduce_sync (tuned per context as for cg_solve).
 // Layout: tiles of 32 x TYv sites, S threads per site.  Group 0 of a block (its
 // first 32 * TYv threads, one per site) runs the stencil phases and the base
 // system; the shift updates of phase A, which read and write only the site's
-// own values, are dealt over the groups by ms_owner, so that the stencil's
-// group gets fewer of them.  With S = 1 and TYv = 8 this is one thread per site
-// of a 32 x 8 tile.  Layouts that
+// own values, are dealt over the groups: non-base shift j goes to group
+// (j + 1) % S, so group 0, which also runs the stencil, gets the fewest (leaving
+// it none measured slower with four groups: 128^2 8.30 -> 8.50 us per
+// iteration).  With S = 1 and TYv = 8 this is one thread per site of a 32 x 8
+// tile.  Layouts that
 // split the lattice into the same blocks give the same bits (the extra groups
 // add zeros to the block sums); otherwise the partial sums group differently.
 template <int RS, int TYv, int S>
@@ -616,6 +610,7 @@ __global__ void __launch_bounds__(32 * TYv * S, TYv * S <= 8 ? 3 : 1) k_cg_multi
     const TileRange TR = tile_range(ntiles, nt1, P.per_block, blockIdx.x);
     const int st = S == 1 ? (int)threadIdx.x : (int)threadIdx.x % TPB;
     const int grp = S == 1 ? 0 : (int)threadIdx.x / TPB;
+    const int j0 = (grp + S - 1) % S;   // this group's first non-base shift
     const LkD L{P.U, V};
     const double m2 = P.m2, mu2 = P.mu2b;
     int k = 0;
@@ -626,8 +621,8 @@ __global__ void __launch_bounds__(32 * TYv * S, TYv * S <= 8 ? 3 : 1) k_cg_multi
          ++tt_, (++t1_ == TR.nt1 ? (t1_ = 0, ++t2_) : 0))                                       \
         if (const Site q = site_at_t<TYv>(P.g, t1_, t2_, st); q.ok)
 #define FOR_MY_SHIFTS(i)                                                                      \
-    for (int j_ = 0, i = P.base == 0 ? 1 : 0; j_ < P.n - 1; ++j_, i = j_ < P.base ? j_ : j_ + 1) \
-        if (ms_owner<S>(j_) == grp)
+    for (int j_ = j0, i = j0 < P.base ? j0 : j0 + 1; j_ < P.n - 1;                            \
+         j_ += S, i = j_ < P.base ? j_ : j_ + 1)
     if (threadIdx.x < kMaxShifts) {
         z[threadIdx.x] = 1.0; zp[threadIdx.x] = 1.0; ai[threadIdx.x] = 0.0; bi[threadIdx.x] = 0.0;
         upd[threadIdx.x] = 0; act[threadIdx.x] = threadIdx.x < P.n;
