@@ -51,6 +51,11 @@ B_MIXED_SETUP = 112.0    # |b|^2, x=0, r32 = b/|b|, x32 = 0
 B_F64_ITER = 384.0       # FP64 fused iteration: phase A 160 B + phase B 224 B
 B_DSLASH_F64 = 96.0      # g5Dw apply, FP64: spinor in 32 + links 32 + out 32
 B_DSLASH_C64 = 48.0      # g5Dw apply on complex64 fields: spinor in 16 + links 16 + out 16
+B_KRNL_FORCE = 64.0      # krnl_force!: links in 32 + frc1, frc2 out 16 + 16
+B_UPDT_FLD = 80.0        # updt_fld!: momenta in 16 + links in and out 32 + 32
+B_TR_DQWDU = 112.0       # tr_dQwdU: links 32 + X 32 + g5Dw X 32 in, force out 16
+B_PLAQ_FIELD = 40.0      # plaquette!: links in 32 + per-site plaquette out 8
+B_OMF4_STEP = 6 * 64.0 + 5 * 80.0   # one pure-gauge OMF4 step: 6 kicks (links 32 + momenta r/w 32), 5 link updates
 # Roofline units of the headline kernel.  Algorithmic bytes per site of one CG
 # iteration on (g5Dw)^2: 256 B in FP32 (two applies at 48 B + ten vector passes
 # at 16 B), 512 B in FP64 -- an FP64 reliable update is counted as one FP64
@@ -542,6 +547,32 @@ def run_ours(args):
         c64_gbs = B_DSLASH_C64 * Vb / t_ap32 / 1e9
         apply_err = float(((so64.to(torch.complex128) - so).abs().max() / so.abs().max()).item())
         del U64, si64, so64
+
+        def kernel_gbs(fn, nbytes):
+            for _ in range(3):
+                fn()
+            a0.record()
+            for _ in range(n_ap):
+                fn()
+            a1.record()
+            torch.cuda.synchronize()
+            t = a0.elapsed_time(a1) / 1e3 / n_ap
+            return {"GBs": nbytes * Vb / t / 1e9, "frac": nbytes * Vb / t / 1e9 / peak, "us": t * 1e6}
+        # the gauge-field kernels of the reference's interface, each on its own
+        frc1 = torch.empty(2, Lbig, Lbig, dtype=torch.float64, device=dev)
+        frc2 = torch.empty_like(frc1)
+        mom = torch.randn(2, Lbig, Lbig, dtype=torch.float64, device=dev) * 1e-12   # keeps U near its start
+        plx = torch.empty(Lbig, Lbig, dtype=torch.float64, device=dev)
+        gauge_kernels = {
+            "krnl_force": kernel_gbs(lambda: qed2d.krnl_force_(frc1, frc2, Ub, pb), B_KRNL_FORCE),
+            "updt_fld": kernel_gbs(lambda: qed2d.updt_fld_(Ub, mom, 1.0), B_UPDT_FLD),
+            "tr_dQwdU": kernel_gbs(lambda: qed2d.tr_dQwdU(frc1, Ub, si, so, pb), B_TR_DQWDU),
+            "plaquette_field": kernel_gbs(lambda: qed2d.plaquette_(plx, Ub, pb), B_PLAQ_FIELD),
+            "omf4_step_pure_gauge": kernel_gbs(lambda: qed2d.OMF4_(mom, Ub, 1e-3, 1, pb, None), B_OMF4_STEP),
+            "bytes_per_site": {"krnl_force": B_KRNL_FORCE, "updt_fld": B_UPDT_FLD, "tr_dQwdU": B_TR_DQWDU,
+                               "plaquette_field": B_PLAQ_FIELD, "omf4_step_pure_gauge": B_OMF4_STEP},
+        }
+        del frc1, frc2, mom, plx
         qed2d.set_precision("mixed")
         xb = torch.zeros_like(si)
         cg_runs = []
@@ -573,7 +604,8 @@ def run_ours(args):
                   "g5dw_c64_us": t_ap32 * 1e6, "g5dw_c64_vs_f64_rel_err": apply_err,
                   "cg_solution_mixed_vs_f64_rel_err": sol_err, "cg_solution_iterations": sol_its,
                   "cg_mixed_GBs": cg_gbs, "cg_mixed_frac": cg_gbs / peak,
-                  "cg_mixed_iters": it_cg, "cg_mixed_updates": upd_cg, "peak_GBs": peak, "peak_kind": peak_kind}
+                  "cg_mixed_iters": it_cg, "cg_mixed_updates": upd_cg, "gauge_kernels": gauge_kernels,
+                  "peak_GBs": peak, "peak_kind": peak_kind}
         del Ub, si, so, xb
         torch.cuda.empty_cache()
 

@@ -167,27 +167,65 @@ __global__ void k_random_normal(double* __restrict__ out, long long n, uint64_t 
 
 // mom += eps * (frc1 + frc2 [+ fermion force]) -- the kick of OMF4!/update_momenta!
 // (src/QED2dHMC.jl:256,478,554) with krnl_force!'s two scattered buffers gathered
-// per link, so no force arrays are stored.
-__global__ void __launch_bounds__(TILE) k_mom_kick(double* __restrict__ mom, const double2* __restrict__ U, Lat g,
+// per link, so no force arrays are stored.  The total gauge force on the links
+// of site x is F1 = -v(x) + v(x - 2), F2 = v(x) - v(x - 1) with v = beta Im P
+// (gauge_force_at).  Each thread computes the plaquette of its own site once
+// into shared memory, the first row of the tile also the row below it and the
+// first column the column left of it (the tile's halo), and reads its
+// neighbours' values from there: 4 link loads per site instead of 10, the same
+// plaquette arithmetic, so the same bits.  FERM: add the fermion force of
+// (X, G = g5Dw X); FRC: add frc.  The kicks without the fermion force fit in 40
+// registers (6 blocks per SM on this streaming kernel), the fermion ones in 64.
+template <bool FERM, bool FRC>
+__global__ void __launch_bounds__(TILE, FERM ? 4 : 6) k_mom_kick(double* __restrict__ mom, const double2* __restrict__ U, Lat g,
                                                    double beta, double eps, const double2* __restrict__ X,
                                                    const double2* __restrict__ G, const double* __restrict__ frc) {
-    const Site q = tile_site(g);
+    __shared__ double sv[TY + 1][TX + 1];   // [1 + row][1 + column]; row 0 / column 0: the halo
+    int t1, t2;
+    if (gridDim.y > 1 || g.L2 <= TY) {
+        t1 = blockIdx.x;
+        t2 = blockIdx.y;
+    } else {
+        const int nt1 = (g.L1 + TX - 1) / TX;
+        t2 = blockIdx.x / nt1;
+        t1 = blockIdx.x - t2 * nt1;
+    }
+    const Site q = site_at(g, t1, t2, threadIdx.x);
+    const int lx = threadIdx.x & (TX - 1), ly = threadIdx.x >> 5;
+    const long long V = g.V;
+    double mo1 = 0.0, mo2 = 0.0;
+    if (q.ok) {
+        mo1 = mom[q.x];   // issued with the link loads
+        mo2 = mom[q.x + V];
+        const double2 u1x = __ldg(U + q.x), u2x = __ldg(U + V + q.x);
+        const double2 u2xp1 = __ldg(U + V + q.xp1), u1xp2 = __ldg(U + q.xp2);
+        sv[ly + 1][lx + 1] = beta * plaquette_of(u1x, u2xp1, u1xp2, u2x).y;
+        if (ly == 0) {   // v(x - 2): links of x - 2, x - 2 + 1 and x
+            const long long xp1m2 = q.xm2 + (q.xp1 - q.x);
+            sv[0][lx + 1] = beta * plaquette_of(__ldg(U + q.xm2), __ldg(U + V + xp1m2), u1x, __ldg(U + V + q.xm2)).y;
+        }
+        if (lx == 0) {   // v(x - 1): links of x - 1, x and x - 1 + 2
+            const long long xm1p2 = q.xp2 + (q.xm1 - q.x);
+            sv[ly + 1][0] = beta * plaquette_of(__ldg(U + q.xm1), u2x, __ldg(U + xm1p2), __ldg(U + V + q.xm1)).y;
+        }
+    }
+    __syncthreads();
     if (!q.ok) return;
-    const double mo1 = mom[q.x], mo2 = mom[q.x + g.V];   // issued with the link loads
-    double F1, F2;
-    gauge_force_at(U, g, q, beta, F1, F2);
-    if (X) {
+    const double v = sv[ly + 1][lx + 1];
+    double F1 = -v + sv[ly][lx + 1];
+    double F2 = v - sv[ly + 1][lx];
+    if constexpr (FERM) {
         double f1, f2;
-        fermion_force_at(U, X, G, g.V, q, f1, f2);
+        fermion_force_at(U, X, G, V, q, f1, f2);
         F1 = F1 + f1;
         F2 = F2 + f2;
     }
-    if (frc) {
+    if constexpr (FRC) {
         F1 = F1 + frc[q.x];
-        F2 = F2 + frc[q.x + g.V];
+        F2 = F2 + frc[q.x + V];
     }
     mom[q.x] = mo1 + eps * F1;
-    mom[q.x + g.V] = mo2 + eps * F2;
+    mom[q.x + V] = mo2 + eps * F2;
 }
 
 // y = a x + b z (complex scalars; z may alias y)
@@ -384,7 +422,11 @@ int launch_random_normal(Ctx& c, double* out, int64_t n, uint64_t seed, uint32_t
 
 int launch_mom_kick(Ctx& c, double* mom, const double2* U, double eps, const double2* X, const double2* G,
                     const double* frc) {
-    k_mom_kick<<<tiles_grid2(c.g), TILE, 0, c.stream>>>(mom, U, c.g, c.beta, eps, X, G, frc);
+    const dim3 grid = tiles_grid2(c.g);
+    if (X && frc) k_mom_kick<true, true><<<grid, TILE, 0, c.stream>>>(mom, U, c.g, c.beta, eps, X, G, frc);
+    else if (X) k_mom_kick<true, false><<<grid, TILE, 0, c.stream>>>(mom, U, c.g, c.beta, eps, X, G, frc);
+    else if (frc) k_mom_kick<false, true><<<grid, TILE, 0, c.stream>>>(mom, U, c.g, c.beta, eps, X, G, frc);
+    else k_mom_kick<false, false><<<grid, TILE, 0, c.stream>>>(mom, U, c.g, c.beta, eps, X, G, frc);
     return post_launch("k_mom_kick");
 }
 

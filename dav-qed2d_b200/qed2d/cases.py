@@ -4,6 +4,8 @@
 
 cases: g5dw (FP64 gamm5Dw apply), cg_mixed / cg_f64 (one persistent CG launch
 capped at --maxiter iterations), force (gamm5Dw + tr_dQwdU), updt (link update),
+gauge (krnl_force!, updt_fld!, tr_dQwdU, plaquette! and one pure-gauge OMF4
+step),
 bcg (one batched mixed CG launch over --batch replicas of L x L), ens (one
 batched mixed CG over the 512-replica ensemble of uneven sizes), ms (MultiCG
 with 12 Zolotarev poles on [0.9 lambda_min, 1.1 lambda_max] from 300 power
@@ -44,7 +46,7 @@ def hot_batch_field(batch, seed):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["g5dw", "cg_mixed", "cg_f64", "force", "updt", "bcg", "ens", "ms", "rhmc"])
+    ap.add_argument("case", choices=["g5dw", "cg_mixed", "cg_f64", "force", "updt", "bcg", "ens", "ms", "rhmc", "gauge"])
     ap.add_argument("--schedule", type=int, default=-1, help="ms: multishift schedule (-1 tuned)")
     ap.add_argument("--batch", type=int, default=4)
     ap.add_argument("--L", type=int, default=2048)
@@ -105,6 +107,16 @@ def main(argv=None):
                 it = "capped"
         elif a.case == "rhmc":
             it = qed2d.HMC_(U, [0.1], 0.05, 20, [], 10000, 1e-24, prm, None, [rp])
+        elif a.case == "gauge":
+            f1 = torch.empty(2, L, L, dtype=torch.float64, device="cuda")
+            f2 = torch.empty_like(f1)
+            mom = torch.randn(2, L, L, dtype=torch.float64, device="cuda", generator=g) * 1e-12
+            plx = torch.empty(L, L, dtype=torch.float64, device="cuda")
+            qed2d.krnl_force_(f1, f2, U, prm)
+            qed2d.updt_fld_(U, mom, 1.0)
+            qed2d.tr_dQwdU(f1, U, si, so, prm)
+            qed2d.plaquette_(plx, U, prm)
+            qed2d.OMF4_(mom, U, 1e-3, 1, prm, None)
         elif a.case == "updt":
             mom = torch.randn(2, L, L, dtype=torch.float64, device="cuda", generator=g)
             qed2d.updt_fld_(U, mom, 0.01)
