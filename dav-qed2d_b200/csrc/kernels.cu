@@ -170,8 +170,9 @@ __global__ void k_random_normal(double* __restrict__ out, long long n, uint64_t 
 // per link, so no force arrays are stored.  The total gauge force on the links
 // of site x is F1 = -v(x) + v(x - 2), F2 = v(x) - v(x - 1) with v = beta Im P
 // (gauge_force_at).  Each thread computes the plaquette of its own site once
-// into shared memory, the first row of the tile also the row below it and the
-// first column the column left of it (the tile's halo), and reads its
+// into shared memory; the last warp also computes the row below the tile and
+// the second-last warp's first TY lanes the column left of it (the tile's halo;
+// two warps with two plaquettes each, the others one); every thread reads its
 // neighbours' values from there: 4 link loads per site instead of 10, the same
 // plaquette arithmetic, so the same bits.  FERM: add the fermion force of
 // (X, G = g5Dw X); FRC: add frc.  The kicks without the fermion force fit in 40
@@ -200,13 +201,20 @@ __global__ void __launch_bounds__(TILE, FERM ? 4 : 6) k_mom_kick(double* __restr
         const double2 u1x = __ldg(U + q.x), u2x = __ldg(U + V + q.x);
         const double2 u2xp1 = __ldg(U + V + q.xp1), u1xp2 = __ldg(U + q.xp2);
         sv[ly + 1][lx + 1] = beta * plaquette_of(u1x, u2xp1, u1xp2, u2x).y;
-        if (ly == 0) {   // v(x - 2): links of x - 2, x - 2 + 1 and x
-            const long long xp1m2 = q.xm2 + (q.xp1 - q.x);
-            sv[0][lx + 1] = beta * plaquette_of(__ldg(U + q.xm2), __ldg(U + V + xp1m2), u1x, __ldg(U + V + q.xm2)).y;
+    }
+    if (ly == TY - 1) {   // v(y - 2) for y in the tile's first row: links of y - 2, y - 2 + 1 and y
+        const Site y = site_at(g, t1, t2, lx);
+        if (y.ok) {
+            const long long xp1m2 = y.xm2 + (y.xp1 - y.x);
+            sv[0][lx + 1] = beta * plaquette_of(__ldg(U + y.xm2), __ldg(U + V + xp1m2), __ldg(U + y.x),
+                                                __ldg(U + V + y.xm2)).y;
         }
-        if (lx == 0) {   // v(x - 1): links of x - 1, x and x - 1 + 2
-            const long long xm1p2 = q.xp2 + (q.xm1 - q.x);
-            sv[ly + 1][0] = beta * plaquette_of(__ldg(U + q.xm1), u2x, __ldg(U + xm1p2), __ldg(U + V + q.xm1)).y;
+    } else if (ly == TY - 2 && lx < TY) {   // v(y - 1) for y in the tile's first column: links of y - 1, y, y - 1 + 2
+        const Site y = site_at(g, t1, t2, TX * lx);
+        if (y.ok) {
+            const long long xm1p2 = y.xp2 + (y.xm1 - y.x);
+            sv[lx + 1][0] = beta * plaquette_of(__ldg(U + y.xm1), __ldg(U + V + y.x), __ldg(U + xm1p2),
+                                                __ldg(U + V + y.xm1)).y;
         }
     }
     __syncthreads();
