@@ -50,6 +50,7 @@ __host__ __device__ __forceinline__ Lat lat_of(const RepInfo& R) { return Lat{R.
 struct TileView {
     const RepInfo* reps;
     const int4* tiles;   // (replica, t1, t2, 0)
+    long long vtot;      // sites of the batch (the stride of the FP32 link planes)
 };
 
 // ---------------------------------------------------------------------------
@@ -110,7 +111,7 @@ __global__ void __launch_bounds__(TILE) k_r_updt(double2* __restrict__ U, const 
         u[q.x] = u1;
         u[q.x + R.V] = u2;
     }
-    U32[R.off + q.x] = make_float4((float)u1.x, (float)u1.y, (float)u2.x, (float)u2.y);
+    st_links32(U32, tv.vtot, R.off + q.x, u1, u2);
 }
 
 // N(0,1) doubles: one thread per pair of doubles of the batch array; the replica
@@ -248,7 +249,8 @@ struct RCGP {
     const int* rep_seg;   // [nrep+1] partial slots of replica r
     const double* m2;     // 2 + m0 per replica
     const double2* U;
-    const float4* U32;
+    const float4* U32;    // FP32 link planes of vtot sites
+    long long vtot;
     const double2* b;
     double2* x;
     double2* r64;
@@ -333,7 +335,7 @@ __device__ __forceinline__ acc_t<PH> tile_work(const RCGP& P, const RepVals& v, 
         const float4* qo = cur ? P.q0 : P.q1;
         const SpAxpy<float, SpF> Q{SpF{P.r32 + o1}, SpF{qo + o1}, (float)v.beta, !v.first};
         const Pair<float> c = Q.ld(q.x);
-        const Pair<float> tt = g5dw_at_c<float>(Q, c, LkF{P.U32 + o1}, q, (float)v.m2);
+        const Pair<float> tt = g5dw_at_c<float>(Q, c, LkF{P.U32, P.vtot, o1}, q, (float)v.m2);
         st_f(qn + o1, q.x, c);
         st_f(P.t32 + o1, q.x, tt);
         return norm2(tt.a) + norm2(tt.b);
@@ -341,7 +343,7 @@ __device__ __forceinline__ acc_t<PH> tile_work(const RCGP& P, const RepVals& v, 
         const float4* qn = cur ? P.q1 : P.q0;
         const float alpha = (float)v.alpha;
         const Pair<float> pc = SpF{qn + o1}.ld(q.x);
-        const Pair<float> a = g5dw_at<float>(SpF{P.t32 + o1}, LkF{P.U32 + o1}, q, (float)v.m2);
+        const Pair<float> a = g5dw_at<float>(SpF{P.t32 + o1}, LkF{P.U32, P.vtot, o1}, q, (float)v.m2);
         Pair<float> xv = SpF{P.x32 + o1}.ld(q.x), rv = SpF{P.r32 + o1}.ld(q.x);
         xv.a = xv.a + alpha * pc.a;
         xv.b = xv.b + alpha * pc.b;
@@ -863,7 +865,7 @@ struct qed2d_batch {
     double2* field(const char* n) { return (double2*)buf(n, sizeof(double2) * 2 * Vtot); }
     double* real2(const char* n) { return (double*)buf(n, sizeof(double) * 2 * Vtot); }
     float4* field32(const char* n) { return (float4*)buf(n, sizeof(float4) * Vtot); }
-    TileView tv() const { return TileView{d_reps, d_tiles}; }
+    TileView tv() const { return TileView{d_reps, d_tiles, Vtot}; }
 };
 
 namespace {
@@ -1081,6 +1083,7 @@ int r_solve(qed2d_batch* h, const double2* U, const float4* U32, const double2* 
     P.m2 = h->d_m2;
     P.U = U;
     P.U32 = U32;
+    P.vtot = h->Vtot;
     P.b = b;
     P.x = x;
     P.t64 = g5x;
@@ -1150,6 +1153,7 @@ int r_solve(qed2d_batch* h, const double2* U, const float4* U32, const double2* 
         C.m2 = h->d_m2;
         C.U = U;
         C.U32 = U32;
+        C.vtot = h->Vtot;
         C.b = b;
         C.x = x;
         C.t64 = g5x;

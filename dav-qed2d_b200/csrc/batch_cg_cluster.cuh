@@ -21,7 +21,8 @@ struct CCGP {
     const int* order;   // cluster c solves replica order[c]
     const double* m2;   // 2 + m0 per replica
     const double2* U;
-    const float4* U32;
+    const float4* U32;   // FP32 link planes of vtot sites
+    long long vtot;
     const double2* b;
     double2* x;
     double2* r64;
@@ -85,7 +86,7 @@ __device__ __forceinline__ void c_body(const CCGP& P, int r, int& k, double* sme
     float4* q0 = P.q0 + o1;
     float4* q1 = P.q1 + o1;
     const LkD L{P.U + o2, V};
-    const LkF Lf{P.U32 + o1};
+    const LkF Lf{P.U32, P.vtot, o1};
     const double m2 = P.m2[r];
     const float m2f = (float)m2;
     const Pair<double> z{make_double2(0, 0), make_double2(0, 0)};

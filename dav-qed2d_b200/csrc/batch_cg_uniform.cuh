@@ -209,7 +209,7 @@ __device__ __forceinline__ bool u_body(const UCGP& P, GridSync& gs, int& k, doub
     double2* r64 = P.r64 + sh;
     double2* t64 = P.t64 + sh;
     const LkD L{P.U + sh, V};
-    const LkF Lf{P.U32};
+    const LkF Lf{P.U32, P.g.V * P.g.B};
     const double m2 = P.m2[myr];
     const float m2f = (float)m2;
     const Pair<double> z{make_double2(0, 0), make_double2(0, 0)};

@@ -347,7 +347,7 @@ __global__ void __launch_bounds__(TILE, 4) k_cg_mixed(const CGP P) {
     const long long ntiles = num_tiles(P.g), V = P.g.V;
     const TileRange TR = tile_range(ntiles, (P.g.L1 + TX - 1) / TX, P.per_block, blockIdx.x);
     const LkD L{P.U, V};
-    const LkF Lf{P.U32};
+    const LkF Lf{P.U32, P.g.V};
     const double m2 = P.m2, mu2 = P.mu2;
     const float m2f = (float)m2, mu2f = (float)mu2;
     double2* t64 = P.g5x ? P.g5x : P.t;
@@ -792,7 +792,7 @@ __global__ void __launch_bounds__(TILE, 3) k_cg_multishift32(const MSP32 P) {
     auto gs = make_sync<RS>(P.ctl);
     const long long ntiles = num_tiles(P.g), V = P.g.V;
     const TileRange TR = tile_range(ntiles, (P.g.L1 + TX - 1) / TX, P.per_block, blockIdx.x);
-    const LkF Lf{P.U32};
+    const LkF Lf{P.U32, P.g.V};
     const float m2f = (float)P.m2, mu2f = (float)P.mu2b;
     const Pair<float> zf{make_float2(0, 0), make_float2(0, 0)};
     int k = 0;

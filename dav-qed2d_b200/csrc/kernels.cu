@@ -115,14 +115,14 @@ __global__ void k_updt_fld(double2* __restrict__ U, const double* __restrict__ m
     const double2 u2 = cmul(make_double2(c2, s2), U[x + V]);
     U[x] = u1;
     U[x + V] = u2;
-    if (U32) U32[x] = make_float4((float)u1.x, (float)u1.y, (float)u2.x, (float)u2.y);
+    if (U32) st_links32(U32, V, x, u1, u2);
 }
 
 __global__ void k_pack_links(float4* __restrict__ U32, const double2* __restrict__ U, long long V) {
     const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (x >= V) return;
     const double2 u1 = U[x], u2 = U[x + V];
-    U32[x] = make_float4((float)u1.x, (float)u1.y, (float)u2.x, (float)u2.y);
+    st_links32(U32, V, x, u1, u2);
 }
 
 // krnl_unfold! / krnl_reflect! -- src/QED2dFields.jl:12-25,37-50

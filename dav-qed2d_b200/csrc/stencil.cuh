@@ -167,17 +167,23 @@ struct LkD {
     __device__ __forceinline__ double2 u1(long long x) const { return __ldg(U + x); }
     __device__ __forceinline__ double2 u2(long long x) const { return __ldg(U + V + x); }
 };
+// packed FP32 links of the mixed solvers: two float2 planes (u1, u2) of
+// `stride` sites each, stored in a float4 array of `stride` elements; a link
+// load reads only the direction it needs (8 bytes, not the site's 16)
 struct LkF {
-    const float4* U;
-    __device__ __forceinline__ float2 u1(long long x) const {
-        const float4 q = __ldg(U + x);
-        return make_float2(q.x, q.y);
-    }
-    __device__ __forceinline__ float2 u2(long long x) const {
-        const float4 q = __ldg(U + x);
-        return make_float2(q.z, q.w);
-    }
+    const float2* U;
+    long long stride;
+    __device__ __forceinline__ LkF(const float4* base, long long stride_, long long off = 0)
+        : U(reinterpret_cast<const float2*>(base) + off), stride(stride_) {}
+    __device__ __forceinline__ float2 u1(long long x) const { return __ldg(U + x); }
+    __device__ __forceinline__ float2 u2(long long x) const { return __ldg(U + stride + x); }
 };
+// store the FP32 links of site x into the planes of `stride` sites
+__device__ __forceinline__ void st_links32(float4* base, long long stride, long long x, double2 u1, double2 u2) {
+    float2* u = reinterpret_cast<float2*>(base);
+    u[x] = make_float2((float)u1.x, (float)u1.y);
+    u[stride + x] = make_float2((float)u2.x, (float)u2.y);
+}
 
 struct LkF2 {   // complex64 link planes
     const float2* U;
