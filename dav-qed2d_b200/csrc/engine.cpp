@@ -236,10 +236,21 @@ static int md_kick_rhmc(Ctx& c, double* mom, const double2* U, double2* X, const
         } else {
             QTRY(multishift_solve(c, U, C2(F[j]), xs.data(), mu2.data(), n, am0[j], maxiter, tol));
         }
-        for (int i = 0; i < n; i++) {
-            QTRY(launch_g5dw(c, g5DX, U, xs[i], am0[j], nullptr, make_double2(0, 0), false));
-            QTRY(launch_force_accum(c, frc, U, xs[i], g5DX, r[j].rho[i], !first));
+        if (c.precision == QED2D_PREC_PLAIN) {   // the reference's sequence: two launches per pole
+            for (int i = 0; i < n; i++) {
+                QTRY(launch_g5dw(c, g5DX, U, xs[i], am0[j], nullptr, make_double2(0, 0), false));
+                QTRY(launch_force_accum(c, frc, U, xs[i], g5DX, r[j].rho[i], !first));
+                first = false;
+            }
+        } else if (n > 0) {   // all poles in two launches
+            std::vector<double2*> gs(n);
+            for (int i = 0; i < n; i++) {
+                gs[i] = c.spinor("mcg_g_" + std::to_string(i));
+                if (!gs[i]) return QED2D_ERR_NO_MEMORY;
+            }
+            QTRY(launch_force_poles(c, frc, U, xs.data(), gs.data(), r[j].rho, n, am0[j], !first));
             first = false;
+            if (j == nf - 1) QTRY(launch_copy(c, g5DX, gs[n - 1], field_bytes(c)));   // g5Dw X of the last pole
         }
         if (j == nf - 1 && n > 0) QTRY(launch_copy(c, X, xs[n - 1], field_bytes(c)));
     }

@@ -113,6 +113,8 @@ int launch_random_normal(Ctx& c, double* out, int64_t n, uint64_t seed, uint32_t
 int launch_mom_kick(Ctx& c, double* mom, const double2* U, double eps, const double2* X, const double2* G,
                     const double* frc);
 // frc (+)= rho * tr_dQwdU(U, X, G)
+int launch_force_poles(Ctx& c, double* frc, const double2* U, const double2* const* X, double2* const* G,
+                       const double* rho, int n, double am0, bool accumulate);
 int launch_force_accum(Ctx& c, double* frc, const double2* U, const double2* X, const double2* G, double rho,
                        bool accumulate);
 // BLAS-1 on complex planes of n = 2V elements (alpha given on host)

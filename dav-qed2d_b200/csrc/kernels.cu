@@ -81,6 +81,47 @@ __global__ void __launch_bounds__(TILE) k_force(double* __restrict__ frc, const 
     }
 }
 
+// The RHMC force of all poles of a flavour in two launches instead of two per
+// pole (src/QED2dHMC.jl:528-545): k_g5dw_poles applies gamm5Dw to every pole's
+// solution (blockIdx.z = pole), k_force_poles sums rho_i tr_dQwdU(X_i, g5Dw X_i)
+// over the poles in pole order, each term as k_force computes it (the same bits
+// as one k_force launch per pole).
+struct Poles {
+    const double2* X[QED2D_MAXPOLES];
+    double2* G[QED2D_MAXPOLES];
+    double rho[QED2D_MAXPOLES];
+    int n;
+};
+__global__ void __launch_bounds__(TILE) k_g5dw_poles(const double2* __restrict__ U, const Poles P, double m2, Lat g) {
+    const Site q = tile_site(g);
+    if (!q.ok) return;
+    const int i = blockIdx.z;
+    st_d(P.G[i], g.V, q.x, g5dw_at<double>(SpDro{P.X[i], g.V}, LkD{U, g.V}, q, m2));
+}
+__global__ void __launch_bounds__(TILE) k_force_poles(double* __restrict__ frc, const double2* __restrict__ U,
+                                                      const Poles P, Lat g, int accumulate) {
+    const Site q = tile_site(g);
+    if (!q.ok) return;
+    double a1 = 0.0, a2 = 0.0;
+    for (int i = 0; i < P.n; i++) {
+        double f1, f2;
+        fermion_force_at(U, P.X[i], P.G[i], g.V, q, f1, f2);
+        if (i == 0 && !accumulate) {
+            a1 = P.rho[0] * f1;
+            a2 = P.rho[0] * f2;
+        } else {
+            if (i == 0) {
+                a1 = frc[q.x];
+                a2 = frc[q.x + g.V];
+            }
+            a1 += P.rho[i] * f1;
+            a2 += P.rho[i] * f2;
+        }
+    }
+    frc[q.x] = a1;
+    frc[q.x + g.V] = a2;
+}
+
 // plaquette! (mode 0, Re P) and qtop! (mode 1, arg P) -- src/QED2dAction.jl:2-32
 __global__ void __launch_bounds__(TILE) k_plaq_field(double* __restrict__ plx, const double2* __restrict__ U, Lat g,
                                                      int mode) {
@@ -376,6 +417,24 @@ int launch_force_accum(Ctx& c, double* frc, const double2* U, const double2* X, 
                        bool accumulate) {
     k_force<<<tiles_grid2(c.g), TILE, 0, c.stream>>>(frc, U, X, G, c.g, rho, accumulate ? 1 : 0);
     return post_launch("k_force");
+}
+
+int launch_force_poles(Ctx& c, double* frc, const double2* U, const double2* const* X, double2* const* G,
+                       const double* rho, int n, double am0, bool accumulate) {
+    if (n < 1 || n > QED2D_MAXPOLES) return QED2D_ERR_BAD_ARG;
+    Poles P{};
+    for (int i = 0; i < n; i++) {
+        P.X[i] = X[i];
+        P.G[i] = G[i];
+        P.rho[i] = rho[i];
+    }
+    P.n = n;
+    dim3 grid = tiles_grid2(c.g);
+    grid.z = (unsigned)n;
+    k_g5dw_poles<<<grid, TILE, 0, c.stream>>>(U, P, 2.0 + am0, c.g);
+    QTRY(post_launch("k_g5dw_poles"));
+    k_force_poles<<<tiles_grid2(c.g), TILE, 0, c.stream>>>(frc, U, P, c.g, accumulate ? 1 : 0);
+    return post_launch("k_force_poles");
 }
 
 int launch_plaq_field(Ctx& c, double* plx, const double2* U, int mode) {
