@@ -64,12 +64,13 @@ B_OMF4_STEP = 6 * 64.0 + 5 * 80.0   # one pure-gauge OMF4 step: 6 kicks (links 3
 B_ITER_F32 = 256.0
 B_ITER_F64 = 512.0
 # Measured traffic per site-iteration of k_u_cg_mixed at 4 x 512^2, from one ncu
-# capture of a 100-iteration launch of the current kernel: DRAM read + write
-# (6.529 GB over 1,048,576 sites x 100) and L1 <-> L2 (18.19 GB read + 6.60 GB
-# written); both grow in proportion to the iterations at fixed size
-U_DRAM_PER_SITE_ITER = 62.3
-U_L2_PER_SITE_ITER = 236.0
-U_L2_THROUGHPUT = 0.377   # lts__throughput.avg.pct_of_peak_sustained_elapsed of the same capture
+# capture of a 100-iteration launch of the tuned kernel (independent replicas,
+# lean reduction, 32 x 16 tiles): DRAM read + write (6.560 GB over 1,048,576
+# sites x 100) and L1 <-> L2 (16.15 GB read + 6.56 GB written); both grow in
+# proportion to the iterations at fixed size
+U_DRAM_PER_SITE_ITER = 62.6
+U_L2_PER_SITE_ITER = 217.0
+U_L2_THROUGHPUT = 0.352   # lts__throughput.avg.pct_of_peak_sustained_elapsed of the same capture
 ENS_NS, ENS_EPS = 10, 0.1   # replica ensemble: leapfrog ns=10, eps=0.1
 CPU_TRAJ = 2                # trajectories of the GPU arm's CPU-baseline sample
 
