@@ -485,7 +485,9 @@ def run_ours(args):
                 "launch_us": t_k * 1e6,
                 "schedule": {0: "last block publishes the sums", 1: "every block sums",
                              4: "independent replicas (a barrier per replica)",
-                             5: "independent replicas, lean reduction"}.get(batch.schedule, "untuned"),
+                             5: "independent replicas, lean reduction",
+                             7: "independent replicas, lean reduction, TMA-staged stencil operands"}.get(
+                                 batch.schedule, "untuned"),
                 "tile_rows": batch.tile_rows,
                 "note": f"one launch = one solve of all {B} replicas: per replica iterations {min(its)}-{max(its)} "
                         f"x {B_ITER_F32:.0f} B/site + reliable updates {min(upd)}-{max(upd)} x {B_ITER_F64:.0f} "

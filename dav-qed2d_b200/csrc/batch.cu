@@ -780,6 +780,52 @@ static const void* uniform_kernel_rs(int rows) {
                         : (const void*)k_u_cg_mixed<RS, 8>;
 }
 
+// host: cuTensorMapEncodeTiled through the runtime's driver entry point
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+int encode_map_2d(CUtensorMap* map, const void* base, unsigned long long nx, unsigned long long ny,
+                  unsigned long long pitch, unsigned bx, unsigned by) {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !p) {
+            cudaGetLastError();
+            set_error("cuTensorMapEncodeTiled is not available from the driver");
+            return QED2D_ERR_UNSUPPORTED;
+        }
+        fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    if (reinterpret_cast<uintptr_t>(base) % 16 || pitch % 16 || (4ull * bx) % 16 || bx > 256 || by > 256 || bx > nx ||
+        by > ny) {
+        set_error("tensor map: unaligned base or pitch, or box outside the tensor");
+        return QED2D_ERR_BAD_ARG;
+    }
+    const cuuint64_t dims[2] = {nx, ny};
+    const cuuint64_t strides[1] = {pitch};
+    const cuuint32_t box[2] = {bx, by};
+    const cuuint32_t es[2] = {1, 1};
+    const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(base), dims, strides, box, es,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled failed");
+        return QED2D_ERR_CUDA;
+    }
+    return QED2D_OK;
+}
+
+// the TMA-staged solver (schedule 7) for a tile height, or null where it has no instance
+static const void* uniform_kernel_tma(int rows) {
+    return rows == 16 ? (const void*)k_u_cg_mixed_tma<16> : rows == 8 ? (const void*)k_u_cg_mixed_tma<8> : nullptr;
+}
+static size_t uniform_tma_smem(int rows) {
+    return (size_t)kTmaStages * (rows == 16 ? UStage<16>::BYTES : UStage<8>::BYTES) + 128;
+}
+
 // the equal-size solver for schedule 0/1 (grid reductions), 4 (a barrier per
 // replica) or 5 (the same, lean reduction) and a tile height
 static const void* uniform_kernel(int sched, int rows) {
@@ -829,6 +875,7 @@ struct qed2d_batch {
     struct UVar {
         int rows = 0, per_block = 0, bpr = 0, grid = 0;
         long long ntr = 0;
+        bool tma = false;   // schedule 7 possible: whole tiles, an instance, co-resident with its shared memory
     } uv[3];
     int nuv = 0;                    // heights whose kernels fit (co-resident grid)
     int utile = -1;                 // index into uv of the tile height in use; -1 untuned
@@ -931,6 +978,9 @@ int tune_uniform(qed2d_batch* h, const UCGP& Q, int maxiter, Launch launch) {
     QCHECK(cudaEventCreate(&e0));
     QCHECK(cudaEventCreate(&e1));
     // candidates: (schedule, tile height); the height only when it is not fixed
+    // (schedule 7, the TMA-staged solver, is not a candidate: it gives the same
+    // bits as 5 and measured slower everywhere, e.g. 4 x 512^2 28.1 -> 33.5 us per
+    // iteration; callers can select it)
     constexpr int scheds[4] = {0, 1, 4, 5};
     const int nsched = h->nrep >= 2 ? 4 : 2;
     const int t_lo = h->utile_fixed ? h->utile : 0, t_hi = h->utile_fixed ? h->utile + 1 : h->nuv;
@@ -1135,6 +1185,33 @@ int r_solve(qed2d_batch* h, const double2* U, const float4* U32, const double2* 
             q.per_block = v.per_block;
             QCHECK(cudaMemsetAsync(&h->ctl->bar, 0, 2 * sizeof(unsigned long long) + sizeof(int), h->stream));
             if (sched >= 4) QCHECK(cudaMemsetAsync(h->d_ubar, 0, sizeof(unsigned long long) * 16 * h->nrep, h->stream));
+            if (sched == 7) {
+                if (!v.tma) {
+                    set_error("batch schedule 7 needs whole 32-site-wide tiles and co-resident blocks at this height");
+                    return QED2D_ERR_UNSUPPORTED;
+                }
+                UTma tm;
+                const unsigned long long L1 = (unsigned long long)q.g.L1, ny = (unsigned long long)q.g.L2 * q.g.B;
+                const unsigned rows = (unsigned)v.rows;
+                const float4* fld[4] = {q.r32, q.q0, q.q1, q.t32};
+                for (int f = 0; f < 4; f++) {
+                    QTRY(encode_map_2d(&tm.fc[f], fld[f], 4 * L1, ny, 16 * L1, 128, rows));
+                    QTRY(encode_map_2d(&tm.fk[f], fld[f], 4 * L1, ny, 16 * L1, 4, rows));
+                    QTRY(encode_map_2d(&tm.fw[f], fld[f], 4 * L1, ny, 16 * L1, 128, 1));
+                }
+                const float2* u1 = reinterpret_cast<const float2*>(q.U32);
+                const float2* u2 = u1 + h->Vtot;   // the second link plane
+                QTRY(encode_map_2d(&tm.u1c, u1, 2 * L1, ny, 8 * L1, 64, rows));
+                QTRY(encode_map_2d(&tm.u1l, u1, 2 * L1, ny, 8 * L1, 4, rows));
+                QTRY(encode_map_2d(&tm.u2c, u2, 2 * L1, ny, 8 * L1, 64, rows));
+                QTRY(encode_map_2d(&tm.u2b, u2, 2 * L1, ny, 8 * L1, 64, 1));
+                void* targs[] = {(void*)&q, (void*)&tm};
+                QCHECK(cudaLaunchCooperativeKernel(uniform_kernel_tma(v.rows), dim3((unsigned)v.grid),
+                                                   dim3((unsigned)(TX * v.rows)), targs, uniform_tma_smem(v.rows),
+                                                   h->stream));
+                count_launch();
+                return QED2D_OK;
+            }
             void* uargs[] = {(void*)&q};
             QCHECK(cudaLaunchCooperativeKernel(uniform_kernel(sched, v.rows), dim3((unsigned)v.grid),
                                                dim3((unsigned)(TX * v.rows)), uargs, 0, h->stream));
@@ -1301,6 +1378,14 @@ int batch_setup(qed2d_batch* h, const int* L1, const int* L2, const double* beta
             v.per_block = (int)((v.ntr + bpr - 1) / bpr);
             v.bpr = (int)((v.ntr + v.per_block - 1) / v.per_block);
             v.grid = v.bpr * B;
+            if (const void* kt = uniform_kernel_tma(rows); kt && R0.L1 % TX == 0 && R0.L2 % rows == 0) {
+                const size_t sm = uniform_tma_smem(rows);
+                int n7 = 0;
+                if (cudaFuncSetAttribute(kt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) == cudaSuccess &&
+                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n7, kt, TX * rows, sm) == cudaSuccess)
+                    v.tma = (long long)n7 * h->num_sms >= v.grid;
+                cudaGetLastError();
+            }
             h->uv[h->nuv++] = v;
         }
         if (h->nuv > 0) {
@@ -1427,10 +1512,10 @@ int qed2d_batch_set_stream(qed2d_batch* h, void* stream) {
 
 int qed2d_batch_set_schedule(qed2d_batch* h, int schedule) {
     const bool ok = h && (schedule == -1 || (h->uniform ? (schedule == 0 || schedule == 1 || schedule == 4 ||
-                                                          schedule == 5)
+                                                          schedule == 5 || schedule == 7)
                                                          : (schedule == 2 || schedule == 3)));
     if (!ok) {
-        set_error("qed2d_batch_set_schedule: -1, or 0/1/4/5 (equal sizes, at most 64 replicas), or 2/3 (otherwise)");
+        set_error("qed2d_batch_set_schedule: -1, or 0/1/4/5/7 (equal sizes, at most 64 replicas), or 2/3 (otherwise)");
         return QED2D_ERR_BAD_ARG;
     }
     if (h->uniform) h->usched = schedule;

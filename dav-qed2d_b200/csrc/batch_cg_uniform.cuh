@@ -20,6 +20,8 @@
 // index.
 #pragma once
 
+#include "tma.cuh"
+
 namespace qed2d {
 
 constexpr int kUniformReps = 64;
@@ -198,9 +200,113 @@ __device__ __forceinline__ bool ureduce(GridSync& gs, double v, const UCGP& P, d
          ++tt_, (++t1_ == TR.nt1 ? (t1_ = 0, ++t2_) : 0))                                       \
         if (const Site q = usite_at<TYv>(P.g, myr, t1_, t2_, threadIdx.x); q.ok)
 
-template <int RS, int TYv>
-__device__ __forceinline__ bool u_body(const UCGP& P, GridSync& gs, int& k, double* smem, RepState* s_st,
-                                       int* s_fl) {
+// ---------------------------------------------------------------------------
+// TMA staging of the stencil operands (schedule 7; lattices of whole 32 x TYv
+// tiles, L1 a multiple of 32).  The FP32 spinor fields are 2D float32 tensors of
+// (4 L1) x (B L2) elements (a replica's rows follow the previous replica's), the
+// link planes (2 L1) x (B L2).  For a tile, one box of the tile itself and four
+// one-wide boxes of its neighbours (the columns left and right, the rows below
+// and above), each at explicitly wrapped coordinates inside its own replica, so
+// no box leaves the tensor and every x coordinate is a multiple of 16 bytes
+// (4 floats; the link planes' left column is loaded two sites wide from i1 - 2).
+struct UTma {
+    // per spinor field (r32, q0, q1, t32): tile box, column box, row box
+    CUtensorMap fc[4], fk[4], fw[4];
+    CUtensorMap u1c, u1l, u2c, u2b;   // link planes: tile boxes, u1's left columns, u2's lower row
+};
+enum { TF_R = 0, TF_Q0 = 1, TF_Q1 = 2, TF_T = 3 };
+constexpr int kTmaStages = 2;   // stages per block: tiles staged one ahead (three measured slower)
+
+// one stage: a spinor field's five boxes (tile [TYv][32], left and right
+// columns [TYv], lower and upper rows [32]), float4 each, at 128-byte aligned
+// offsets; two spinor slots, then the link boxes
+template <int TYv>
+struct UStage {
+    static constexpr int C = TYv * 32 * 16, K = TYv * 16, W = 32 * 16;
+    static constexpr int FIELD = C + 2 * K + 2 * W;               // one spinor field's boxes
+    static constexpr int U1C = 2 * FIELD, U1L = U1C + TYv * 32 * 8;
+    static constexpr int U2C = U1L + TYv * 16, U2B = U2C + TYv * 32 * 8;
+    static constexpr int BYTES = U2B + 32 * 8;
+    static constexpr int LINKS = BYTES - U1C;
+    static_assert(TYv < 8 || (C % 128 == 0 && K % 128 == 0 && FIELD % 128 == 0 && U1L % 128 == 0 &&
+                              U2C % 128 == 0 && U2B % 128 == 0),
+                  "TMA destinations must be 128-byte aligned (tile heights of 8 rows and more)");
+};
+
+// The five values of a spinor field around site (lx, ly) of the tile staged at
+// `f` (pointer selects, so edge lanes take the halo without diverging).
+template <int TYv>
+__device__ __forceinline__ void tma_ld5(const char* f, int lx, int ly, Pair<float>& c, Pair<float>& p1,
+                                        Pair<float>& m1, Pair<float>& p2, Pair<float>& mm2) {
+    using S = UStage<TYv>;
+    const float4* C = reinterpret_cast<const float4*>(f);
+    const float4* K0 = reinterpret_cast<const float4*>(f + S::C);
+    const float4* K1 = reinterpret_cast<const float4*>(f + S::C + S::K);
+    const float4* W0 = reinterpret_cast<const float4*>(f + S::C + 2 * S::K);
+    const float4* W1 = reinterpret_cast<const float4*>(f + S::C + 2 * S::K + S::W);
+    const int o = ly * 32 + lx;
+    const float4 vc = C[o];
+    const float4 vp1 = *(lx < 31 ? C + o + 1 : K1 + ly);
+    const float4 vm1 = *(lx > 0 ? C + o - 1 : K0 + ly);
+    const float4 vp2 = *(ly < TYv - 1 ? C + o + 32 : W1 + lx);
+    const float4 vm2 = *(ly > 0 ? C + o - 32 : W0 + lx);
+    c = {make_float2(vc.x, vc.y), make_float2(vc.z, vc.w)};
+    p1 = {make_float2(vp1.x, vp1.y), make_float2(vp1.z, vp1.w)};
+    m1 = {make_float2(vm1.x, vm1.y), make_float2(vm1.z, vm1.w)};
+    p2 = {make_float2(vp2.x, vp2.y), make_float2(vp2.z, vp2.w)};
+    mm2 = {make_float2(vm2.x, vm2.y), make_float2(vm2.z, vm2.w)};
+}
+
+// the four links of site (lx, ly)'s stencil from the staged link boxes
+template <int TYv>
+__device__ __forceinline__ void tma_links(const char* st, int lx, int ly, float2& u1x, float2& u2x, float2& u1m1,
+                                          float2& u2m2) {
+    using S = UStage<TYv>;
+    const float2* U1 = reinterpret_cast<const float2*>(st + S::U1C);
+    const float2* U1L = reinterpret_cast<const float2*>(st + S::U1L);
+    const float2* U2 = reinterpret_cast<const float2*>(st + S::U2C);
+    const float2* U2B = reinterpret_cast<const float2*>(st + S::U2B);
+    const int o = ly * 32 + lx;
+    u1x = U1[o];
+    u2x = U2[o];
+    u1m1 = *(lx > 0 ? U1 + o - 1 : U1L + 2 * ly + 1);   // the left box holds sites i1 - 2 and i1 - 1
+    u2m2 = *(ly > 0 ? U2 + o - 32 : U2B + lx);
+}
+
+// Thread 0: the boxes of tile (t1, t2) of replica r into stage `st`, completing
+// on `bar`: spinor fields f0 (and f1 when f1 >= 0) and the links.
+template <int TYv>
+__device__ __forceinline__ void tma_issue(const UTma& T, const UGeom& g, char* st, uint64_t* bar, int r, int t1,
+                                          int t2, int f0, int f1) {
+    using S = UStage<TYv>;
+    const int L1 = g.L1, L2 = g.L2;
+    const int y = r * L2 + t2 * TYv;
+    const int ylo = r * L2 + (t2 == 0 ? L2 - 1 : t2 * TYv - 1);
+    const int yhi = r * L2 + ((t2 + 1) * TYv == L2 ? 0 : (t2 + 1) * TYv);
+    const int xl = t1 == 0 ? L1 - 1 : 32 * t1 - 1, xr = (32 * t1 + 32) % L1;
+    const int nf = f1 >= 0 ? 2 : 1;
+    mbar_arrive_expect_tx(bar, nf * S::FIELD + S::LINKS);
+    for (int j = 0; j < nf; j++) {
+        const int f = j ? f1 : f0;
+        char* d = st + j * S::FIELD;
+        tma_load_2d(d, &T.fc[f], 128 * t1, y, bar);
+        tma_load_2d(d + S::C, &T.fk[f], 4 * xl, y, bar);
+        tma_load_2d(d + S::C + S::K, &T.fk[f], 4 * xr, y, bar);
+        tma_load_2d(d + S::C + 2 * S::K, &T.fw[f], 128 * t1, ylo, bar);
+        tma_load_2d(d + S::C + 2 * S::K + S::W, &T.fw[f], 128 * t1, yhi, bar);
+    }
+    tma_load_2d(st + S::U1C, &T.u1c, 64 * t1, y, bar);
+    tma_load_2d(st + S::U1L, &T.u1l, 2 * (t1 == 0 ? L1 - 2 : 32 * t1 - 2), y, bar);
+    tma_load_2d(st + S::U2C, &T.u2c, 64 * t1, y, bar);
+    tma_load_2d(st + S::U2B, &T.u2b, 64 * t1, ylo, bar);
+}
+
+// TMA: the stencil operands of phases A and B come through shared memory
+// (T: the tensor maps; stg: kTmaStages stages; bar: their mbarriers), staged up
+// to kTmaStages - 1 tiles ahead.
+template <int RS, int TYv, bool TMA = false>
+__device__ __forceinline__ bool u_body(const UCGP& P, const UTma* T, char* stg, uint64_t* bar, GridSync& gs, int& k,
+                                       double* smem, RepState* s_st, int* s_fl) {
     const int myr = blockIdx.x / P.bpr, lb = blockIdx.x - myr * P.bpr;
     const TileRange TR = tile_range(P.g.ntr, P.g.nt1, P.per_block, lb);
     const long long V = P.g.V, sh = (long long)myr * V;   // FP64 planes of replica myr: base + sh, stride V
@@ -223,6 +329,47 @@ __device__ __forceinline__ bool u_body(const UCGP& P, GridSync& gs, int& k, doub
     // often (192 -> 176 algorithmic bytes per site-iteration).
     bool pend = false;
     float apend = 0.f;
+    // TMA staging: kTmaStages stages, the next to compute (sg), the mbarrier phase
+    // parities, this thread's site in the tile
+    constexpr int SB = UStage<TYv>::BYTES, NS = kTmaStages;
+    int sg = 0;
+    unsigned par = 0u;   // bit s: the phase parity stage s waits for next
+    const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
+    // Runs fn(stage, t1, t2) over the block's tiles with fields f0 (and f1) and
+    // the links of each tile staged, NS - 1 tiles ahead; a block barrier after
+    // each tile frees its stage for the next copy.  False (with no copy in
+    // flight) when a stage's copies did not complete.  (Per-stage "read"
+    // mbarriers with one arrival per warp instead of the block barrier measured
+    // slower: 4x512^2 33.5 -> 35.4 us per iteration.)
+    auto staged = [&](int f0, int f1, auto&& fn) -> bool {
+        const int n = TR.hi - TR.lo;
+        int t1 = TR.s1, t2 = TR.s2, i1 = TR.s1, i2 = TR.s2, issued = 0, si = sg;
+        if (threadIdx.x == 0) fence_proxy_async_global();   // the phase reads what the last one wrote
+        auto issue = [&]() {
+            if (threadIdx.x == 0) {
+                fence_proxy_async_shared();
+                tma_issue<TYv>(*T, P.g, stg + si * SB, bar + si, myr, i1, i2, f0, f1);
+            }
+            if (++i1 == TR.nt1) i1 = 0, ++i2;
+            si = si + 1 == NS ? 0 : si + 1;
+            ++issued;
+        };
+        while (issued < n && issued < NS - 1) issue();
+        for (int k = 0; k < n; k++) {
+            if (issued < n) issue();   // into the stage tile k - 1 released
+            const bool ok = mbar_wait(bar + sg, (par >> sg) & 1u, gs.err);
+            par ^= 1u << sg;
+            fn((const char*)(stg + sg * SB), t1, t2);
+            if (++t1 == TR.nt1) t1 = 0, ++t2;
+            sg = sg + 1 == NS ? 0 : sg + 1;
+            if (!__syncthreads_and(ok)) {   // drain the copies still in flight, then give up
+                for (int j = k + 1, s2 = sg; j < issued; j++, s2 = s2 + 1 == NS ? 0 : s2 + 1)
+                    mbar_wait(bar + s2, (par >> s2) & 1u, gs.err);
+                return false;
+            }
+        }
+        return true;
+    };
 
     {   // |b|^2 per replica; x = 0
         double v = 0.0;
@@ -255,7 +402,40 @@ __device__ __forceinline__ bool u_body(const UCGP& P, GridSync& gs, int& k, doub
         {   // p = r + beta p_old, t = g5Dw p, <p, A p> = |t|^2
             float f = 0.f;   // per-thread sum in FP32, one conversion per phase
             const RepState st = s_st[myr];
-            if (st.act) {
+            if constexpr (TMA) {
+                if (st.act) {   // r and p_old of the tile and its halo staged in shared memory
+                    const float beta = (float)st.beta;
+                    const bool use_p = !st.first;
+                    const bool ok = staged(TF_R, cur ? TF_Q0 : TF_Q1, [&](const char* sb, int t1, int t2) {
+                        Pair<float> c, p1, m1, p2, mm2;
+                        tma_ld5<TYv>(sb, lx, ly, c, p1, m1, p2, mm2);
+                        if (use_p) {
+                            Pair<float> w, w1, wm1, w2, wm2;
+                            tma_ld5<TYv>(sb + UStage<TYv>::FIELD, lx, ly, w, w1, wm1, w2, wm2);
+                            c.a = c.a + beta * w.a;
+                            c.b = c.b + beta * w.b;
+                            p1.a = p1.a + beta * w1.a;
+                            p1.b = p1.b + beta * w1.b;
+                            m1.a = m1.a + beta * wm1.a;
+                            m1.b = m1.b + beta * wm1.b;
+                            p2.a = p2.a + beta * w2.a;
+                            p2.b = p2.b + beta * w2.b;
+                            mm2.a = mm2.a + beta * wm2.a;
+                            mm2.b = mm2.b + beta * wm2.b;
+                        }
+                        float2 u1x, u2x, u1m1, u2m2;
+                        tma_links<TYv>(sb, lx, ly, u1x, u2x, u1m1, u2m2);
+                        Pair<float> tt_;
+                        g5dw_site<float>(c.a, c.b, p1.a, p1.b, m1.a, m1.b, p2.a, p2.b, mm2.a, mm2.b, u1x, u2x, u1m1,
+                                         u2m2, m2f, tt_.a, tt_.b);
+                        const Site q = usite_at<TYv>(P.g, myr, t1, t2, threadIdx.x);
+                        st_f(qn, q.x, c);
+                        st_f(P.t32, q.x, tt_);
+                        f += norm2(tt_.a) + norm2(tt_.b);
+                    });
+                    if (!ok) return false;
+                }
+            } else if (st.act) {
                 const SpAxpy<float, SpF> Q{SpF{P.r32}, SpF{qo}, (float)st.beta, !st.first};
                 FOR_MY_UTILES(q) {
                     const Pair<float> c = Q.ld(q.x);
@@ -270,7 +450,35 @@ __device__ __forceinline__ bool u_body(const UCGP& P, GridSync& gs, int& k, doub
         {   // x += alpha p, r -= alpha g5Dw t
             float f = 0.f;
             const RepState st = s_st[myr];
-            if (st.act) {
+            if (TMA && st.act) {   // t of the tile and its halo staged in shared memory
+                const float alpha = (float)st.alpha;
+                const bool ok = staged(TF_T, -1, [&](const char* sb, int t1, int t2) {
+                    const Site q = usite_at<TYv>(P.g, myr, t1, t2, threadIdx.x);
+                    Pair<float> c, p1, m1, p2, mm2, a;
+                    tma_ld5<TYv>(sb, lx, ly, c, p1, m1, p2, mm2);
+                    float2 u1x, u2x, u1m1, u2m2;
+                    tma_links<TYv>(sb, lx, ly, u1x, u2x, u1m1, u2m2);
+                    g5dw_site<float>(c.a, c.b, p1.a, p1.b, m1.a, m1.b, p2.a, p2.b, mm2.a, mm2.b, u1x, u2x, u1m1, u2m2,
+                                     m2f, a.a, a.b);
+                    Pair<float> r = SpF{P.r32}.ld(q.x);
+                    if (pend) {   // x += apend p_old, then x += alpha p
+                        const Pair<float> po = SpF{qo}.ld(q.x), pc = SpF{qn}.ld(q.x);
+                        Pair<float> xv = SpF{P.x32}.ld(q.x);
+                        xv.a = xv.a + apend * po.a;
+                        xv.b = xv.b + apend * po.b;
+                        xv.a = xv.a + alpha * pc.a;
+                        xv.b = xv.b + alpha * pc.b;
+                        st_f(P.x32, q.x, xv);
+                    }
+                    r.a = r.a - alpha * a.a;
+                    r.b = r.b - alpha * a.b;
+                    st_f(P.r32, q.x, r);
+                    f += norm2(r.a) + norm2(r.b);
+                });
+                if (!ok) return false;
+                apend = alpha;
+                pend = !pend;
+            } else if (st.act) {
                 const float alpha = (float)st.alpha;
                 if (pend) {
                     FOR_MY_UTILES(q) {   // x += apend p_old, then x += alpha p
@@ -365,7 +573,7 @@ __global__ void __launch_bounds__(32 * TYv, 32 / TYv) k_u_cg_mixed(const UCGP P)
     if constexpr (RS >= 2) {   // independent replicas: a barrier per replica; its blocks leave when it is done
         const int myr = blockIdx.x / P.bpr;
         GridSync gs{P.rbar + 16 * myr, &P.ctl->gen, &P.ctl->err, (unsigned)P.bpr};
-        const bool ok = u_body<RS, TYv>(P, gs, k, smem, s_st, s_fl);
+        const bool ok = u_body<RS, TYv>(P, nullptr, nullptr, nullptr, gs, k, smem, s_st, s_fl);
         if (blockIdx.x == myr * P.bpr && threadIdx.x == 0) {   // the replica's first block
             if (ok) P.st_out[myr] = s_st[myr];
             DevCtl* c = P.ctl;
@@ -375,7 +583,7 @@ __global__ void __launch_bounds__(32 * TYv, 32 / TYv) k_u_cg_mixed(const UCGP P)
         return;
     }
     GridSync gs{&P.ctl->bar, &P.ctl->gen, &P.ctl->err};
-    const bool ok = u_body<RS, TYv>(P, gs, k, smem, s_st, s_fl);
+    const bool ok = u_body<RS, TYv>(P, nullptr, nullptr, nullptr, gs, k, smem, s_st, s_fl);
     if (blockIdx.x == 0) {
         if (ok)   // every block holds the same records: block 0 stores them
             for (int r = threadIdx.x; r < P.g.B; r += blockDim.x) P.st_out[r] = s_st[r];
@@ -384,6 +592,38 @@ __global__ void __launch_bounds__(32 * TYv, 32 / TYv) k_u_cg_mixed(const UCGP P)
             c->last_iters = k;
             if (c->status == 0 && (ld_volatile_int(&c->err) || !ok)) c->status = QED2D_ERR_TIMEOUT;
         }
+    }
+}
+
+// Schedule 7: schedule 5 (independent replicas, lean reduction) with the
+// stencil operands of both CG phases staged by TMA one tile ahead (UTma).
+// Lattices of whole tiles only (L1 % 32 == 0, L2 % TYv == 0).  The arithmetic,
+// its order and the reductions are those of schedule 5, so the bits are too.
+// Dynamic shared memory: kTmaStages stages plus 128 bytes of alignment slack.
+template <int TYv>
+__global__ void __launch_bounds__(32 * TYv, 32 / TYv)
+    k_u_cg_mixed_tma(const __grid_constant__ UCGP P, const __grid_constant__ UTma T) {
+    extern __shared__ char dyn[];
+    __shared__ double smem[32];
+    __shared__ RepState s_st[kUniformReps];
+    __shared__ int s_fl[FL_N];
+    __shared__ __align__(8) uint64_t s_bar[kTmaStages];   // stage filled
+    char* stg = dyn + ((128u - (smem_addr(dyn) & 127u)) & 127u);
+    if (threadIdx.x < FL_N) s_fl[threadIdx.x] = 0;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < kTmaStages; i++) mbar_init(&s_bar[i], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    int k = 0;
+    const int myr = blockIdx.x / P.bpr;
+    GridSync gs{P.rbar + 16 * myr, &P.ctl->gen, &P.ctl->err, (unsigned)P.bpr};
+    const bool ok = u_body<3, TYv, true>(P, &T, stg, s_bar, gs, k, smem, s_st, s_fl);
+    if (blockIdx.x == myr * P.bpr && threadIdx.x == 0) {   // the replica's first block
+        if (ok) P.st_out[myr] = s_st[myr];
+        DevCtl* c = P.ctl;
+        if (myr == 0) c->last_iters = k;
+        if (ld_volatile_int(&c->err) || !ok) atomicCAS(&c->status, 0, QED2D_ERR_TIMEOUT);
     }
 }
 

@@ -766,9 +766,10 @@ class Batch:
     def schedule(self) -> int:
         """Schedule of the batched solver: -1 untuned; equal-size batches of at
         most 64 replicas 0/1 (reduction schedules), 4 (independent replicas, a
-        barrier per replica) or 5 (the same with a leaner reduction), all four
-        with the same bits; other batches 2 (one launch with grid barriers) or 3
-        (one thread-block cluster per replica)."""
+        barrier per replica), 5 (the same with a leaner reduction) or 7 (5 with
+        the stencil operands staged by TMA; replicas of whole 32 x 8 or 32 x 16
+        tiles), all with the same bits; other batches 2 (one launch with grid
+        barriers) or 3 (one thread-block cluster per replica)."""
         v = C.c_int(0)
         check(lib().qed2d_batch_get_schedule(self.h, C.byref(v)), "batch_get_schedule")
         return v.value

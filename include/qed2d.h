@@ -313,7 +313,10 @@ int qed2d_batch_set_stream(qed2d_batch* batch, void* cuda_stream);
  * as qed2d_ctx_set_schedule, 4 = independent replicas (each replica's blocks
  * have a barrier of their own and leave when it has converged), 5 = the same
  * with a leaner reduction (two block barriers per grid reduction instead of
- * seven); 0, 1, 4 and 5 give the same bits.  Other batches: 2 = one launch over all replicas with grid
+ * seven), 7 = schedule 5 with the stencil operands of each tile staged into
+ * shared memory by TMA one tile ahead (replicas of whole tiles only: L1 a
+ * multiple of 32, L2 of the tile height 8 or 16; QED2D_ERR_UNSUPPORTED
+ * otherwise); 0, 1, 4, 5 and 7 give the same bits.  Other batches: 2 = one launch over all replicas with grid
  * barriers, 3 = one thread-block cluster per replica (no grid barrier; replicas
  * stream through the GPU, largest first); these group their sums differently.
  * The first solve times the candidates and keeps the fastest; -1 = tune again

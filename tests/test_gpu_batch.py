@@ -293,6 +293,63 @@ def test_ragged_cluster_solver_matches_grid_solver(nrep):
     qed2d.set_precision("f64")
 
 
+@pytest.mark.parametrize("nrep,L1,L2", [(3, 64, 48), (2, 128, 64), (4, 64, 32)])
+def test_tma_schedule_same_bits_as_lean(nrep, L1, L2):
+    """Batch schedule 7 (the stencil operands of every tile staged into shared
+    memory by TMA one tile ahead) runs the arithmetic of schedule 5 in the same
+    order: identical iterations and solutions, bit for bit, at both tile
+    heights it supports; then two batched Nf=2 trajectories from the same start
+    give identical dH and links."""
+    import qed2d
+    b = qed2d.Batch(nrep, L1, L2, 4.0)
+    U, src = b.field(), b.field()
+    for r in range(nrep):
+        U[r] = to_dev(hot_links(L1, L2, 160 + r))
+        src[r] = to_dev(cgauss(L1, L2, 170 + r, 2))
+    am0 = [0.15 + 0.05 * r for r in range(nrep)]
+    for rows in (8, 16):
+        b.tile_rows = rows
+        out = []
+        for sched in (5, 7):
+            b.schedule = sched
+            x = b.field()
+            its, _ = b.cg(x, U, src, am0, 20000, 1e-24)
+            out.append((list(its), to_host(x)))
+        assert out[0][0] == out[1][0], rows
+        assert np.array_equal(out[0][1], out[1][1]), rows
+    traj = []
+    for sched in (5, 7):
+        bt = qed2d.Batch(nrep, L1, L2, 4.0)
+        bt.tile_rows, bt.schedule = 16, sched
+        Ut = bt.field()
+        for r in range(nrep):
+            Ut[r] = to_dev(hot_links(L1, L2, 180 + r))
+        infos = [bt.hmc_nf2(Ut, am0, 0.1, 4, 20000, 1e-24, [950 + r for r in range(nrep)], c) for c in (0, 1)]
+        traj.append(([(i.dH, i.cg_iterations) for inf in infos for i in inf], to_host(Ut)))
+    assert traj[0][0] == traj[1][0]
+    assert np.array_equal(traj[0][1], traj[1][1])
+
+
+@pytest.mark.parametrize("L1,L2,rows", [(100, 37, 8), (96, 40, 16), (64, 48, 4)])
+def test_tma_schedule_refuses_partial_tiles(L1, L2, rows):
+    """Schedule 7 needs whole tiles (L1 a multiple of 32, L2 of the tile height
+    8 or 16): otherwise the solve returns QED2D_ERR_UNSUPPORTED without
+    launching, and the batch still solves under its other schedules."""
+    import qed2d
+    b = qed2d.Batch(2, L1, L2, 4.0)
+    U, src = b.field(), b.field()
+    for r in range(2):
+        U[r] = to_dev(hot_links(L1, L2, 190 + r))
+        src[r] = to_dev(cgauss(L1, L2, 195 + r, 2))
+    b.tile_rows, b.schedule = rows, 7
+    with pytest.raises(qed2d.Qed2dError) as e:
+        b.cg(b.field(), U, src, 0.2, 20000, 1e-24)
+    assert e.value.status == qed2d._lib.UNSUPPORTED
+    b.schedule = 5
+    its, _ = b.cg(b.field(), U, src, 0.2, 20000, 1e-24)
+    assert min(its) > 0
+
+
 def test_independent_replica_schedule_trajectories():
     """Batched Nf=2 trajectories under the grid schedule (1) and the independent-
     replica schedule (4) from the same start: identical dH, iterations and links."""
