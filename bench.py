@@ -371,6 +371,8 @@ def run_ours(args):
     infos = [step() for _ in range(args.steps)]
     ev1.record()
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     launches = Lb.qed2d_launch_count() - n0
     clk = clocks.stop()
     elapsed = ev0.elapsed_time(ev1) / 1e3
