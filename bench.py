@@ -55,7 +55,8 @@ B_KRNL_FORCE = 64.0      # krnl_force!: links in 32 + frc1, frc2 out 16 + 16
 B_UPDT_FLD = 80.0        # updt_fld!: momenta in 16 + links in and out 32 + 32
 B_TR_DQWDU = 112.0       # tr_dQwdU: links 32 + X 32 + g5Dw X 32 in, force out 16
 B_PLAQ_FIELD = 40.0      # plaquette!: links in 32 + per-site plaquette out 8
-B_OMF4_STEP = 6 * 64.0 + 5 * 80.0   # one pure-gauge OMF4 step: 6 kicks (links 32 + momenta r/w 32), 5 link updates
+B_OMF4_STEP = 6 * 64.0 + 5 * 80.0   # one pure-gauge OMF4 step as the reference's kernels move it: 6 kicks
+                                    # (links 32 + momenta r/w 32), 5 link updates (the fused passes move 544)
 # Roofline units of the headline kernel.  Algorithmic bytes per site of one CG
 # iteration on (g5Dw)^2: 256 B in FP32 (two applies at 48 B + ten vector passes
 # at 16 B), 512 B in FP64 -- an FP64 reliable update is counted as one FP64
@@ -573,10 +574,12 @@ def run_ours(args):
             "updt_fld": kernel_gbs(lambda: qed2d.updt_fld_(Ub, mom, 1.0), B_UPDT_FLD),
             "tr_dQwdU": kernel_gbs(lambda: qed2d.tr_dQwdU(frc1, Ub, si, so, pb), B_TR_DQWDU),
             "plaquette_field": kernel_gbs(lambda: qed2d.plaquette_(plx, Ub, pb), B_PLAQ_FIELD),
-            "omf4_step_pure_gauge": kernel_gbs(lambda: qed2d.OMF4_(mom, Ub, 1e-3, 1, pb, None), B_OMF4_STEP),
+            # two steps per call (an even number of fused update+kick passes: no copy back), per step
+            "omf4_step_pure_gauge": kernel_gbs(lambda: qed2d.OMF4_(mom, Ub, 1e-3, 2, pb, None), 2 * B_OMF4_STEP),
             "bytes_per_site": {"krnl_force": B_KRNL_FORCE, "updt_fld": B_UPDT_FLD, "tr_dQwdU": B_TR_DQWDU,
                                "plaquette_field": B_PLAQ_FIELD, "omf4_step_pure_gauge": B_OMF4_STEP},
         }
+        gauge_kernels["omf4_step_pure_gauge"]["us"] /= 2   # per step
         del frc1, frc2, mom, plx
         qed2d.set_precision("mixed")
         xb = torch.zeros_like(si)

@@ -257,26 +257,73 @@ static int md_kick_rhmc(Ctx& c, double* mom, const double2* U, double2* X, const
     return launch_mom_kick(c, mom, U, eps, nullptr, nullptr, first ? nullptr : frc);
 }
 
+// Pure-gauge MD whose link updates are each followed by a kick: every such pair
+// runs as one k_updt_kick pass that reads one (links, momenta) buffer pair and
+// writes the other (the caller's arrays and a workspace pair, alternating), the
+// other kicks in place on the current pair; the caller's arrays hold the result
+// at the end (one copy when the pass count is odd).  Same operations in the same
+// order as separate updates and kicks; the compiler contracts them into FMAs
+// differently in the fused kernel, so results agree to rounding (1e-14 on links
+// after OMF4 trajectories), not bit for bit.  Lattices of whole 32 x 8 tiles
+// (kernel requirement) without an FP32 link copy to refresh.  Measured per
+// OMF4 step: up to 256^2 44.5 -> 34.9 us (fewer launches), 512^2 67.1 -> 49.5,
+// 2048^2 555 -> 516, 4096^2 2082 -> 1942, 8192^2 8274 -> 8179; but 1024^2
+// 112.8 -> 143.4 us, where the separate kernels' links and momenta (48 B/site)
+// stay in the 126 MB L2 and the two buffer pairs (96 B/site) do not -- so not
+// for 2^19 < V <= 2^21 sites.
+struct GaugePingPong {
+    Ctx& c;
+    double2* U[2];
+    double* mom[2];
+    int cur = 0;
+    bool on = false;
+    GaugePingPong(Ctx& c_, double2* U0, double* m0, const MDState& s) : c(c_) {
+        U[0] = U0;
+        mom[0] = m0;
+        U[1] = nullptr;
+        mom[1] = nullptr;
+        if (s.U32 || !updt_kick_fits(c) || (c.g.V > (1LL << 19) && c.g.V <= (1LL << 21))) return;
+        U[1] = c.spinor("md_u_alt");
+        mom[1] = c.real2("md_mom_alt");
+        on = U[1] && mom[1];
+    }
+    int kick(double eps) { return md_kick_gauge(c, mom[cur], U[cur], eps); }
+    int links_then_kick(double eu, double ek, MDState& s) {
+        if (!on) {
+            QTRY(md_links(c, U[cur], mom[cur], eu, s));
+            return md_kick_gauge(c, mom[cur], U[cur], ek);
+        }
+        QTRY(launch_updt_kick(c, U[cur ^ 1], U[cur], mom[cur ^ 1], mom[cur], eu, ek));
+        cur ^= 1;
+        return QED2D_OK;
+    }
+    int finish() {   // the result into the caller's arrays
+        if (cur == 0) return QED2D_OK;
+        QTRY(launch_copy(c, U[0], U[1], field_bytes(c)));
+        QTRY(launch_copy(c, mom[0], mom[1], sizeof(double) * 2 * (size_t)c.g.V));
+        cur = 0;
+        return QED2D_OK;
+    }
+};
+
 static int md_omf4_gauge(Ctx& c, double* mom, double2* U, double eps, int ns, MDState& s) {
     const double r5 = 0.5 - R1 - R3, r6 = 1.0 - 2.0 * (R2 + R4);
     const double cm[6] = {R1, R3, r5, r5, R3, R1};
     const double cu[5] = {R2, R4, r6, R4, R2};
-    for (int i = 0; i < ns; i++)
-        for (int k = 0; k < 6; k++) {
-            QTRY(md_kick_gauge(c, mom, U, cm[k] * eps));
-            if (k < 5) QTRY(md_links(c, U, mom, eps * cu[k], s));
-        }
-    return QED2D_OK;
+    GaugePingPong pp(c, U, mom, s);
+    for (int i = 0; i < ns; i++) {
+        QTRY(pp.kick(cm[0] * eps));
+        for (int k = 0; k < 5; k++) QTRY(pp.links_then_kick(eps * cu[k], cm[k + 1] * eps, s));
+    }
+    return pp.finish();
 }
 
 static int md_leapfrog_gauge(Ctx& c, double* mom, double2* U, double eps, int ns, MDState& s) {
-    QTRY(md_kick_gauge(c, mom, U, 0.5 * eps));
-    for (int i = 0; i < ns - 1; i++) {
-        QTRY(md_links(c, U, mom, eps, s));
-        QTRY(md_kick_gauge(c, mom, U, eps));
-    }
-    QTRY(md_links(c, U, mom, eps, s));
-    return md_kick_gauge(c, mom, U, 0.5 * eps);
+    GaugePingPong pp(c, U, mom, s);
+    QTRY(pp.kick(0.5 * eps));
+    for (int i = 0; i < ns - 1; i++) QTRY(pp.links_then_kick(eps, eps, s));
+    QTRY(pp.links_then_kick(eps, 0.5 * eps, s));
+    return pp.finish();
 }
 
 static int md_leapfrog_nf2(Ctx& c, double* mom, double2* U, double2* X, const double2* F, double2* g5DX,

@@ -108,6 +108,12 @@ int launch_unfold(Ctx& c, double2* Uout, const double2* Uin, int reflect);
 int launch_plwv(Ctx& c, double2* so, double k1, double k2);
 int launch_random_normal(Ctx& c, double* out, int64_t n, uint64_t seed, uint32_t stream, uint32_t counter,
                          double scale);
+// Uout = e^{i eu mom_in} Uin, then mom_out = mom_in + ek * gauge force(Uout): a
+// link update and the pure-gauge kick after it in one pass (distinct in/out
+// buffers); QED2D_ERR_UNSUPPORTED unless the lattice is whole 32 x 8 tiles
+int launch_updt_kick(Ctx& c, double2* Uout, const double2* Uin, double* mom_out, const double* mom_in, double eu,
+                     double ek);
+bool updt_kick_fits(const Ctx& c);   // the lattice is whole tiles of launch_updt_kick
 // mom += eps * (gauge force + fermion force), the fermion force either from
 // (X, G = g5Dw X) or precomputed in frc (either may be null)
 int launch_mom_kick(Ctx& c, double* mom, const double2* U, double eps, const double2* X, const double2* G,

@@ -277,6 +277,74 @@ __global__ void __launch_bounds__(TILE, FERM ? 4 : 6) k_mom_kick(double* __restr
     mom[q.x + V] = mo2 + eps * F2;
 }
 
+// updt_fld! followed by the pure-gauge kick, in one pass (OMF4! and leapfrog
+// pure gauge alternate the two, src/QED2dHMC.jl:248-305): Uout = e^{i eu mom_in} Uin,
+// mom_out = mom_in + ek F(Uout).  The tile's updated links and the halo the force
+// needs (U1 on rows -1..TY of columns -1..31, U2 on rows -1..TY-1 of columns
+// -1..32) are computed into shared memory, each with the operations of
+// updt_fld!; then the plaquettes of the tile, of the row below and of the
+// column to its left; then the kick with those of k_mom_kick.  Reads Uin and mom_in,
+// writes Uout and mom_out (distinct buffers: neighbours read the old momenta).  Lattices
+// of whole 32 x TY tiles only.  Per site: links in 32 + out 32, momenta in 16 +
+// out 16 (96 B) instead of 80 + 64 B for the two kernels.
+__global__ void __launch_bounds__(TILE) k_updt_kick(double2* __restrict__ Uout, const double2* __restrict__ Uin,
+                                                    double* __restrict__ mom_out, const double* __restrict__ mom_in, Lat g,
+                                                    double beta, double eu, double ek) {
+    constexpr int R1 = TY + 2, C1 = TX + 1;   // U1: rows -1..TY, columns -1..31
+    constexpr int R2 = TY + 1, C2 = TX + 2;   // U2: rows -1..TY-1, columns -1..32
+    __shared__ double2 s1[R1 * C1], s2[R2 * C2];
+    __shared__ double sv[(TY + 1) * (TX + 1)];   // v on rows -1..TY-1, columns -1..31
+    int t1, t2;
+    if (gridDim.y > 1 || g.L2 <= TY) {
+        t1 = blockIdx.x;
+        t2 = blockIdx.y;
+    } else {
+        const int nt1 = g.L1 / TX;
+        t2 = blockIdx.x / nt1;
+        t1 = blockIdx.x - t2 * nt1;
+    }
+    const long long V = g.V;
+    const int i10 = t1 * TX, i20 = t2 * TY;
+    // the updated link of direction mu at tile position (row, col), periodic
+    auto upd = [&](int mu, int row, int col, bool own) {
+        int i1 = i10 + col, i2 = i20 + row;
+        i1 = i1 < 0 ? i1 + g.L1 : (i1 >= g.L1 ? i1 - g.L1 : i1);
+        i2 = i2 < 0 ? i2 + g.L2 : (i2 >= g.L2 ? i2 - g.L2 : i2);
+        const long long x = i1 + (long long)g.L1 * i2 + (mu ? V : 0);
+        double s, c;
+        sincos(eu * mom_in[x], &s, &c);
+        const double2 u = cmul(make_double2(c, s), Uin[x]);
+        if (own) Uout[x] = u;
+        return u;
+    };
+    for (int e = threadIdx.x; e < R1 * C1; e += TILE) {
+        const int row = e / C1 - 1, col = e % C1 - 1;
+        s1[e] = upd(0, row, col, row >= 0 && row < TY && col >= 0);
+    }
+    for (int e = threadIdx.x; e < R2 * C2; e += TILE) {
+        const int row = e / C2 - 1, col = e % C2 - 1;
+        s2[e] = upd(1, row, col, row >= 0 && col >= 0 && col < TX);
+    }
+    __syncthreads();
+    // v(y) = beta Im P(y) from U1(y), U2(y + 1), U1(y + 2), U2(y)
+    for (int e = threadIdx.x; e < (TY + 1) * (TX + 1); e += TILE) {
+        const int row = e / (TX + 1) - 1, col = e % (TX + 1) - 1;
+        if (row >= 0 && col >= 0 || row < 0 && col >= 0 || row >= 0 && col < 0) {   // not the corner
+            const double2 u1y = s1[(row + 1) * C1 + col + 1], u1yp2 = s1[(row + 2) * C1 + col + 1];
+            const double2 u2y = s2[(row + 1) * C2 + col + 1], u2yp1 = s2[(row + 1) * C2 + col + 2];
+            sv[e] = beta * plaquette_of(u1y, u2yp1, u1yp2, u2y).y;
+        }
+    }
+    __syncthreads();
+    const int lx = threadIdx.x & (TX - 1), ly = threadIdx.x >> 5;
+    const long long x = (i10 + lx) + (long long)g.L1 * (i20 + ly);
+    const double v = sv[(ly + 1) * (TX + 1) + lx + 1];
+    const double F1 = -v + sv[ly * (TX + 1) + lx + 1];
+    const double F2 = v - sv[(ly + 1) * (TX + 1) + lx];
+    mom_out[x] = mom_in[x] + ek * F1;
+    mom_out[x + V] = mom_in[x + V] + ek * F2;
+}
+
 // y = a x + b z (complex scalars; z may alias y)
 __global__ void k_zaxpby(double2* y, double2 a, const double2* x, double2 b, const double2* z,
                          long long n) {
@@ -485,6 +553,15 @@ int launch_random_normal(Ctx& c, double* out, int64_t n, uint64_t seed, uint32_t
     if (n <= 0) return QED2D_OK;
     k_random_normal<<<blocks_for((n + 1) / 2, 256), 256, 0, c.stream>>>(out, n, seed, stream, counter, scale);
     return post_launch("k_random_normal");
+}
+
+bool updt_kick_fits(const Ctx& c) { return c.g.L1 % TX == 0 && c.g.L2 % TY == 0; }
+
+int launch_updt_kick(Ctx& c, double2* Uout, const double2* Uin, double* mom_out, const double* mom_in, double eu,
+                     double ek) {
+    if (!updt_kick_fits(c)) return QED2D_ERR_UNSUPPORTED;
+    k_updt_kick<<<tiles_grid2(c.g), TILE, 0, c.stream>>>(Uout, Uin, mom_out, mom_in, c.g, c.beta, eu, ek);
+    return post_launch("k_updt_kick");
 }
 
 int launch_mom_kick(Ctx& c, double* mom, const double2* U, double eps, const double2* X, const double2* G,
