@@ -32,6 +32,7 @@
 #include <type_traits>
 #include <vector>
 
+#include "graph.h"
 #include "stencil.cuh"
 
 namespace qed2d {
@@ -892,13 +893,17 @@ struct qed2d_batch {
     DevCtl* ctl = nullptr;
     DevCtl* ctl_host = nullptr;
     std::map<std::string, std::pair<void*, size_t>> ws;
+    uint64_t ws_gen = 0;            // bumped whenever a workspace buffer is reallocated
+    GraphCache md_graph;            // MD integration of qed2d_batch_hmc_nf2 (graph.h)
 
     void* buf(const std::string& name, size_t bytes) {
         auto it = ws.find(name);
         if (it != ws.end() && it->second.second >= bytes) return it->second.first;
         if (it != ws.end()) {
+            cudaStreamSynchronize(stream);
             cudaFree(it->second.first);
             ws.erase(it);
+            ws_gen++;   // a captured graph holding the old address is stale
         }
         void* p = nullptr;
         if (cudaMalloc(&p, bytes) != cudaSuccess) {
@@ -1492,6 +1497,7 @@ int qed2d_batch_destroy(qed2d_batch* h) {
     if (!h) return QED2D_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
     else cudaDeviceSynchronize();
+    h->md_graph.release();
     for (auto& kv : h->ws) cudaFree(kv.second.first);
     void* dev[] = {h->d_reps,  h->d_tiles, h->d_seg0,  h->d_segs,  h->d_order, h->d_rep_seg, h->d_dbase_c,
                    h->d_dbase_r, h->d_m2,  h->d_beta,  h->d_seed,  h->d_st,    h->d_flags,   h->d_red,
@@ -1501,6 +1507,23 @@ int qed2d_batch_destroy(qed2d_batch* h) {
         if (p) cudaFree(p);
     if (h->ctl_host) cudaFreeHost(h->ctl_host);
     delete h;
+    return QED2D_OK;
+}
+
+int qed2d_batch_set_graphs(qed2d_batch* h, int on) {
+    if (!h) return QED2D_ERR_BAD_ARG;
+    h->md_graph.drop();
+    h->md_graph.on = on != 0;
+    return QED2D_OK;
+}
+
+int qed2d_batch_graph_stats(const qed2d_batch* h, int* on, int64_t* captures, int64_t* replays, int64_t* failures) {
+    if (!h) return QED2D_ERR_BAD_ARG;
+    const GraphCache& g = h->md_graph;
+    if (on) *on = g.on ? 1 : 0;
+    if (captures) *captures = g.captures;
+    if (replays) *replays = g.replays;
+    if (failures) *failures = g.failures;
     return QED2D_OK;
 }
 
@@ -1623,15 +1646,22 @@ int qed2d_batch_hmc_nf2(qed2d_batch* h, double* Ud, const double* am0, double ep
     QTRY(r_sums(h, U, mom, X, nullptr, 0));
     k_r_g5dw<<<h->ntiles, TILE, 0, s>>>(F, U, X, h->tv(), h->d_m2);
     QTRY(r_post("k_r_g5dw"));
-    QTRY(r_pack(h, U, mom, 0.0, U32));
-    // leapfrog (src/QED2dHMC.jl:426-449)
-    QTRY(r_kick(h, mom, U, U32, X, F, G, 0.5 * eps, maxiter, tol));
-    for (int i = 0; i < ns - 1; i++) {
+    // FP32 links, then leapfrog (src/QED2dHMC.jl:426-449): replayed from a CUDA
+    // graph from the third trajectory with the same arguments on (graph.h)
+    GraphKey k;
+    k.p(U).p(mom).p(X).p(F).p(G).p(U32).d(eps).i(ns).i(maxiter).d(tol);
+    k.i(h->usched).i(h->utile).i(h->rsched).i(h->rcs).i((long long)h->ws_gen);
+    for (int r = 0; r < B; r++) k.d(h->m2[r]);
+    QTRY(run_graphed(h->md_graph, h->stream, k.s, [&]() -> int {
+        QTRY(r_pack(h, U, mom, 0.0, U32));
+        QTRY(r_kick(h, mom, U, U32, X, F, G, 0.5 * eps, maxiter, tol));
+        for (int i = 0; i < ns - 1; i++) {
+            QTRY(r_pack(h, U, mom, eps, U32));
+            QTRY(r_kick(h, mom, U, U32, X, F, G, eps, maxiter, tol));
+        }
         QTRY(r_pack(h, U, mom, eps, U32));
-        QTRY(r_kick(h, mom, U, U32, X, F, G, eps, maxiter, tol));
-    }
-    QTRY(r_pack(h, U, mom, eps, U32));
-    QTRY(r_kick(h, mom, U, U32, X, F, G, 0.5 * eps, maxiter, tol));
+        return r_kick(h, mom, U, U32, X, F, G, 0.5 * eps, maxiter, tol);
+    }));
     // H_fin with <X, F> (:82)
     QTRY(r_sums(h, U, mom, X, F, 1));
     std::vector<double> sc(2 * 5 * (size_t)B);

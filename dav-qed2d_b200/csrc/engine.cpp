@@ -11,6 +11,7 @@
 #include <string>
 #include <vector>
 
+#include "graph.h"
 #include "internal.h"
 
 struct qed2d_ctx {
@@ -39,6 +40,7 @@ void* Ctx::buf(const std::string& name, size_t bytes) {
         cudaStreamSynchronize(stream);
         cudaFree(it->second.first);
         ws.erase(it);
+        ws_gen++;   // a captured graph holding the old address is stale
     }
     void* p = nullptr;
     if (cudaMalloc(&p, bytes) != cudaSuccess) {
@@ -427,6 +429,7 @@ int qed2d_ctx_destroy(qed2d_ctx* ctx) {
     Ctx& c = ctx->c;
     if (c.stream) cudaStreamSynchronize(c.stream);
     else cudaDeviceSynchronize();
+    c.md_graph.release();
     for (auto& kv : c.ws) cudaFree(kv.second.first);
     if (c.ctl) cudaFree(c.ctl);
     if (c.part) cudaFree(c.part);
@@ -501,6 +504,23 @@ int qed2d_ctx_set_multishift_layout(qed2d_ctx* ctx, int layout) {
 int qed2d_ctx_get_multishift_layout(const qed2d_ctx* ctx, int* layout) {
     if (!ctx || !layout) return bad_arg("context or layout is NULL");
     *layout = ctx->c.ms_layout;
+    return QED2D_OK;
+}
+
+int qed2d_ctx_set_graphs(qed2d_ctx* ctx, int on) {
+    QCTX(ctx);
+    c.md_graph.drop();
+    c.md_graph.on = on != 0;
+    return QED2D_OK;
+}
+
+int qed2d_ctx_graph_stats(const qed2d_ctx* ctx, int* on, int64_t* captures, int64_t* replays, int64_t* failures) {
+    if (!ctx) return bad_arg("context is NULL");
+    const GraphCache& g = ctx->c.md_graph;
+    if (on) *on = g.on ? 1 : 0;
+    if (captures) *captures = g.captures;
+    if (replays) *replays = g.replays;
+    if (failures) *failures = g.failures;
     return QED2D_OK;
 }
 
@@ -1074,9 +1094,13 @@ int qed2d_hmc_gauge(qed2d_ctx* ctx, double* U, double eps, int ns, int integrato
     QTRY(launch_copy(c, Ucp, U, field_bytes(c)));
     QTRY(launch_random_normal(c, mom, 2 * c.g.V, seed, QED2D_STREAM_MOMENTA, counter, 1.0));
     QTRY(launch_reduce_gauge(c, C2(U), mom, 0));
-    MDState s;
-    if (integrator == QED2D_OMF4) QTRY(md_omf4_gauge(c, mom, C2(U), eps, ns, s));
-    else QTRY(md_leapfrog_gauge(c, mom, C2(U), eps, ns, s));
+    GraphKey k;
+    k.i(1).p(U).p(mom).d(eps).i(ns).i(integrator).d(c.beta).i((long long)c.ws_gen);
+    QTRY(run_graphed(c.md_graph, c.stream, k.s, [&]() -> int {
+        MDState s;
+        if (integrator == QED2D_OMF4) return md_omf4_gauge(c, mom, C2(U), eps, ns, s);
+        return md_leapfrog_gauge(c, mom, C2(U), eps, ns, s);
+    }));
     QTRY(launch_reduce_gauge(c, C2(U), mom, 4));
     double h[8];
     QTRY(fetch_scal(c, 0, 8, h));
@@ -1111,10 +1135,20 @@ int qed2d_hmc_nf2(qed2d_ctx* ctx, double* U, double am0, double eps, int ns, int
     QTRY(launch_reduce_vec(c, 0, X, nullptr, N, 3));
     // F = g5Dw X  (:76-78)
     QTRY(launch_g5dw(c, F, C2(U), X, am0, nullptr, make_double2(0, 0), false));
-    MDState s;
-    QTRY(md_prepare(c, C2(U), s));
-    if (integrator == QED2D_OMF4) QTRY(md_omf4_nf2(c, mom, C2(U), X, F, g5DX, am0, eps, ns, maxiter, tol, s));
-    else QTRY(md_leapfrog_nf2(c, mom, C2(U), X, F, g5DX, am0, eps, ns, maxiter, tol, s));
+    auto md = [&]() -> int {
+        MDState s;
+        QTRY(md_prepare(c, C2(U), s));
+        if (integrator == QED2D_OMF4) return md_omf4_nf2(c, mom, C2(U), X, F, g5DX, am0, eps, ns, maxiter, tol, s);
+        return md_leapfrog_nf2(c, mom, C2(U), X, F, g5DX, am0, eps, ns, maxiter, tol, s);
+    };
+    if (c.precision == QED2D_PREC_PLAIN) {   // host-synchronised solver: not capturable
+        QTRY(md());
+    } else {
+        GraphKey k;
+        k.i(2).p(U).p(mom).p(X).p(F).p(g5DX).d(am0).d(eps).i(ns).i(integrator).i(maxiter).d(tol).d(c.beta);
+        k.i(c.precision).i(c.sched[0]).i(c.sched[1]).i((long long)c.ws_gen);
+        QTRY(run_graphed(c.md_graph, c.stream, k.s, md));
+    }
     QTRY(launch_reduce_gauge(c, C2(U), mom, 4));
     QTRY(launch_reduce_vec(c, 1, X, F, N, 8));
     double h[10];
@@ -1171,8 +1205,23 @@ int qed2d_hmc_rhmc(qed2d_ctx* ctx, double* U, int nf, const double* am0, double 
         QTRY(pf_generate_core(c, C2(F[j]), C2(U), X, am0[j], maxiter, tol, &rprm[j]));
     }
     MDState s;
-    QTRY(md_prepare(c, C2(U), s));
-    QTRY(md_leapfrog_rhmc(c, mom, C2(U), X, F.data(), g5DX, nf, am0, eps, ns, maxiter, tol, rprm, s));
+    auto md = [&]() -> int {
+        QTRY(md_prepare(c, C2(U), s));
+        return md_leapfrog_rhmc(c, mom, C2(U), X, F.data(), g5DX, nf, am0, eps, ns, maxiter, tol, rprm, s);
+    };
+    if (c.precision == QED2D_PREC_PLAIN) {   // host-synchronised solver: not capturable
+        QTRY(md());
+    } else {
+        GraphKey k;
+        k.i(3).p(U).p(mom).p(X).p(g5DX).i(nf).d(eps).i(ns).i(maxiter).d(tol).d(c.beta);
+        k.i(c.precision).i(c.sched[0]).i(c.sched[1]).i(c.sched[2]).i(c.ms_layout).i((long long)c.ws_gen);
+        for (int j = 0; j < nf; j++) {
+            k.p(F[j]).d(am0[j]).i(rprm[j].n);
+            for (int i = 0; i < rprm[j].n; i++) k.d(rprm[j].mu[i]).d(rprm[j].rho[i]);
+        }
+        QTRY(run_graphed(c.md_graph, c.stream, k.s, md));
+        s.U32 = c.precision == QED2D_PREC_MIXED ? c.spinor32("md_u32") : nullptr;   // as md_prepare leaves it
+    }
     QTRY(launch_reduce_gauge(c, C2(U), mom, 4));
     QTRY(fetch_scal(c, 4, 3, &h[4]));
     double hfin = h[6] / 2.0 + c.beta * (V - h[4]);

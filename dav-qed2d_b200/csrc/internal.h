@@ -39,6 +39,29 @@ constexpr int kMaxPartBlocks = 2048;   // partial-sum slots per reduced quantity
 constexpr int kMsLayoutCount = 4;      // layouts of the multishift kernel (tile rows, threads per site)
 constexpr int kMaxPartVals = 8;        // quantities reduced together
 
+// CUDA graph of the MD part of a trajectory, replayed per trajectory (graph.h)
+struct GraphCache {
+    bool on = true;
+    std::string key;    // key of exec
+    std::string warm;   // key of the last direct run
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t cap = nullptr;   // private capture stream
+    int64_t nlaunch = 0;          // library launches inside the graph
+    int64_t captures = 0, replays = 0, failures = 0;
+
+    void drop() {
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        key.clear();
+        warm.clear();
+    }
+    void release() {
+        drop();
+        if (cap) cudaStreamDestroy(cap);
+        cap = nullptr;
+    }
+};
+
 struct Ctx {
     Lat g;
     double beta = 0.0;
@@ -55,6 +78,8 @@ struct Ctx {
     double last_relres = 0.0;
     int sched[3] = {-1, -1, -1};   // reduction schedule of the F64 / MIXED / multishift solvers (-1: not tuned yet)
     int ms_layout = -1;            // layout of the multishift kernel (kMsLayouts; -1: tuned with the schedule)
+    GraphCache md_graph;           // MD integration of the HMC trajectories (graph.h)
+    uint64_t ws_gen = 0;           // bumped whenever a workspace buffer is reallocated
 
     void* buf(const std::string& name, size_t bytes);   // grow-only named workspace
     double2* spinor(const std::string& name) { return (double2*)buf(name, sizeof(double2) * 2 * g.V); }

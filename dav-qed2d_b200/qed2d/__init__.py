@@ -329,6 +329,25 @@ def get_schedule(prm: LattParm, precision="mixed") -> int:
     return v.value
 
 
+def set_graphs(prm: LattParm, on: bool) -> None:
+    """Turn CUDA-graph replay of the MD integration of HMC_ on or off for this
+    lattice's context (on by default): the first trajectory with given
+    arguments runs its launches directly, the second captures them into a
+    graph, later ones replay it.  Results are bitwise those of direct launches."""
+    check(lib().qed2d_ctx_set_graphs(_c(prm), 1 if on else 0), "set_graphs")
+
+
+def _stats(fn, h):
+    on, cap, rep, fail = C.c_int(0), C.c_int64(0), C.c_int64(0), C.c_int64(0)
+    check(fn(h, C.byref(on), C.byref(cap), C.byref(rep), C.byref(fail)), "graph_stats")
+    return {"on": bool(on.value), "captures": cap.value, "replays": rep.value, "failures": fail.value}
+
+
+def graph_stats(prm: LattParm) -> dict:
+    """{"on", "captures", "replays", "failures"} of this lattice's MD graph."""
+    return _stats(lib().qed2d_ctx_graph_stats, _c(prm))
+
+
 def last_solve(prm: LattParm):
     """(iterations, |r|^2/|b|^2, reliable updates) of the most recent solve on this lattice."""
     it, rel, upd = C.c_int64(0), C.c_double(0), C.c_int64(0)
@@ -789,6 +808,16 @@ class Batch:
     @tile_rows.setter
     def tile_rows(self, rows: int) -> None:
         check(lib().qed2d_batch_set_tile_rows(self.h, int(rows)), "batch_set_tile_rows")
+
+    @property
+    def graphs(self) -> dict:
+        """{"on", "captures", "replays", "failures"} of the batch's MD graph
+        (CUDA-graph replay of the leapfrog inside hmc_nf2, on by default)."""
+        return _stats(lib().qed2d_batch_graph_stats, self.h)
+
+    @graphs.setter
+    def graphs(self, on: bool) -> None:
+        check(lib().qed2d_batch_set_graphs(self.h, 1 if on else 0), "batch_set_graphs")
 
     def field(self, dtype=torch.complex128):
         if self.uniform:

@@ -51,6 +51,8 @@ SIGNATURES = {
     "qed2d_ctx_get_schedule": (I, [P, I, PI]),
     "qed2d_ctx_set_multishift_layout": (I, [P, I]),
     "qed2d_ctx_get_multishift_layout": (I, [P, PI]),
+    "qed2d_ctx_set_graphs": (I, [P, I]),
+    "qed2d_ctx_graph_stats": (I, [P, PI, PI64, PI64, PI64]),
     "qed2d_last_solve": (I, [P, PI64, PD, PI64]),
     "qed2d_selftest_barrier_timeout": (I, [P, I64]),
     "qed2d_status_string": (C.c_char_p, [I]),
@@ -106,6 +108,8 @@ SIGNATURES = {
     "qed2d_batch_get_schedule": (I, [P, PI]),
     "qed2d_batch_set_tile_rows": (I, [P, I]),
     "qed2d_batch_get_tile_rows": (I, [P, PI]),
+    "qed2d_batch_set_graphs": (I, [P, I]),
+    "qed2d_batch_graph_stats": (I, [P, PI, PI64, PI64, PI64]),
     "qed2d_batch_destroy": (I, [P]),
     "qed2d_batch_set_stream": (I, [P, P]),
     "qed2d_batch_cg": (I, [P, P, P, P, PD, I, D, PI, PI]),

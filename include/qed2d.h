@@ -134,6 +134,23 @@ int qed2d_ctx_get_schedule(const qed2d_ctx* ctx, int precision, int* schedule);
  * and 512^2 layout 0 fastest (12.7 and 42.9 us). */
 int qed2d_ctx_set_multishift_layout(qed2d_ctx* ctx, int layout);
 int qed2d_ctx_get_multishift_layout(const qed2d_ctx* ctx, int* layout);
+
+/* No counterpart in the reference (CUDA.jl enqueues and synchronises every
+ * launch from the host).  CUDA-graph replay of the MD integration inside
+ * qed2d_hmc_gauge, qed2d_hmc_nf2 and qed2d_hmc_rhmc (not in the PLAIN
+ * precision, whose solver reads scalars back every iteration; not the RHMC
+ * reversibility pass): the first trajectory with a given set of arguments runs
+ * directly (it tunes the solvers and allocates the workspace), the second
+ * captures its MD launches -- every force evaluation's persistent solver
+ * launch, the kicks and the link updates -- into a graph, and later ones replay
+ * it with one cudaGraphLaunch.  Any change of arguments, field pointers,
+ * precision, schedule, beta or workspace starts over.  Results are bitwise
+ * those of the direct launches.  On by default; a capture the driver refuses
+ * turns it off for the context (failures counts those).  set: 0 off, 1 on
+ * (drops a captured graph).  stats: on, graphs captured, graph launches,
+ * failed captures (any pointer may be NULL). */
+int qed2d_ctx_set_graphs(qed2d_ctx* ctx, int on);
+int qed2d_ctx_graph_stats(const qed2d_ctx* ctx, int* on, int64_t* captures, int64_t* replays, int64_t* failures);
 /* Self-test of failure detection (no counterpart in the reference): runs one
  * kernel whose grid-barrier wait can never complete, with the wait bounded to
  * `polls` polls (1..2^26, rounded up to a multiple of 8: the limit is checked
@@ -332,6 +349,15 @@ int qed2d_batch_get_schedule(const qed2d_batch* batch, int* schedule);
  * agree to rounding, not bit for bit.  Other batches: BAD_ARG. */
 int qed2d_batch_set_tile_rows(qed2d_batch* batch, int rows);
 int qed2d_batch_get_tile_rows(const qed2d_batch* batch, int* rows);
+/* No counterpart in the reference.  CUDA-graph replay of the leapfrog inside
+ * qed2d_batch_hmc_nf2 (the FP32 link copy, every force evaluation's batched
+ * solver launch, the kicks and link updates), with the protocol and stats of
+ * qed2d_ctx_set_graphs / qed2d_ctx_graph_stats: direct on the first trajectory
+ * with given arguments (masses, eps, ns, tolerances, field pointers,
+ * schedules), captured on the second, replayed after.  On by default. */
+int qed2d_batch_set_graphs(qed2d_batch* batch, int on);
+int qed2d_batch_graph_stats(const qed2d_batch* batch, int* on, int64_t* captures, int64_t* replays,
+                            int64_t* failures);
 /* every replica's CG method 1 (src/QED2dSolver.jl:3-46) in one launch:
  * x_r = ((g5Dw)^2)^-1 b_r with mass am0[r]; iterations[nrep] and updates[nrep]
  * (FP64 reliable updates) may be NULL */
