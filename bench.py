@@ -66,12 +66,12 @@ B_ITER_F32 = 256.0
 B_ITER_F64 = 512.0
 # Measured traffic per site-iteration of k_u_cg_mixed at 4 x 512^2, from one ncu
 # capture of a 100-iteration launch of the tuned kernel (independent replicas,
-# lean reduction, 32 x 16 tiles): DRAM read + write (6.560 GB over 1,048,576
-# sites x 100) and L1 <-> L2 (16.15 GB read + 6.56 GB written); both grow in
-# proportion to the iterations at fixed size
-U_DRAM_PER_SITE_ITER = 62.6
-U_L2_PER_SITE_ITER = 217.0
-U_L2_THROUGHPUT = 0.352   # lts__throughput.avg.pct_of_peak_sustained_elapsed of the same capture
+# lean reduction, phase-A stencil on r, 32 x 16 tiles): DRAM read + write
+# (6.780 GB over 1,048,576 sites x 100) and L1 <-> L2 (17.21 GB read + 6.56 GB
+# written); both grow in proportion to the iterations at fixed size
+U_DRAM_PER_SITE_ITER = 64.7
+U_L2_PER_SITE_ITER = 226.7
+U_L2_THROUGHPUT = 0.373   # lts__throughput.avg.pct_of_peak_sustained_elapsed of the same capture
 ENS_NS, ENS_EPS = 10, 0.1   # replica ensemble: leapfrog ns=10, eps=0.1
 CPU_TRAJ = 2                # trajectories of the GPU arm's CPU-baseline sample
 
@@ -444,7 +444,9 @@ def run_ours(args):
                     "accepted": sum(p[1] for p in per_rep), "of": n_traj * len(sizes),
                     "timed": f"{n_traj} batched trajectories after 1 warm-up",
                     "solver": {2: "one launch over all replicas, grid barriers",
-                               3: "one thread-block cluster per replica"}.get(eb.schedule, "untuned")}
+                               3: "one thread-block cluster per replica",
+                               6: "one thread-block cluster per replica, phase-A stencil on r"}.get(eb.schedule,
+                                                                                                    "untuned")}
         del eb, Ue
         torch.cuda.empty_cache()
 
@@ -489,7 +491,8 @@ def run_ours(args):
                 "schedule": {0: "last block publishes the sums", 1: "every block sums",
                              4: "independent replicas (a barrier per replica)",
                              5: "independent replicas, lean reduction",
-                             7: "independent replicas, lean reduction, TMA-staged stencil operands"}.get(
+                             7: "independent replicas, lean reduction, TMA-staged stencil operands",
+                             8: "independent replicas, lean reduction, phase-A stencil on r"}.get(
                                  batch.schedule, "untuned"),
                 "tile_rows": batch.tile_rows,
                 "note": f"one launch = one solve of all {B} replicas: per replica iterations {min(its)}-{max(its)} "

@@ -774,11 +774,11 @@ namespace qed2d {
 // the first is the default when the tuner is off
 constexpr int kUTileRows[3] = {8, 16, 4};
 
-template <int RS>
+template <int RS, bool RSTEN = false>
 static const void* uniform_kernel_rs(int rows) {
-    return rows == 4    ? (const void*)k_u_cg_mixed<RS, 4>
-           : rows == 16 ? (const void*)k_u_cg_mixed<RS, 16>
-                        : (const void*)k_u_cg_mixed<RS, 8>;
+    return rows == 4    ? (const void*)k_u_cg_mixed<RS, 4, RSTEN>
+           : rows == 16 ? (const void*)k_u_cg_mixed<RS, 16, RSTEN>
+                        : (const void*)k_u_cg_mixed<RS, 8, RSTEN>;
 }
 
 // host: cuTensorMapEncodeTiled through the runtime's driver entry point
@@ -828,12 +828,14 @@ static size_t uniform_tma_smem(int rows) {
 }
 
 // the equal-size solver for schedule 0/1 (grid reductions), 4 (a barrier per
-// replica) or 5 (the same, lean reduction) and a tile height
+// replica), 5 (the same, lean reduction) or 8 (5 with the phase-A stencil on r)
+// and a tile height
 static const void* uniform_kernel(int sched, int rows) {
     switch (sched) {
         case 0: return uniform_kernel_rs<0>(rows);
         case 1: return uniform_kernel_rs<1>(rows);
         case 4: return uniform_kernel_rs<2>(rows);
+        case 8: return uniform_kernel_rs<3, true>(rows);
         default: return uniform_kernel_rs<3>(rows);
     }
 }
@@ -867,8 +869,9 @@ struct qed2d_batch {
     int* d_cnt = nullptr;           // [nrep + 1]: per-replica counters, then the flag accumulator
     bool shared_state = false;      // records in shared memory (nrep <= kSharedReps)
     bool uniform = false;           // equal sizes, nrep <= kUniformReps: k_u_cg_mixed
-    int usched = -1;                // its schedule: 0, 1 (grid reductions), 4 (independent replicas); -1 untuned
-    int rsched = -1;                // uneven batches: 2 grid solver, 3 one cluster per replica (-1: not tuned)
+    int usched = -1;                // its schedule: 0, 1 (grid reductions), 4, 5, 8 (independent replicas); -1 untuned
+    int rsched = -1;                // uneven batches: 2 grid solver, 3 one cluster per replica, 6 the same with
+                                    // the first phase's stencil on r (-1: not tuned)
     int rcs = 8;                    // blocks per cluster of the cluster solver (tuned)
     int* d_order = nullptr;         // [nrep] replicas by decreasing size (cluster solver)
     // k_u_cg_mixed geometry per tile height (kUTileRows): tiles per replica,
@@ -957,12 +960,16 @@ int r_pack(qed2d_batch* h, double2* U, const double* mom, double eps, float4* U3
 // two replicas up (schedule 1 -> 4 per iteration: 2 x 512^2 23.1 -> 20.2 us,
 // 4 x 512^2 39.1 -> 30.8 us, 32 x 64^2 28.8 -> 9.8 us; 4 -> 5: 16 x 128^2
 // 11.9 -> 11.3 us, 8 x 256^2 16.9 -> 16.6 us, 4 x 512^2 within 4% either way
-// over runs), every block sums for one; tiles of 16 rows for replicas of 2^18
+// over runs), every block sums for one; with the phase-A stencil on r
+// (schedule 8) while the batch's FP32 working set stays in L2 (at most 2^20
+// sites: 4 x 512^2 26.5 -> 24.5 us per iteration, same iteration counts), where
+// its three fewer float4 loads per site count; beyond, phase A's extra read of
+// t_old (16 B per site from DRAM) does; tiles of 16 rows for replicas of 2^18
 // sites and more (the tuner's choice at 4 x 512^2), else 8.
 template <class Launch>
 int tune_uniform(qed2d_batch* h, const UCGP& Q, int maxiter, Launch launch) {
     if (!tuning_enabled()) {
-        h->usched = h->nrep >= 2 ? 5 : 1;
+        h->usched = h->nrep >= 2 ? (h->Vtot <= (1LL << 20) ? 8 : 5) : 1;
         if (!h->utile_fixed) {
             h->utile = 0;
             if (h->Vtot / h->nrep >= (1LL << 18))
@@ -986,8 +993,8 @@ int tune_uniform(qed2d_batch* h, const UCGP& Q, int maxiter, Launch launch) {
     // (schedule 7, the TMA-staged solver, is not a candidate: it gives the same
     // bits as 5 and measured slower everywhere, e.g. 4 x 512^2 28.1 -> 33.5 us per
     // iteration; callers can select it)
-    constexpr int scheds[4] = {0, 1, 4, 5};
-    const int nsched = h->nrep >= 2 ? 4 : 2;
+    constexpr int scheds[5] = {0, 1, 4, 5, 8};
+    const int nsched = h->nrep >= 2 ? 5 : 2;
     const int t_lo = h->utile_fixed ? h->utile : 0, t_hi = h->utile_fixed ? h->utile + 1 : h->nuv;
     std::vector<std::pair<int, int>> cand;
     for (int t = t_lo; t < t_hi; t++)
@@ -1041,11 +1048,16 @@ static bool cluster_fits(int cs, const void* kern) {
     return true;
 }
 
-static const void* replica_cluster_kernel(int cs) {
+static const void* replica_cluster_kernel(int cs, bool rsten = false) {
+    if (rsten)
+        return cs == 4    ? (const void*)k_rc_cg_mixed<4, true>
+               : cs == 16 ? (const void*)k_rc_cg_mixed<16, true>
+                          : (const void*)k_rc_cg_mixed<8, true>;
     return cs == 4 ? (const void*)k_rc_cg_mixed<4> : cs == 16 ? (const void*)k_rc_cg_mixed<16> : (const void*)k_rc_cg_mixed<8>;
 }
 
-int launch_replica_clusters(qed2d_batch* h, const CCGP& cc, int cs) {
+// rsten: the first phase's stencil on r (schedule 6)
+int launch_replica_clusters(qed2d_batch* h, const CCGP& cc, int cs, bool rsten) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(h->nrep * cs));
     cfg.blockDim = dim3(TILE);
@@ -1057,9 +1069,15 @@ int launch_replica_clusters(qed2d_batch* h, const CCGP& cc, int cs) {
     at[0].val.clusterDim.z = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    if (cs == 4) QCHECK(cudaLaunchKernelEx(&cfg, k_rc_cg_mixed<4>, cc));
-    else if (cs == 16) QCHECK(cudaLaunchKernelEx(&cfg, k_rc_cg_mixed<16>, cc));
-    else QCHECK(cudaLaunchKernelEx(&cfg, k_rc_cg_mixed<8>, cc));
+    if (rsten) {
+        if (cs == 4) QCHECK(cudaLaunchKernelEx(&cfg, k_rc_cg_mixed<4, true>, cc));
+        else if (cs == 16) QCHECK(cudaLaunchKernelEx(&cfg, k_rc_cg_mixed<16, true>, cc));
+        else QCHECK(cudaLaunchKernelEx(&cfg, k_rc_cg_mixed<8, true>, cc));
+    } else {
+        if (cs == 4) QCHECK(cudaLaunchKernelEx(&cfg, k_rc_cg_mixed<4>, cc));
+        else if (cs == 16) QCHECK(cudaLaunchKernelEx(&cfg, k_rc_cg_mixed<16>, cc));
+        else QCHECK(cudaLaunchKernelEx(&cfg, k_rc_cg_mixed<8>, cc));
+    }
     return QED2D_OK;
 }
 
@@ -1072,16 +1090,21 @@ int launch_replica_clusters(qed2d_batch* h, const CCGP& cc, int cs) {
 // 8..96 x 4..40 sites 1.83 -> 0.49 ms, 32 of 32^2..128^2 4.30 -> 1.40 ms, 128 of
 // 32^2..256^2 19.7 -> 11.9 ms, the 512-replica ensemble 46.1 -> 30.3 ms), else
 // the grid solver.  The solvers group their sums differently (same accuracy, not
-// the same bits).
+// the same bits).  The cluster solver runs in two forms, both candidates: the
+// plain phase A (schedule 3) and the stencil on r (schedule 6, as schedule 8 of
+// the equal-size solver; results agree to the solver's accuracy).
 template <class Launch>
 int tune_ragged(qed2d_batch* h, const RCGP& P, const CCGP& C, int maxiter, Launch launch) {
     h->rsched = 2;
-    std::vector<int> cand = {0};   // 0: grid solver; cs > 0: clusters of cs blocks
+    std::vector<std::pair<int, int>> cand = {{2, 0}};   // (schedule, blocks per cluster)
     for (int cs : kClusterSizes)
-        if (cluster_fits(cs, replica_cluster_kernel(cs))) cand.push_back(cs);
+        if (cluster_fits(cs, replica_cluster_kernel(cs))) {
+            cand.push_back({3, cs});
+            if (cluster_fits(cs, replica_cluster_kernel(cs, true))) cand.push_back({6, cs});
+        }
     if (!tuning_enabled()) {
-        for (int cs : cand)
-            if (cs == 8) {
+        for (const auto& c : cand)
+            if (c.first == 3 && c.second == 8) {
                 h->rsched = 3;
                 h->rcs = 8;
             }
@@ -1105,7 +1128,7 @@ int tune_ragged(qed2d_batch* h, const RCGP& P, const CCGP& C, int maxiter, Launc
     for (int rep = 0; rep < 3 && st == QED2D_OK; rep++)
         for (size_t c = 0; c < cand.size() && st == QED2D_OK; c++) {
             cudaEventRecord(e0, h->stream);
-            st = cand[c] ? launch(3, TP, TC, cand[c]) : launch(2, TP, TC, 0);
+            st = launch(cand[c].first, TP, TC, cand[c].second);
             cudaEventRecord(e1, h->stream);
             if (cudaEventSynchronize(e1) != cudaSuccess) st = cuda_status(cudaGetLastError(), "schedule tuning");
             float ms = 0.f;
@@ -1120,10 +1143,8 @@ int tune_ragged(qed2d_batch* h, const RCGP& P, const CCGP& C, int maxiter, Launc
     size_t best = 0;
     for (size_t c = 1; c < cand.size(); c++)
         if (tbest[c] < tbest[best]) best = c;
-    if (cand[best]) {
-        h->rsched = 3;
-        h->rcs = cand[best];
-    }
+    h->rsched = cand[best].first;
+    if (cand[best].second) h->rcs = cand[best].second;
     return QED2D_OK;
 }
 
@@ -1250,8 +1271,8 @@ int r_solve(qed2d_batch* h, const double2* U, const float4* U32, const double2* 
         C.maxiter = maxiter;
         C.st_out = h->d_st;
         auto launch = [&](int sched, const RCGP& p, const CCGP& cc, int cs) -> int {
-            if (sched == 3) {
-                QTRY(launch_replica_clusters(h, cc, cs));
+            if (sched == 3 || sched == 6) {
+                QTRY(launch_replica_clusters(h, cc, cs, sched == 6));
             } else {
                 QCHECK(cudaMemsetAsync(&h->ctl->bar, 0, 2 * sizeof(unsigned long long) + sizeof(int), h->stream));
                 QCHECK(cudaMemsetAsync(h->d_cnt, 0, sizeof(int) * (h->nrep + 1), h->stream));   // counters at zero
@@ -1535,10 +1556,11 @@ int qed2d_batch_set_stream(qed2d_batch* h, void* stream) {
 
 int qed2d_batch_set_schedule(qed2d_batch* h, int schedule) {
     const bool ok = h && (schedule == -1 || (h->uniform ? (schedule == 0 || schedule == 1 || schedule == 4 ||
-                                                          schedule == 5 || schedule == 7)
-                                                         : (schedule == 2 || schedule == 3)));
+                                                          schedule == 5 || schedule == 7 || schedule == 8)
+                                                         : (schedule == 2 || schedule == 3 || schedule == 6)));
     if (!ok) {
-        set_error("qed2d_batch_set_schedule: -1, or 0/1/4/5/7 (equal sizes, at most 64 replicas), or 2/3 (otherwise)");
+        set_error(
+            "qed2d_batch_set_schedule: -1, or 0/1/4/5/7/8 (equal sizes, at most 64 replicas), or 2/3/6 (otherwise)");
         return QED2D_ERR_BAD_ARG;
     }
     if (h->uniform) h->usched = schedule;

@@ -68,7 +68,9 @@ __device__ __forceinline__ void cluster_step(RepState* S, int kind, double s, in
     __syncthreads();
 }
 
-template <int CS>
+// RSTEN: the first phase's stencil on r, t = g5Dw r + beta t_old (as schedule 8
+// of the equal-size solver)
+template <int CS, bool RSTEN = false>
 __device__ __forceinline__ void c_body(const CCGP& P, int r, int& k, double* smem, double* s_slot, RepState* S) {
     namespace cgr = cooperative_groups;
     const int rank = (int)cgr::this_cluster().block_rank();
@@ -126,13 +128,32 @@ __device__ __forceinline__ void c_body(const CCGP& P, int r, int& k, double* sme
         {   // p = r + beta p_old, t = g5Dw p, <p, A p> = |t|^2
             float f = 0.f;
             const RepState st = *S;
-            const SpAxpy<float, SpF> Q{SpF{r32}, SpF{qo}, (float)st.beta, !st.first};
-            FOR_MY_CTILES(q) {
-                const Pair<float> c = Q.ld(q.x);
-                const Pair<float> tt = g5dw_at_c<float>(Q, c, Lf, q, m2f);
-                st_f(qn, q.x, c);
-                st_f(t32, q.x, tt);
-                f += norm2(tt.a) + norm2(tt.b);
+            if constexpr (RSTEN) {
+                const float beta = (float)st.beta;
+                const bool use_p = !st.first;
+                FOR_MY_CTILES(q) {
+                    const Pair<float> rc = SpF{r32}.ld(q.x);
+                    Pair<float> tt = g5dw_at_c<float>(SpF{r32}, rc, Lf, q, m2f), c = rc;
+                    if (use_p) {   // p = r + beta p_old, t = g5Dw r + beta t_old
+                        const Pair<float> po = SpF{qo}.ld(q.x), to = SpF{t32}.ld(q.x);
+                        c.a = c.a + beta * po.a;
+                        c.b = c.b + beta * po.b;
+                        tt.a = tt.a + beta * to.a;
+                        tt.b = tt.b + beta * to.b;
+                    }
+                    st_f(qn, q.x, c);
+                    st_f(t32, q.x, tt);
+                    f += norm2(tt.a) + norm2(tt.b);
+                }
+            } else {
+                const SpAxpy<float, SpF> Q{SpF{r32}, SpF{qo}, (float)st.beta, !st.first};
+                FOR_MY_CTILES(q) {
+                    const Pair<float> c = Q.ld(q.x);
+                    const Pair<float> tt = g5dw_at_c<float>(Q, c, Lf, q, m2f);
+                    st_f(qn, q.x, c);
+                    st_f(t32, q.x, tt);
+                    f += norm2(tt.a) + norm2(tt.b);
+                }
             }
             cluster_step(S, RED_PAP, cluster_sum<CS>((double)f, smem, s_slot, nred), k, P);
         }
@@ -213,7 +234,7 @@ __device__ __forceinline__ void c_body(const CCGP& P, int r, int& k, double* sme
 #undef FOR_MY_CTILES
 }
 
-template <int CS>
+template <int CS, bool RSTEN = false>
 __global__ void __launch_bounds__(TILE, 4) k_rc_cg_mixed(const CCGP P) {
     namespace cgr = cooperative_groups;
     __shared__ double smem[32];
@@ -221,7 +242,7 @@ __global__ void __launch_bounds__(TILE, 4) k_rc_cg_mixed(const CCGP P) {
     __shared__ RepState s_st;
     const int r = P.order[blockIdx.x / CS];
     int k = 0;
-    c_body<CS>(P, r, k, smem, s_slot, &s_st);
+    c_body<CS, RSTEN>(P, r, k, smem, s_slot, &s_st);
     if (cgr::this_cluster().block_rank() == 0 && threadIdx.x == 0) P.st_out[r] = s_st;
     cgr::this_cluster().sync();   // no block leaves while another may still read its slots
 }

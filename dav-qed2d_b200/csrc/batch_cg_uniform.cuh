@@ -304,7 +304,14 @@ __device__ __forceinline__ void tma_issue(const UTma& T, const UGeom& g, char* s
 // TMA: the stencil operands of phases A and B come through shared memory
 // (T: the tensor maps; stg: kTmaStages stages; bar: their mbarriers), staged up
 // to kTmaStages - 1 tiles ahead.
-template <int RS, int TYv, bool TMA = false>
+// RSTEN (schedule 8): phase A applies the stencil to r instead of p, t = g5Dw r
+// + beta t_old (g5Dw is linear, so t = g5Dw p as before), and forms p only at
+// the thread's own site: 7 float4 loads per site instead of 10 and no p at the
+// four neighbours.  Same recurrences; t carries the rounding of its own
+// recurrence (the Chronopoulos-Gear form of the direction update), so the bits
+// differ from the other schedules while the FP64 stop rule is unchanged.  After
+// a reliable update the rescaled beta of RED_R4 keeps t = g5Dw p, as it keeps p.
+template <int RS, int TYv, bool TMA = false, bool RSTEN = false>
 __device__ __forceinline__ bool u_body(const UCGP& P, const UTma* T, char* stg, uint64_t* bar, GridSync& gs, int& k,
                                        double* smem, RepState* s_st, int* s_fl) {
     const int myr = blockIdx.x / P.bpr, lb = blockIdx.x - myr * P.bpr;
@@ -435,6 +442,23 @@ __device__ __forceinline__ bool u_body(const UCGP& P, const UTma* T, char* stg, 
                     });
                     if (!ok) return false;
                 }
+            } else if (RSTEN && st.act) {
+                const float beta = (float)st.beta;
+                const bool use_p = !st.first;
+                FOR_MY_UTILES(q) {
+                    const Pair<float> rc = SpF{P.r32}.ld(q.x);
+                    Pair<float> tt = g5dw_at_c<float>(SpF{P.r32}, rc, Lf, q, m2f), c = rc;
+                    if (use_p) {   // p = r + beta p_old, t = g5Dw r + beta t_old
+                        const Pair<float> po = SpF{qo}.ld(q.x), to = SpF{P.t32}.ld(q.x);
+                        c.a = c.a + beta * po.a;
+                        c.b = c.b + beta * po.b;
+                        tt.a = tt.a + beta * to.a;
+                        tt.b = tt.b + beta * to.b;
+                    }
+                    st_f(qn, q.x, c);
+                    st_f(P.t32, q.x, tt);
+                    f += norm2(tt.a) + norm2(tt.b);
+                }
             } else if (st.act) {
                 const SpAxpy<float, SpF> Q{SpF{P.r32}, SpF{qo}, (float)st.beta, !st.first};
                 FOR_MY_UTILES(q) {
@@ -562,7 +586,7 @@ __device__ __forceinline__ bool u_body(const UCGP& P, const UTma* T, char* stg, 
 // barriers) and how many tiles each block walks; the register budget (64 per
 // thread) is the same for all three.  Different heights group the partial sums
 // differently, so they agree to rounding, not bit for bit.
-template <int RS, int TYv>
+template <int RS, int TYv, bool RSTEN = false>
 __global__ void __launch_bounds__(32 * TYv, 32 / TYv) k_u_cg_mixed(const UCGP P) {
     __shared__ double smem[32];
     __shared__ RepState s_st[kUniformReps];
@@ -573,7 +597,7 @@ __global__ void __launch_bounds__(32 * TYv, 32 / TYv) k_u_cg_mixed(const UCGP P)
     if constexpr (RS >= 2) {   // independent replicas: a barrier per replica; its blocks leave when it is done
         const int myr = blockIdx.x / P.bpr;
         GridSync gs{P.rbar + 16 * myr, &P.ctl->gen, &P.ctl->err, (unsigned)P.bpr};
-        const bool ok = u_body<RS, TYv>(P, nullptr, nullptr, nullptr, gs, k, smem, s_st, s_fl);
+        const bool ok = u_body<RS, TYv, false, RSTEN>(P, nullptr, nullptr, nullptr, gs, k, smem, s_st, s_fl);
         if (blockIdx.x == myr * P.bpr && threadIdx.x == 0) {   // the replica's first block
             if (ok) P.st_out[myr] = s_st[myr];
             DevCtl* c = P.ctl;

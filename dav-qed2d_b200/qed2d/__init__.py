@@ -787,8 +787,11 @@ class Batch:
         most 64 replicas 0/1 (reduction schedules), 4 (independent replicas, a
         barrier per replica), 5 (the same with a leaner reduction) or 7 (5 with
         the stencil operands staged by TMA; replicas of whole 32 x 8 or 32 x 16
-        tiles), all with the same bits; other batches 2 (one launch with grid
-        barriers) or 3 (one thread-block cluster per replica)."""
+        tiles), all with the same bits, or 8 (5 with the first phase's stencil
+        applied to r, t = g5Dw r + beta t_old; agrees with 5 to solver
+        accuracy); other batches 2 (one launch with grid barriers), 3 (one
+        thread-block cluster per replica) or 6 (3 with the first phase's stencil
+        on r)."""
         v = C.c_int(0)
         check(lib().qed2d_batch_get_schedule(self.h, C.byref(v)), "batch_get_schedule")
         return v.value

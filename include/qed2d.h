@@ -333,9 +333,15 @@ int qed2d_batch_set_stream(qed2d_batch* batch, void* cuda_stream);
  * seven), 7 = schedule 5 with the stencil operands of each tile staged into
  * shared memory by TMA one tile ahead (replicas of whole tiles only: L1 a
  * multiple of 32, L2 of the tile height 8 or 16; QED2D_ERR_UNSUPPORTED
- * otherwise); 0, 1, 4, 5 and 7 give the same bits.  Other batches: 2 = one launch over all replicas with grid
+ * otherwise); 0, 1, 4, 5 and 7 give the same bits.  8 = schedule 5 with the
+ * first phase's stencil applied to r (t = g5Dw r + beta t_old; p formed at the
+ * site only): the same recurrences with t rounded along its own recurrence, so
+ * results agree with 5 to the solver's accuracy (FP64 stop rule unchanged);
+ * faster where the FP32 working set stays in L2 (4 x 512^2: 26.5 -> 24.5 us per
+ * iteration).  Other batches: 2 = one launch over all replicas with grid
  * barriers, 3 = one thread-block cluster per replica (no grid barrier; replicas
- * stream through the GPU, largest first); these group their sums differently.
+ * stream through the GPU, largest first), 6 = 3 with the first phase's stencil
+ * on r (as 8); these group their sums differently.
  * The first solve times the candidates and keeps the fastest; -1 = tune again
  * on the next solve (get: -1 while untuned). */
 int qed2d_batch_set_schedule(qed2d_batch* batch, int schedule);

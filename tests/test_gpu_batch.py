@@ -198,7 +198,7 @@ def test_batch_reduction_schedules_give_identical_bits():
         src[r] = to_dev(cgauss(L1, L2, 50 + r, 2))
     x = b.field()
     b.cg(x, U, src, [0.2, 0.3, 0.25], 20000, 1e-24)
-    assert b.schedule in (0, 1, 4, 5)
+    assert b.schedule in (0, 1, 4, 5, 8)
     res = []
     for sched in (0, 1, 4, 5):
         b.schedule = sched
@@ -229,7 +229,7 @@ def test_batch_tile_heights(L1, L2):
         src[r] = to_dev(cgauss(L1, L2, 150 + r, 2))
     am0 = [0.2, 0.3, 0.25]
     b.cg(b.field(), U, src, am0, 20000, 1e-24)
-    assert b.tile_rows in (4, 8, 16) and b.schedule in (0, 1, 4, 5)
+    assert b.tile_rows in (4, 8, 16) and b.schedule in (0, 1, 4, 5, 8)
     res = {}
     for rows in (8, 4, 16):
         b.tile_rows = rows
@@ -255,9 +255,10 @@ def test_batch_tile_heights(L1, L2):
 @pytest.mark.parametrize("nrep", [6, 80])
 def test_ragged_cluster_solver_matches_grid_solver(nrep):
     """Uneven batches have two solvers: one launch over all replicas with grid
-    barriers (schedule 2) and one thread-block cluster per replica (schedule 3).
-    They group their sums differently: solutions agree to 1e-9 relative and with
-    the single-lattice solve; the first solve tunes the choice."""
+    barriers (schedule 2) and one thread-block cluster per replica (schedule 3;
+    schedule 6 is 3 with the first phase's stencil on r).  They group their sums
+    differently: solutions agree to the solver's accuracy and with the
+    single-lattice solve; the first solve tunes the choice."""
     import qed2d
     rng = np.random.default_rng(123 + nrep)
     sizes = [(int(a), int(b)) for a, b in zip(rng.choice([8, 16, 33, 64, 96], nrep), rng.choice([4, 8, 17, 40], nrep))]
@@ -269,9 +270,9 @@ def test_ragged_cluster_solver_matches_grid_solver(nrep):
         b.replica(src, r).copy_(to_dev(cgauss(l1, l2, 90 + r, 2)))
     x = b.field()
     b.cg(x, U, src, am0s, 20000, 1e-24)
-    assert b.schedule in (2, 3)
+    assert b.schedule in (2, 3, 6)
     res = {}
-    for sched in (2, 3):
+    for sched in (2, 3, 6):
         b.schedule = sched
         x = b.field()
         its, upd = b.cg(x, U, src, am0s, 20000, 1e-24)
@@ -280,8 +281,10 @@ def test_ragged_cluster_solver_matches_grid_solver(nrep):
         b.cg(x2, U, src, am0s, 20000, 1e-24)
         assert np.array_equal(to_host(x2), res[sched][1])   # each solver is deterministic
     bound("cluster-per-replica vs grid solver", rel(res[3][1], res[2][1]), 2e-12)
+    bound("cluster-per-replica, stencil on r, vs grid solver", rel(res[6][1], res[2][1]), 2e-12)
     for r in range(nrep):
         bound("cluster-per-replica vs grid iterations", abs(res[3][0][r] - res[2][0][r]), 2)  # r
+        bound("cluster-per-replica, stencil on r, vs grid iterations", abs(res[6][0][r] - res[2][0][r]), 2)  # r
     qed2d.set_precision("mixed")
     for r in (0, nrep - 1):
         l1, l2 = sizes[r]
@@ -409,7 +412,7 @@ def test_capped_solves_agree_across_solvers(maxiter):
     Ub, bb = bt.field(), bt.field()
     for r in range(2):
         Ub[r], bb[r] = U, b
-    for sched in (1, 4, 5):
+    for sched in (1, 4, 5, 8):
         bt.schedule = sched
         x = bt.field()
         capped(lambda: bt.cg(x, Ub, bb, [am0, am0], maxiter, 1e-24))
@@ -421,8 +424,70 @@ def test_capped_solves_agree_across_solvers(maxiter):
     rb.replica(br, 0).copy_(b)
     rb.replica(Ur, 1).copy_(to_dev(hot_links(32, 32, 83)))
     rb.replica(br, 1).copy_(to_dev(cgauss(32, 32, 84, 2)))
-    for sched in (2, 3):
+    for sched in (2, 3, 6):
         rb.schedule = sched
         x = rb.field()
         capped(lambda: rb.cg(x, Ur, br, [am0, am0], maxiter, 1e-24))
         bound("capped ragged solve vs single-lattice", rel(to_host(rb.replica(x, 0)), ref[2]), 1e-6)  # sched
+
+
+@pytest.mark.parametrize("L1,L2,rows", [(64, 48, 8), (100, 37, 16), (96, 40, 4)])
+def test_rstencil_schedule_matches_lean(L1, L2, rows):
+    """Batch schedule 8 (phase A applies the stencil to r and carries t = g5Dw r +
+    beta t_old) runs the same CG recurrences as schedule 5 with t rounded along
+    its own recurrence: both stop on the same FP64 true residual, so solutions
+    agree to the solver's accuracy and iteration counts within 5%."""
+    import qed2d
+    nrep = 3
+    b = qed2d.Batch(nrep, L1, L2, 4.0)
+    U, src = b.field(), b.field()
+    for r in range(nrep):
+        U[r] = to_dev(hot_links(L1, L2, 240 + r))
+        src[r] = to_dev(cgauss(L1, L2, 250 + r, 2))
+    am0 = [0.2, 0.3, 0.25]
+    b.tile_rows = rows
+    res = {}
+    for sched in (5, 8):
+        b.schedule = sched
+        x = b.field()
+        its, upd = b.cg(x, U, src, am0, 20000, 1e-24)
+        res[sched] = (list(its), to_host(x))
+    bound("schedule 8 vs schedule 5 solution rel", rel(res[8][1], res[5][1]), 1e-11)
+    for r in range(nrep):
+        assert abs(res[8][0][r] - res[5][0][r]) <= max(3, res[5][0][r] // 20), (r, res[8][0], res[5][0])
+    # the solution satisfies the reference's stop rule on the FP64 operator
+    prm = qed2d.LattParm((L1, L2), 4.0)
+    for r in range(nrep):
+        ax, tmp = qed2d.cfield(L1, L2), qed2d.cfield(L1, L2)
+        xr = to_dev(res[8][1][r])
+        qed2d.gamm5Dw_sqr_msq(ax, tmp, U[r].contiguous(), xr, am0[r], prm, None)
+        bh = to_host(src[r])
+        rr = np.linalg.norm(to_host(ax) - bh) / np.linalg.norm(bh)
+        bound("schedule 8 true relative residual |b - A x| / |b|", rr, 1.01e-12)
+
+
+def test_rstencil_schedule_trajectories_vs_oracle():
+    """Batched Nf=2 trajectories under schedule 8 against the oracle replaying
+    the same draws (as under the other schedules: links 5e-12 relative, Delta H
+    5e-10 absolute, same accept/reject)."""
+    import qed2d
+    nrep, L1, L2 = 2, 48, 40
+    betas, am0s, seeds = [4.0, 4.0], [0.2, 0.3], [31, 32]
+    b = qed2d.Batch(nrep, L1, L2, betas)
+    b.schedule = 8
+    U0 = [hot_links(L1, L2, 330 + r) for r in range(nrep)]
+    U = b.field()
+    for r in range(nrep):
+        U[r] = to_dev(U0[r])
+    counter = 5
+    infos = b.hmc_nf2(U, am0s, 0.1, 5, 10000, 1e-24, seeds, counter)
+    assert b.schedule == 8
+    for r in range(nrep):
+        o = Oracle(L1, L2, betas[r])
+        mom0 = Oracle.normal(2 * L1 * L2, seeds[r], 1, counter).reshape(2, L2, L1)
+        noise = cgauss(L1, L2, seeds[r], 16, counter)
+        st, Uo, acc, hi, hf, _ = o.hmc_nf2(U0[r], am0s[r], 0.1, 5, 10000, 1e-24, mom0, noise,
+                                            Oracle.uniform(seeds[r], 3, counter))
+        assert st == 0 and acc == infos[r].accepted
+        bound("schedule 8 batch vs oracle dH abs", abs(infos[r].dH - (hf - hi)), 5e-10)
+        bound("schedule 8 batch vs oracle links", rel(to_host(U[r]), Uo), 5e-12)
