@@ -492,7 +492,9 @@ def run_ours(args):
                              4: "independent replicas (a barrier per replica)",
                              5: "independent replicas, lean reduction",
                              7: "independent replicas, lean reduction, TMA-staged stencil operands",
-                             8: "independent replicas, lean reduction, phase-A stencil on r"}.get(
+                             8: "independent replicas, lean reduction, phase-A stencil on r",
+                             9: "independent replicas, lean reduction, phase-A stencil on r, links in shared "
+                                "memory"}.get(
                                  batch.schedule, "untuned"),
                 "tile_rows": batch.tile_rows,
                 "note": f"one launch = one solve of all {B} replicas: per replica iterations {min(its)}-{max(its)} "

@@ -774,11 +774,15 @@ namespace qed2d {
 // the first is the default when the tuner is off
 constexpr int kUTileRows[3] = {8, 16, 4};
 
-template <int RS, bool RSTEN = false>
+template <int RS, bool RSTEN = false, bool LSM = false>
 static const void* uniform_kernel_rs(int rows) {
-    return rows == 4    ? (const void*)k_u_cg_mixed<RS, 4, RSTEN>
-           : rows == 16 ? (const void*)k_u_cg_mixed<RS, 16, RSTEN>
-                        : (const void*)k_u_cg_mixed<RS, 8, RSTEN>;
+    return rows == 4    ? (const void*)k_u_cg_mixed<RS, 4, RSTEN, LSM>
+           : rows == 16 ? (const void*)k_u_cg_mixed<RS, 16, RSTEN, LSM>
+                        : (const void*)k_u_cg_mixed<RS, 8, RSTEN, LSM>;
+}
+// shared memory of schedule 9's staged links for a tile height and tiles per block
+static size_t uniform_lsm_bytes(int rows, int per_block) {
+    return rows == 4 ? ULsm<4>::bytes(per_block) : rows == 16 ? ULsm<16>::bytes(per_block) : ULsm<8>::bytes(per_block);
 }
 
 // host: cuTensorMapEncodeTiled through the runtime's driver entry point
@@ -828,14 +832,15 @@ static size_t uniform_tma_smem(int rows) {
 }
 
 // the equal-size solver for schedule 0/1 (grid reductions), 4 (a barrier per
-// replica), 5 (the same, lean reduction) or 8 (5 with the phase-A stencil on r)
-// and a tile height
+// replica), 5 (the same, lean reduction), 8 (5 with the phase-A stencil on r) or
+// 9 (8 with the links staged in shared memory) and a tile height
 static const void* uniform_kernel(int sched, int rows) {
     switch (sched) {
         case 0: return uniform_kernel_rs<0>(rows);
         case 1: return uniform_kernel_rs<1>(rows);
         case 4: return uniform_kernel_rs<2>(rows);
         case 8: return uniform_kernel_rs<3, true>(rows);
+        case 9: return uniform_kernel_rs<3, true, true>(rows);
         default: return uniform_kernel_rs<3>(rows);
     }
 }
@@ -880,10 +885,12 @@ struct qed2d_batch {
         int rows = 0, per_block = 0, bpr = 0, grid = 0;
         long long ntr = 0;
         bool tma = false;   // schedule 7 possible: whole tiles, an instance, co-resident with its shared memory
+        size_t lsm = 0;     // schedule 9's dynamic shared memory; 0: not co-resident with it
     } uv[3];
     int nuv = 0;                    // heights whose kernels fit (co-resident grid)
     int utile = -1;                 // index into uv of the tile height in use; -1 untuned
     bool utile_fixed = false;       // set by qed2d_batch_set_tile_rows: the tuner keeps it
+    bool usched_fixed = false;      // set by qed2d_batch_set_schedule: the tuner keeps it (tunes the height only)
     UGeom ug{};
     double* d_upart = nullptr;      // [2][max grid over uv]
     double* d_ured = nullptr;       // [2][nrep]
@@ -964,19 +971,45 @@ int r_pack(qed2d_batch* h, double2* U, const double* mom, double eps, float4* U3
 // (schedule 8) while the batch's FP32 working set stays in L2 (at most 2^20
 // sites: 4 x 512^2 26.5 -> 24.5 us per iteration, same iteration counts), where
 // its three fewer float4 loads per site count; beyond, phase A's extra read of
-// t_old (16 B per site from DRAM) does; tiles of 16 rows for replicas of 2^18
+// t_old (16 B per site from DRAM) does; and with the links staged in shared
+// memory (schedule 9) where they fit beside co-resident blocks (4 x 512^2
+// 27.4 -> 25.3 us per iteration; the tuner picked 9 at every equal-size batch
+// measured from 32 x 64^2 to 4 x 512^2); tiles of 16 rows for replicas of 2^18
 // sites and more (the tuner's choice at 4 x 512^2), else 8.
 template <class Launch>
 int tune_uniform(qed2d_batch* h, const UCGP& Q, int maxiter, Launch launch) {
     if (!tuning_enabled()) {
-        h->usched = h->nrep >= 2 ? (h->Vtot <= (1LL << 20) ? 8 : 5) : 1;
         if (!h->utile_fixed) {
             h->utile = 0;
             if (h->Vtot / h->nrep >= (1LL << 18))
                 for (int t = 0; t < h->nuv; t++)
                     if (h->uv[t].rows == 16) h->utile = t;
         }
+        if (!h->usched_fixed)
+            h->usched = h->nrep >= 2 ? (h->Vtot <= (1LL << 20) ? (h->uv[h->utile].lsm ? 9 : 8) : 5) : 1;
         return QED2D_OK;
+    }
+    // candidates: (schedule, tile height); the height only when it is not fixed,
+    // the schedule only when the caller has not fixed it
+    // (schedule 7, the TMA-staged solver, is not a candidate: it gives the same
+    // bits as 5 and measured slower everywhere, e.g. 4 x 512^2 28.1 -> 33.5 us per
+    // iteration; callers can select it)
+    constexpr int scheds[6] = {0, 1, 4, 5, 8, 9};
+    const int nsched = h->nrep >= 2 ? 6 : 2;
+    const int t_lo = h->utile_fixed ? h->utile : 0, t_hi = h->utile_fixed ? h->utile + 1 : h->nuv;
+    auto fits = [&](int s, int t) { return (s != 9 || h->uv[t].lsm) && (s != 7 || h->uv[t].tma); };
+    std::vector<std::pair<int, int>> cand;
+    for (int t = t_lo; t < t_hi; t++) {
+        if (h->usched_fixed) {
+            if (fits(h->usched, t)) cand.push_back({h->usched, t});
+            continue;
+        }
+        for (int rs = 0; rs < nsched; rs++)
+            if (fits(scheds[rs], t)) cand.push_back({scheds[rs], t});
+    }
+    if (cand.empty()) {
+        set_error("batch schedule " + std::to_string(h->usched) + ": no tile height fits it");
+        return QED2D_ERR_UNSUPPORTED;
     }
     DevCtl saved;
     QCHECK(cudaMemcpyAsync(&saved, h->ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, h->stream));
@@ -989,16 +1022,6 @@ int tune_uniform(qed2d_batch* h, const UCGP& Q, int maxiter, Launch launch) {
     cudaEvent_t e0, e1;
     QCHECK(cudaEventCreate(&e0));
     QCHECK(cudaEventCreate(&e1));
-    // candidates: (schedule, tile height); the height only when it is not fixed
-    // (schedule 7, the TMA-staged solver, is not a candidate: it gives the same
-    // bits as 5 and measured slower everywhere, e.g. 4 x 512^2 28.1 -> 33.5 us per
-    // iteration; callers can select it)
-    constexpr int scheds[5] = {0, 1, 4, 5, 8};
-    const int nsched = h->nrep >= 2 ? 5 : 2;
-    const int t_lo = h->utile_fixed ? h->utile : 0, t_hi = h->utile_fixed ? h->utile + 1 : h->nuv;
-    std::vector<std::pair<int, int>> cand;
-    for (int t = t_lo; t < t_hi; t++)
-        for (int rs = 0; rs < nsched; rs++) cand.push_back({scheds[rs], t});
     std::vector<float> tbest(cand.size(), 1e30f);
     int st = QED2D_OK;
     for (int rep = 0; rep < 3 && st == QED2D_OK; rep++)
@@ -1238,9 +1261,14 @@ int r_solve(qed2d_batch* h, const double2* U, const float4* U32, const double2* 
                 count_launch();
                 return QED2D_OK;
             }
+            if (sched == 9 && !v.lsm) {
+                set_error("batch schedule 9: the staged links do not fit co-resident at this tile height");
+                return QED2D_ERR_UNSUPPORTED;
+            }
             void* uargs[] = {(void*)&q};
             QCHECK(cudaLaunchCooperativeKernel(uniform_kernel(sched, v.rows), dim3((unsigned)v.grid),
-                                               dim3((unsigned)(TX * v.rows)), uargs, 0, h->stream));
+                                               dim3((unsigned)(TX * v.rows)), uargs, sched == 9 ? v.lsm : 0,
+                                               h->stream));
             count_launch();
             return QED2D_OK;
         };
@@ -1390,7 +1418,7 @@ int batch_setup(qed2d_batch* h, const int* L1, const int* L2, const double* beta
         const RepInfo& R0 = h->reps[0];
         for (int rows : kUTileRows) {
             int per_smu = 1 << 30;
-            for (int sched : {0, 1, 4, 5}) {
+            for (int sched : {0, 1, 4, 5, 8}) {
                 int n = 0;
                 QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, uniform_kernel(sched, rows), TX * rows, 0));
                 per_smu = std::min(per_smu, n);
@@ -1410,6 +1438,23 @@ int batch_setup(qed2d_batch* h, const int* L1, const int* L2, const double* beta
                 if (cudaFuncSetAttribute(kt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) == cudaSuccess &&
                     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n7, kt, TX * rows, sm) == cudaSuccess)
                     v.tma = (long long)n7 * h->num_sms >= v.grid;
+                cudaGetLastError();
+            }
+            {   // schedule 9: the grid stays co-resident with the staged links
+                // (the attribute is set to what the device allows beside the
+                // kernel's static shared memory, so batches of other sizes keep
+                // launching the same kernel)
+                const size_t sm = uniform_lsm_bytes(rows, v.per_block);
+                const void* k9 = uniform_kernel(9, rows);
+                int n9 = 0, optin = 0;
+                cudaFuncAttributes fa{};
+                if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device) == cudaSuccess &&
+                    cudaFuncGetAttributes(&fa, k9) == cudaSuccess && sm + fa.sharedSizeBytes <= (size_t)optin &&
+                    cudaFuncSetAttribute(k9, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         optin - (int)fa.sharedSizeBytes) == cudaSuccess &&
+                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n9, k9, TX * rows, sm) == cudaSuccess &&
+                    (long long)n9 * h->num_sms >= v.grid)
+                    v.lsm = sm;
                 cudaGetLastError();
             }
             h->uv[h->nuv++] = v;
@@ -1556,15 +1601,20 @@ int qed2d_batch_set_stream(qed2d_batch* h, void* stream) {
 
 int qed2d_batch_set_schedule(qed2d_batch* h, int schedule) {
     const bool ok = h && (schedule == -1 || (h->uniform ? (schedule == 0 || schedule == 1 || schedule == 4 ||
-                                                          schedule == 5 || schedule == 7 || schedule == 8)
+                                                          schedule == 5 || schedule == 7 || schedule == 8 ||
+                                                          schedule == 9)
                                                          : (schedule == 2 || schedule == 3 || schedule == 6)));
     if (!ok) {
         set_error(
-            "qed2d_batch_set_schedule: -1, or 0/1/4/5/7/8 (equal sizes, at most 64 replicas), or 2/3/6 (otherwise)");
+            "qed2d_batch_set_schedule: -1, or 0/1/4/5/7/8/9 (equal sizes, at most 64 replicas), or 2/3/6 (otherwise)");
         return QED2D_ERR_BAD_ARG;
     }
-    if (h->uniform) h->usched = schedule;
-    else h->rsched = schedule;
+    if (h->uniform) {
+        h->usched = schedule;
+        h->usched_fixed = schedule >= 0;
+    } else {
+        h->rsched = schedule;
+    }
     return QED2D_OK;
 }
 

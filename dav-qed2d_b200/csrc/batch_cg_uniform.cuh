@@ -311,9 +311,22 @@ __device__ __forceinline__ void tma_issue(const UTma& T, const UGeom& g, char* s
 // recurrence (the Chronopoulos-Gear form of the direction update), so the bits
 // differ from the other schedules while the FP64 stop rule is unchanged.  After
 // a reliable update the rescaled beta of RED_R4 keeps t = g5Dw p, as it keeps p.
-template <int RS, int TYv, bool TMA = false, bool RSTEN = false>
+// FP32 links of the block's tiles staged once per solve in shared memory (LSM,
+// schedule 9 with RSTEN): per tile a box of u1 over the tile's rows and the
+// column left of it (TYv x 33) and a box of u2 over the tile's columns and the
+// row below it ((TYv + 1) x 32), so a site reads u1(x), u1(x - 1), u2(x) and
+// u2(x - 2) from shared memory without a branch.  The links do not change during
+// a solve; the values are those of the global planes, so the bits are those of
+// the same schedule without staging.
+template <int TYv>
+struct ULsm {
+    static constexpr int B1 = TYv * 33, TS = TYv * 33 + (TYv + 1) * 32;   // float2 per tile
+    static __host__ __device__ constexpr size_t bytes(int per_block) { return sizeof(float2) * TS * (size_t)per_block; }
+};
+
+template <int RS, int TYv, bool TMA = false, bool RSTEN = false, bool LSM = false>
 __device__ __forceinline__ bool u_body(const UCGP& P, const UTma* T, char* stg, uint64_t* bar, GridSync& gs, int& k,
-                                       double* smem, RepState* s_st, int* s_fl) {
+                                       double* smem, RepState* s_st, int* s_fl, const float2* lsm = nullptr) {
     const int myr = blockIdx.x / P.bpr, lb = blockIdx.x - myr * P.bpr;
     const TileRange TR = tile_range(P.g.ntr, P.g.nt1, P.per_block, lb);
     const long long V = P.g.V, sh = (long long)myr * V;   // FP64 planes of replica myr: base + sh, stride V
@@ -378,6 +391,29 @@ __device__ __forceinline__ bool u_body(const UCGP& P, const UTma* T, char* stg, 
         return true;
     };
 
+    // the FP32 stencil of spinor accessor S around site q of the block's tile j
+    // (centre value c given), links from shared memory (LSM) or the planes
+    auto sten = [&](const auto& S, const Pair<float>& c, const Site& q, int j) -> Pair<float> {
+        if constexpr (LSM) {
+            const float2* b1 = lsm + j * ULsm<TYv>::TS + ly * 33 + lx;
+            const float2* b2 = lsm + j * ULsm<TYv>::TS + ULsm<TYv>::B1 + ly * 32 + lx;
+            return g5dw_at_cl<float>(S, c, q, b1[1], b2[32], b1[0], b2[0], m2f);
+        } else {
+            return g5dw_at_c<float>(S, c, Lf, q, m2f);
+        }
+    };
+    if constexpr (LSM) {   // stage the links of the block's tiles
+        float2* w = const_cast<float2*>(lsm);
+        FOR_MY_UTILES(q) {
+            float2* b1 = w + (tt_ - TR.lo) * ULsm<TYv>::TS + ly * 33 + lx;
+            float2* b2 = w + (tt_ - TR.lo) * ULsm<TYv>::TS + ULsm<TYv>::B1 + ly * 32 + lx;
+            b1[1] = Lf.u1(q.x);
+            b2[32] = Lf.u2(q.x);
+            if (lx == 0) b1[0] = Lf.u1(q.xm1);
+            if (ly == 0) b2[0] = Lf.u2(q.xm2);
+        }
+        __syncthreads();
+    }
     {   // |b|^2 per replica; x = 0
         double v = 0.0;
         FOR_MY_UTILES(q) {
@@ -447,7 +483,7 @@ __device__ __forceinline__ bool u_body(const UCGP& P, const UTma* T, char* stg, 
                 const bool use_p = !st.first;
                 FOR_MY_UTILES(q) {
                     const Pair<float> rc = SpF{P.r32}.ld(q.x);
-                    Pair<float> tt = g5dw_at_c<float>(SpF{P.r32}, rc, Lf, q, m2f), c = rc;
+                    Pair<float> tt = sten(SpF{P.r32}, rc, q, tt_ - TR.lo), c = rc;
                     if (use_p) {   // p = r + beta p_old, t = g5Dw r + beta t_old
                         const Pair<float> po = SpF{qo}.ld(q.x), to = SpF{P.t32}.ld(q.x);
                         c.a = c.a + beta * po.a;
@@ -463,7 +499,7 @@ __device__ __forceinline__ bool u_body(const UCGP& P, const UTma* T, char* stg, 
                 const SpAxpy<float, SpF> Q{SpF{P.r32}, SpF{qo}, (float)st.beta, !st.first};
                 FOR_MY_UTILES(q) {
                     const Pair<float> c = Q.ld(q.x);
-                    const Pair<float> tt = g5dw_at_c<float>(Q, c, Lf, q, m2f);
+                    const Pair<float> tt = sten(Q, c, q, tt_ - TR.lo);
                     st_f(qn, q.x, c);
                     st_f(P.t32, q.x, tt);
                     f += norm2(tt.a) + norm2(tt.b);
@@ -507,7 +543,7 @@ __device__ __forceinline__ bool u_body(const UCGP& P, const UTma* T, char* stg, 
                 if (pend) {
                     FOR_MY_UTILES(q) {   // x += apend p_old, then x += alpha p
                         const Pair<float> po = SpF{qo}.ld(q.x), pc = SpF{qn}.ld(q.x);
-                        const Pair<float> a = g5dw_at<float>(SpF{P.t32}, Lf, q, m2f);
+                        const Pair<float> a = sten(SpF{P.t32}, SpF{P.t32}.ld(q.x), q, tt_ - TR.lo);
                         Pair<float> xv = SpF{P.x32}.ld(q.x), r = SpF{P.r32}.ld(q.x);
                         xv.a = xv.a + apend * po.a;
                         xv.b = xv.b + apend * po.b;
@@ -521,7 +557,7 @@ __device__ __forceinline__ bool u_body(const UCGP& P, const UTma* T, char* stg, 
                     }
                 } else {
                     FOR_MY_UTILES(q) {   // x's update waits for the next iteration
-                        const Pair<float> a = g5dw_at<float>(SpF{P.t32}, Lf, q, m2f);
+                        const Pair<float> a = sten(SpF{P.t32}, SpF{P.t32}.ld(q.x), q, tt_ - TR.lo);
                         Pair<float> r = SpF{P.r32}.ld(q.x);
                         r.a = r.a - alpha * a.a;
                         r.b = r.b - alpha * a.b;
@@ -586,8 +622,9 @@ __device__ __forceinline__ bool u_body(const UCGP& P, const UTma* T, char* stg, 
 // barriers) and how many tiles each block walks; the register budget (64 per
 // thread) is the same for all three.  Different heights group the partial sums
 // differently, so they agree to rounding, not bit for bit.
-template <int RS, int TYv, bool RSTEN = false>
+template <int RS, int TYv, bool RSTEN = false, bool LSM = false>
 __global__ void __launch_bounds__(32 * TYv, 32 / TYv) k_u_cg_mixed(const UCGP P) {
+    extern __shared__ float2 lsm_dyn[];   // LSM: ULsm<TYv>::bytes(P.per_block)
     __shared__ double smem[32];
     __shared__ RepState s_st[kUniformReps];
     __shared__ int s_fl[FL_N];
@@ -597,7 +634,8 @@ __global__ void __launch_bounds__(32 * TYv, 32 / TYv) k_u_cg_mixed(const UCGP P)
     if constexpr (RS >= 2) {   // independent replicas: a barrier per replica; its blocks leave when it is done
         const int myr = blockIdx.x / P.bpr;
         GridSync gs{P.rbar + 16 * myr, &P.ctl->gen, &P.ctl->err, (unsigned)P.bpr};
-        const bool ok = u_body<RS, TYv, false, RSTEN>(P, nullptr, nullptr, nullptr, gs, k, smem, s_st, s_fl);
+        const bool ok =
+            u_body<RS, TYv, false, RSTEN, LSM>(P, nullptr, nullptr, nullptr, gs, k, smem, s_st, s_fl, lsm_dyn);
         if (blockIdx.x == myr * P.bpr && threadIdx.x == 0) {   // the replica's first block
             if (ok) P.st_out[myr] = s_st[myr];
             DevCtl* c = P.ctl;

@@ -212,6 +212,16 @@ __device__ __forceinline__ Pair<R> g5dw_at_c(const S& s, const Pair<R>& c, const
     return o;
 }
 
+// gamma5 Dw at one site with the centre value and the four links given
+template <typename R, class S, typename LT>
+__device__ __forceinline__ Pair<R> g5dw_at_cl(const S& s, const Pair<R>& c, const Site& q, LT u1x, LT u2x, LT u1m1,
+                                              LT u2m2, R m2) {
+    const Pair<R> p1 = s.ld(q.xp1), m1 = s.ld(q.xm1), p2 = s.ld(q.xp2), mm2 = s.ld(q.xm2);
+    Pair<R> o;
+    g5dw_site<R>(c.a, c.b, p1.a, p1.b, m1.a, m1.b, p2.a, p2.b, mm2.a, mm2.b, u1x, u2x, u1m1, u2m2, m2, o.a, o.b);
+    return o;
+}
+
 // total gauge force on the two links of site y: frc1+frc2 of krnl_force!
 //   F1(y) = -v(y) + v(y-2),  F2(y) = v(y) - v(y-1)
 // The three plaquettes share links: the 10 distinct links are addressed from

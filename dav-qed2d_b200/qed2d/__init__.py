@@ -789,7 +789,8 @@ class Batch:
         the stencil operands staged by TMA; replicas of whole 32 x 8 or 32 x 16
         tiles), all with the same bits, or 8 (5 with the first phase's stencil
         applied to r, t = g5Dw r + beta t_old; agrees with 5 to solver
-        accuracy); other batches 2 (one launch with grid barriers), 3 (one
+        accuracy) or 9 (8 with the links staged in shared memory once per
+        solve; agrees with 8 to rounding); other batches 2 (one launch with grid barriers), 3 (one
         thread-block cluster per replica) or 6 (3 with the first phase's stencil
         on r)."""
         v = C.c_int(0)

@@ -338,12 +338,16 @@ int qed2d_batch_set_stream(qed2d_batch* batch, void* cuda_stream);
  * site only): the same recurrences with t rounded along its own recurrence, so
  * results agree with 5 to the solver's accuracy (FP64 stop rule unchanged);
  * faster where the FP32 working set stays in L2 (4 x 512^2: 26.5 -> 24.5 us per
- * iteration).  Other batches: 2 = one launch over all replicas with grid
+ * iteration).  9 = schedule 8 with the FP32 links of each block's tiles staged
+ * once per solve in shared memory (where they fit beside co-resident blocks;
+ * QED2D_ERR_UNSUPPORTED otherwise); agrees with 8 to rounding.  Other batches:
+ * 2 = one launch over all replicas with grid
  * barriers, 3 = one thread-block cluster per replica (no grid barrier; replicas
  * stream through the GPU, largest first), 6 = 3 with the first phase's stencil
  * on r (as 8); these group their sums differently.
- * The first solve times the candidates and keeps the fastest; -1 = tune again
- * on the next solve (get: -1 while untuned). */
+ * The first solve times the candidates and keeps the fastest; a schedule set
+ * here is kept (for equal sizes the first solve then tunes the tile height
+ * only); -1 = tune again on the next solve (get: -1 while untuned). */
 int qed2d_batch_set_schedule(qed2d_batch* batch, int schedule);
 int qed2d_batch_get_schedule(const qed2d_batch* batch, int* schedule);
 /* Tile height of the equal-size batched solver: tiles of 32 x rows sites, rows =
