@@ -66,12 +66,13 @@ B_ITER_F32 = 256.0
 B_ITER_F64 = 512.0
 # Measured traffic per site-iteration of k_u_cg_mixed at 4 x 512^2, from one ncu
 # capture of a 100-iteration launch of the tuned kernel (independent replicas,
-# lean reduction, phase-A stencil on r, 32 x 16 tiles): DRAM read + write
-# (6.780 GB over 1,048,576 sites x 100) and L1 <-> L2 (17.21 GB read + 6.56 GB
-# written); both grow in proportion to the iterations at fixed size
-U_DRAM_PER_SITE_ITER = 64.7
-U_L2_PER_SITE_ITER = 226.7
-U_L2_THROUGHPUT = 0.373   # lts__throughput.avg.pct_of_peak_sustained_elapsed of the same capture
+# lean reduction, phase-A stencil on r, links staged in shared memory, 32 x 16
+# tiles): DRAM read + write (5.391 GB over 1,048,576 sites x 100) and L1 <-> L2
+# (13.29 GB read + 6.56 GB written); both grow in proportion to the iterations
+# at fixed size
+U_DRAM_PER_SITE_ITER = 51.4
+U_L2_PER_SITE_ITER = 189.3
+U_L2_THROUGHPUT = 0.360   # lts__throughput.avg.pct_of_peak_sustained_elapsed of the same capture
 ENS_NS, ENS_EPS = 10, 0.1   # replica ensemble: leapfrog ns=10, eps=0.1
 CPU_TRAJ = 2                # trajectories of the GPU arm's CPU-baseline sample
 
