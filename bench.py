@@ -277,6 +277,7 @@ def run_configs(qed2d, torch, dev):
         qed2d.HMC_(U2, 0.1, 10, [], p2, None)   # pure-gauge thermalisation
     c2, sched = {}, {}
     names = {0: "grid, last block publishes", 1: "grid, every block sums", 2: "one thread-block cluster"}
+    names.update({k + 4: v + "; stencil on r, links in shared memory" for k, v in list(names.items())})
     for prec in ("mixed", "f64", "plain"):
         qed2d.set_precision(prec)
         Uc = U2.clone()

@@ -311,18 +311,9 @@ __device__ __forceinline__ void tma_issue(const UTma& T, const UGeom& g, char* s
 // recurrence (the Chronopoulos-Gear form of the direction update), so the bits
 // differ from the other schedules while the FP64 stop rule is unchanged.  After
 // a reliable update the rescaled beta of RED_R4 keeps t = g5Dw p, as it keeps p.
-// FP32 links of the block's tiles staged once per solve in shared memory (LSM,
-// schedule 9 with RSTEN): per tile a box of u1 over the tile's rows and the
-// column left of it (TYv x 33) and a box of u2 over the tile's columns and the
-// row below it ((TYv + 1) x 32), so a site reads u1(x), u1(x - 1), u2(x) and
-// u2(x - 2) from shared memory without a branch.  The links do not change during
-// a solve; the values are those of the global planes, so the bits are those of
-// the same schedule without staging.
-template <int TYv>
-struct ULsm {
-    static constexpr int B1 = TYv * 33, TS = TYv * 33 + (TYv + 1) * 32;   // float2 per tile
-    static __host__ __device__ constexpr size_t bytes(int per_block) { return sizeof(float2) * TS * (size_t)per_block; }
-};
+// LSM (schedule 9 with RSTEN): the FP32 links of the block's tiles staged once
+// per solve in shared memory (ULsm, stencil.cuh).  The links do not change
+// during a solve, and the values are those of the global planes.
 
 template <int RS, int TYv, bool TMA = false, bool RSTEN = false, bool LSM = false>
 __device__ __forceinline__ bool u_body(const UCGP& P, const UTma* T, char* stg, uint64_t* bar, GridSync& gs, int& k,
@@ -394,24 +385,11 @@ __device__ __forceinline__ bool u_body(const UCGP& P, const UTma* T, char* stg, 
     // the FP32 stencil of spinor accessor S around site q of the block's tile j
     // (centre value c given), links from shared memory (LSM) or the planes
     auto sten = [&](const auto& S, const Pair<float>& c, const Site& q, int j) -> Pair<float> {
-        if constexpr (LSM) {
-            const float2* b1 = lsm + j * ULsm<TYv>::TS + ly * 33 + lx;
-            const float2* b2 = lsm + j * ULsm<TYv>::TS + ULsm<TYv>::B1 + ly * 32 + lx;
-            return g5dw_at_cl<float>(S, c, q, b1[1], b2[32], b1[0], b2[0], m2f);
-        } else {
-            return g5dw_at_c<float>(S, c, Lf, q, m2f);
-        }
+        if constexpr (LSM) return ULsm<TYv>::stencil(lsm, j, S, c, q, m2f);
+        else return g5dw_at_c<float>(S, c, Lf, q, m2f);
     };
     if constexpr (LSM) {   // stage the links of the block's tiles
-        float2* w = const_cast<float2*>(lsm);
-        FOR_MY_UTILES(q) {
-            float2* b1 = w + (tt_ - TR.lo) * ULsm<TYv>::TS + ly * 33 + lx;
-            float2* b2 = w + (tt_ - TR.lo) * ULsm<TYv>::TS + ULsm<TYv>::B1 + ly * 32 + lx;
-            b1[1] = Lf.u1(q.x);
-            b2[32] = Lf.u2(q.x);
-            if (lx == 0) b1[0] = Lf.u1(q.xm1);
-            if (ly == 0) b2[0] = Lf.u2(q.xm2);
-        }
+        FOR_MY_UTILES(q) ULsm<TYv>::stage(const_cast<float2*>(lsm), tt_ - TR.lo, Lf, q);
         __syncthreads();
     }
     {   // |b|^2 per replica; x = 0

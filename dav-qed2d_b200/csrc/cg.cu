@@ -339,9 +339,16 @@ done:
 }
 
 // ---------------------------------------------------------------------------
-// mixed FP32/FP64 reliable-update CG
-template <int RS>
+// mixed FP32/FP64 reliable-update CG.  RL (schedules 4, 5, 6 = 0, 1, 2 with it):
+// the first phase applies the stencil to r and carries t = g5Dw r + beta t_old
+// (g5Dw is linear, so t = g5Dw p; p is formed at the site only), and the FP32
+// links of the block's tiles are staged once per solve in shared memory
+// (ULsm<TY>; dynamic shared memory of per_block tiles).  The same recurrences,
+// with t rounded along its own recurrence, so results agree with the plain form
+// to the solver's accuracy.
+template <int RS, bool RL = false>
 __global__ void __launch_bounds__(TILE, 4) k_cg_mixed(const CGP P) {
+    extern __shared__ float2 lsm_dyn[];   // RL: ULsm<TY>::bytes(P.per_block)
     __shared__ double smem[32 * 2];
     auto gs = make_sync<RS>(P.ctl);
     const long long ntiles = num_tiles(P.g), V = P.g.V;
@@ -354,6 +361,15 @@ __global__ void __launch_bounds__(TILE, 4) k_cg_mixed(const CGP P) {
     int k = 0, nupd = 0;
     bool conv = false;
     double rr64 = 0.0, bb = 0.0;
+    // the FP32 stencil of accessor S around site q of the block's tile j (centre c given)
+    auto sten = [&](const auto& S, const Pair<float>& c, const Site& q, int j) -> Pair<float> {
+        if constexpr (RL) return ULsm<TY>::stencil(lsm_dyn, j, S, c, q, m2f);
+        else return g5dw_at_c<float>(S, c, Lf, q, m2f);
+    };
+    if constexpr (RL) {   // stage the links of the block's tiles
+        FOR_TILES(q) ULsm<TY>::stage(lsm_dyn, tt_ - TR.lo, Lf, q);
+        __syncthreads();
+    }
 
     {
         double v[1] = {0.0};
@@ -423,15 +439,34 @@ __global__ void __launch_bounds__(TILE, 4) k_cg_mixed(const CGP P) {
         for (k = 1; k <= P.maxiter; k++) {
             float4* qn = cur ? P.q1 : P.q0;
             const float4* qo = cur ? P.q0 : P.q1;
-            const SpAxpy<float, SpF> Q{SpF{P.r32}, SpF{qo}, (float)beta, !first};
             float ft = 0.f, fc = 0.f;   // per-thread sums in FP32: one conversion per phase
-            FOR_TILES(q) {
-                const Pair<float> c = Q.ld(q.x);
-                const Pair<float> tt = g5dw_at_c<float>(Q, c, Lf, q, m2f);
-                st_f(qn, q.x, c);
-                st_f(P.t32, q.x, tt);
-                ft += norm2(tt.a) + norm2(tt.b);
-                fc += norm2(c.a) + norm2(c.b);
+            if constexpr (RL) {
+                const float bf = (float)beta;
+                FOR_TILES(q) {
+                    const Pair<float> rc = SpF{P.r32}.ld(q.x);
+                    Pair<float> tt = sten(SpF{P.r32}, rc, q, tt_ - TR.lo), c = rc;
+                    if (!first) {   // p = r + beta p_old, t = g5Dw r + beta t_old
+                        const Pair<float> po = SpF{qo}.ld(q.x), to = SpF{P.t32}.ld(q.x);
+                        c.a = c.a + bf * po.a;
+                        c.b = c.b + bf * po.b;
+                        tt.a = tt.a + bf * to.a;
+                        tt.b = tt.b + bf * to.b;
+                    }
+                    st_f(qn, q.x, c);
+                    st_f(P.t32, q.x, tt);
+                    ft += norm2(tt.a) + norm2(tt.b);
+                    fc += norm2(c.a) + norm2(c.b);
+                }
+            } else {
+                const SpAxpy<float, SpF> Q{SpF{P.r32}, SpF{qo}, (float)beta, !first};
+                FOR_TILES(q) {
+                    const Pair<float> c = Q.ld(q.x);
+                    const Pair<float> tt = g5dw_at_c<float>(Q, c, Lf, q, m2f);
+                    st_f(qn, q.x, c);
+                    st_f(P.t32, q.x, tt);
+                    ft += norm2(tt.a) + norm2(tt.b);
+                    fc += norm2(c.a) + norm2(c.b);
+                }
             }
             double v[1] = {(double)ft + mu2 * (double)fc};
             if (!reduce_sync<1, RS>(gs, v, P.part, P.ctl->red, smem)) goto done;
@@ -440,7 +475,7 @@ __global__ void __launch_bounds__(TILE, 4) k_cg_mixed(const CGP P) {
             if (!kPair) {
                 FOR_TILES(q) {
                     const Pair<float> pc = SpF{qn}.ld(q.x);
-                    const Pair<float> a = g5dw_at<float>(SpF{P.t32}, Lf, q, m2f);
+                    const Pair<float> a = sten(SpF{P.t32}, SpF{P.t32}.ld(q.x), q, tt_ - TR.lo);
                     Pair<float> xv = SpF{P.x32}.ld(q.x), r = SpF{P.r32}.ld(q.x);
                     xv.a = xv.a + alpha * pc.a;
                     xv.b = xv.b + alpha * pc.b;
@@ -453,7 +488,7 @@ __global__ void __launch_bounds__(TILE, 4) k_cg_mixed(const CGP P) {
             } else if (pend) {
                 FOR_TILES(q) {   // x += apend p_old, then x += alpha p
                     const Pair<float> po = SpF{qo}.ld(q.x), pc = SpF{qn}.ld(q.x);
-                    const Pair<float> a = g5dw_at<float>(SpF{P.t32}, Lf, q, m2f);
+                    const Pair<float> a = sten(SpF{P.t32}, SpF{P.t32}.ld(q.x), q, tt_ - TR.lo);
                     Pair<float> xv = SpF{P.x32}.ld(q.x), r = SpF{P.r32}.ld(q.x);
                     xv.a = xv.a + apend * po.a;
                     xv.b = xv.b + apend * po.b;
@@ -468,7 +503,7 @@ __global__ void __launch_bounds__(TILE, 4) k_cg_mixed(const CGP P) {
             } else if (shifted) {
                 FOR_TILES(q) {   // x's update waits for the next iteration
                     const Pair<float> pc = SpF{qn}.ld(q.x);
-                    const Pair<float> a = g5dw_at<float>(SpF{P.t32}, Lf, q, m2f);
+                    const Pair<float> a = sten(SpF{P.t32}, SpF{P.t32}.ld(q.x), q, tt_ - TR.lo);
                     Pair<float> r = SpF{P.r32}.ld(q.x);
                     r.a = r.a - alpha * (a.a + mu2f * pc.a);
                     r.b = r.b - alpha * (a.b + mu2f * pc.b);
@@ -477,7 +512,7 @@ __global__ void __launch_bounds__(TILE, 4) k_cg_mixed(const CGP P) {
                 }
             } else {
                 FOR_TILES(q) {   // the same without a shift (a + 0 p = a exactly)
-                    const Pair<float> a = g5dw_at<float>(SpF{P.t32}, Lf, q, m2f);
+                    const Pair<float> a = sten(SpF{P.t32}, SpF{P.t32}.ld(q.x), q, tt_ - TR.lo);
                     Pair<float> r = SpF{P.r32}.ld(q.x);
                     r.a = r.a - alpha * a.a;
                     r.b = r.b - alpha * a.b;
@@ -1061,12 +1096,69 @@ static int launch_cluster(Ctx& c, void (*kernel)(Par), Par P, int threads = TILE
     return QED2D_OK;
 }
 
-// the solver of precision slot (0 = F64, 1 = MIXED) under schedule rs
+// The mixed solver's RL form (schedules 4, 5, 6): the reduction schedule rs =
+// 0, 1 (cooperative grid) or 2 (one cluster) with the links of every block's
+// tiles in dynamic shared memory.  The geometry is the plain form's; the launch
+// is refused (QED2D_ERR_UNSUPPORTED, nothing enqueued) when the blocks of that
+// geometry are not co-resident with the staged links.
+static int launch_mixed_rl(Ctx& c, const CGP& P0, int rs) {
+    void (*kern)(CGP) = rs == 2 ? k_cg_mixed<2, true> : rs ? k_cg_mixed<1, true> : k_cg_mixed<0, true>;
+    const long long nt = num_tiles(c.g);
+    int grid = 0;
+    if (rs == 2) QTRY(cluster_grid(c, kern, &grid));
+    else QTRY(coop_grid(c, kern, &grid));
+    CGP P = P0;
+    P.per_block = (int)((nt + grid - 1) / grid);
+    grid = (int)((nt + P.per_block - 1) / P.per_block);
+    const size_t sm = ULsm<TY>::bytes(P.per_block);
+    int optin = 0;
+    cudaFuncAttributes fa{};
+    QCHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device));
+    QCHECK(cudaFuncGetAttributes(&fa, (const void*)kern));
+    if (sm + fa.sharedSizeBytes > (size_t)optin) return QED2D_ERR_UNSUPPORTED;
+    QCHECK(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                optin - (int)fa.sharedSizeBytes));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(TILE);
+    cfg.dynamicSmemBytes = sm;
+    cfg.stream = c.stream;
+    cudaLaunchAttribute at[1];
+    if (rs == 2) {
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = grid;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        int n = 0;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        if (cudaOccupancyMaxActiveClusters(&n, (const void*)kern, &cfg) != cudaSuccess || n < 1) {
+            cudaGetLastError();
+            return QED2D_ERR_UNSUPPORTED;
+        }
+    } else {
+        int n = 0;
+        QCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, (const void*)kern, TILE, sm));
+        if ((long long)n * c.num_sms < grid) return QED2D_ERR_UNSUPPORTED;
+        at[0].id = cudaLaunchAttributeCooperative;
+        at[0].val.cooperative = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+    }
+    QTRY(reset_barrier(c));
+    QCHECK(cudaLaunchKernelEx(&cfg, kern, P));
+    count_launch();
+    return QED2D_OK;
+}
+
+// the solver of precision slot (0 = F64, 1 = MIXED) under schedule rs (the
+// mixed solver's 4, 5, 6: its RL form under 0, 1, 2)
 static int launch_cg(Ctx& c, const CGP& P, int slot, int rs) {
     if (slot == 0) {
         if (rs == 2) return launch_cluster(c, k_cg_f64<2>, P);
         return launch_coop(c, rs ? k_cg_f64<1> : k_cg_f64<0>, P);
     }
+    if (rs >= 4) return launch_mixed_rl(c, P, rs - 4);
     if (rs == 2) return launch_cluster(c, k_cg_mixed<2>, P);
     return launch_coop(c, rs ? k_cg_mixed<1> : k_cg_mixed<0>, P);
 }
@@ -1095,34 +1187,39 @@ bool tuning_enabled() {
     return !(e && e[0] == '0');
 }
 
+// Times every candidate schedule (3 rounds, the first warms up) and returns the
+// fastest in *best; a candidate whose launch is refused with
+// QED2D_ERR_UNSUPPORTED (a cluster or staged links that do not fit) is dropped.
 template <class Launch>
-static int time_schedules(Ctx& c, Launch launch, int ncand, int* best) {
+static int time_schedules(Ctx& c, Launch launch, const std::vector<int>& cand, int* best) {
     cudaEvent_t e0, e1;
     QCHECK(cudaEventCreate(&e0));
     QCHECK(cudaEventCreate(&e1));
-    float tbest[3] = {1e30f, 1e30f, 1e30f};
+    std::vector<float> tbest(cand.size(), 1e30f);
     int st = QED2D_OK;
     for (int rep = 0; rep < 3 && st == QED2D_OK; rep++)
-        for (int rs = 0; rs < ncand && st == QED2D_OK; rs++) {
+        for (size_t i = 0; i < cand.size() && st == QED2D_OK; i++) {
+            if (tbest[i] >= 2e30f) continue;
             cudaEventRecord(e0, c.stream);
-            const int lst = launch(rs);
+            const int lst = launch(cand[i]);
             cudaEventRecord(e1, c.stream);
-            if (lst != QED2D_OK && rs == 2) {   // the cluster launch was refused: drop the candidate
+            if (lst == QED2D_ERR_UNSUPPORTED) {   // refused before anything was enqueued: drop it
                 cudaGetLastError();
-                tbest[2] = 2e30f;
+                tbest[i] = 3e30f;
                 continue;
             }
             st = lst;
             if (cudaEventSynchronize(e1) != cudaSuccess) st = cuda_status(cudaGetLastError(), "schedule tuning");
             float ms = 0.f;
             cudaEventElapsedTime(&ms, e0, e1);
-            if (rep > 0 && tbest[rs] < 2e30f) tbest[rs] = std::min(tbest[rs], ms);   // the first repetition warms up
+            if (rep > 0) tbest[i] = std::min(tbest[i], ms);
         }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    *best = 0;
-    for (int rs = 1; rs < ncand; rs++)
-        if (tbest[rs] <= tbest[*best]) *best = rs;
+    size_t b = 0;
+    for (size_t i = 1; i < cand.size(); i++)
+        if (tbest[i] <= tbest[b]) b = i;
+    *best = cand[b];
     return st;
 }
 
@@ -1140,7 +1237,12 @@ static int tune_cg(Ctx& c, const CGP& P, int slot) {
     if (!T.x || (P.g5x && !T.g5x)) return QED2D_ERR_NO_MEMORY;
     T.maxiter = std::min(P.maxiter, kTuneIters);
     const size_t fb = sizeof(double2) * 2 * (size_t)c.g.V;
-    const int ncand = cluster_possible(c, slot) ? 3 : 2;
+    std::vector<int> cand = {0, 1};
+    if (cluster_possible(c, slot)) cand.push_back(2);
+    if (slot == 1) {   // the RL form under each reduction schedule
+        const size_t n = cand.size();
+        for (size_t i = 0; i < n; i++) cand.push_back(cand[i] + 4);
+    }
     int best = 1;
     const int st = time_schedules(
         c,
@@ -1148,7 +1250,7 @@ static int tune_cg(Ctx& c, const CGP& P, int slot) {
             if (P.guess) QCHECK(cudaMemcpyAsync(T.x, P.x, fb, cudaMemcpyDeviceToDevice, c.stream));
             return launch_cg(c, T, slot, rs);
         },
-        ncand, &best);
+        cand, &best);
     QCHECK(cudaMemcpyAsync(c.ctl, &saved, sizeof(DevCtl), cudaMemcpyHostToDevice, c.stream));
     QCHECK(cudaStreamSynchronize(c.stream));
     if (st != QED2D_OK) return st;
@@ -1194,7 +1296,7 @@ int cg_solve(Ctx& c, const SolveArgs& a, int precision) {
         P.U32 = u32;
     }
     if (c.sched[1] < 0) QTRY(tune_cg(c, P, 1));
-    if (c.sched[1] == 2 && !cluster_possible(c, 1)) c.sched[1] = 1;
+    if ((c.sched[1] & 3) == 2 && !cluster_possible(c, 1)) c.sched[1] -= 1;
     return launch_cg(c, P, 1, c.sched[1]);
 }
 

@@ -478,9 +478,13 @@ int qed2d_ctx_set_schedule(qed2d_ctx* ctx, int precision, int schedule) {
     QCTX(ctx);
     const int slot = sched_slot(precision);
     if (slot < 0) return bad_arg("schedule: QED2D_PREC_F64, QED2D_PREC_MIXED or QED2D_MULTISHIFT only");
-    const int top = slot == 2 ? 3 : 2;   // the multishift solver also has its FP32-inner form (3)
-    if (schedule < -1 || schedule > top)
-        return bad_arg(slot == 2 ? "multishift schedule must be -1, 0, 1, 2 or 3" : "schedule must be -1, 0, 1 or 2");
+    // the multishift solver also has its FP32-inner form (3), the mixed CG its RL form (4, 5, 6)
+    const bool ok = schedule >= -1 && (schedule <= 2 || (slot == 2 && schedule == 3) ||
+                                       (slot == 1 && schedule >= 4 && schedule <= 6));
+    if (!ok)
+        return bad_arg(slot == 2   ? "multishift schedule must be -1, 0, 1, 2 or 3"
+                       : slot == 1 ? "mixed CG schedule must be -1, 0, 1, 2, 4, 5 or 6"
+                                   : "schedule must be -1, 0, 1 or 2");
     c.sched[slot] = schedule;
     return QED2D_OK;
 }

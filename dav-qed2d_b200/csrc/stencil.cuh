@@ -222,6 +222,35 @@ __device__ __forceinline__ Pair<R> g5dw_at_cl(const S& s, const Pair<R>& c, cons
     return o;
 }
 
+// FP32 links of a block's tiles staged in shared memory for the length of a
+// solve (they do not change during one): per tile of 32 x TYv sites a box of u1
+// over the tile's rows and the column left of it (TYv x 33) and a box of u2 over
+// the tile's columns and the row below it ((TYv + 1) x 32), so a site reads
+// u1(x), u1(x - 1), u2(x) and u2(x - 2) without a branch.  j is the tile's index
+// in the block's range; thread t of the tile is site (t % 32, t / 32).
+template <int TYv>
+struct ULsm {
+    static constexpr int B1 = TYv * 33, TS = TYv * 33 + (TYv + 1) * 32;   // float2 per tile
+    static __host__ __device__ constexpr size_t bytes(int per_block) { return sizeof(float2) * TS * (size_t)per_block; }
+    static __device__ __forceinline__ void stage(float2* s, int j, const LkF& Lf, const Site& q) {
+        const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
+        float2* b1 = s + j * TS + ly * 33 + lx;
+        float2* b2 = s + j * TS + B1 + ly * 32 + lx;
+        b1[1] = Lf.u1(q.x);
+        b2[32] = Lf.u2(q.x);
+        if (lx == 0) b1[0] = Lf.u1(q.xm1);
+        if (ly == 0) b2[0] = Lf.u2(q.xm2);
+    }
+    template <class S>
+    static __device__ __forceinline__ Pair<float> stencil(const float2* s, int j, const S& sp, const Pair<float>& c,
+                                                          const Site& q, float m2) {
+        const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
+        const float2* b1 = s + j * TS + ly * 33 + lx;
+        const float2* b2 = s + j * TS + B1 + ly * 32 + lx;
+        return g5dw_at_cl<float>(sp, c, q, b1[1], b2[32], b1[0], b2[0], m2);
+    }
+};
+
 // total gauge force on the two links of site y: frc1+frc2 of krnl_force!
 //   F1(y) = -v(y) + v(y-2),  F2(y) = v(y) - v(y-1)
 // The three plaquettes share links: the 10 distinct links are addressed from

@@ -302,7 +302,9 @@ def set_schedule(prm: LattParm, schedule: int, precision="mixed") -> None:
     solve.  0 and 1 give the same bits.  `precision` selects the solver:
     "f64" or "mixed" (CG), "multishift" (the RHMC shifted solves; its schedule
     3 is the FP32 shared Krylov space with every shift refined by the mixed CG,
-    the untuned choice from 2^22 sites on)."""
+    the untuned choice from 2^22 sites on).  The mixed CG also has 4, 5, 6:
+    0, 1, 2 with the first stencil applied to r and the links staged in shared
+    memory (agrees with 0, 1, 2 to the solver's accuracy; small lattices)."""
     check(lib().qed2d_ctx_set_schedule(_c(prm), _PRECS[precision], int(schedule)), "set_schedule")
 
 

@@ -115,7 +115,13 @@ int qed2d_ctx_get_dims(const qed2d_ctx* ctx, int* L1, int* L2);
  * the shared Krylov space in FP32 (to a relative residual of 1e-6), then every
  * shift refined by the mixed CG from that start to the FP64 stop rule; it is the
  * first solve's choice on lattices of 2^22 sites and more (measured faster there,
- * slower below), and is otherwise chosen only when set. */
+ * slower below), and is otherwise chosen only when set.  The mixed CG has a
+ * second form under each reduction schedule, 4, 5, 6 = 0, 1, 2 with the first
+ * phase's stencil applied to r (t = g5Dw r + beta t_old) and the FP32 links of
+ * every block's tiles staged once per solve in shared memory; it agrees with
+ * the first form to the solver's accuracy, is a candidate of the first solve's
+ * timing, and is refused (QED2D_ERR_UNSUPPORTED) where the staged links do not
+ * fit beside co-resident blocks (large lattices). */
 #define QED2D_MULTISHIFT 3   /* schedule selector of the multishift solver (FP64) */
 int qed2d_ctx_set_schedule(qed2d_ctx* ctx, int precision, int schedule);
 int qed2d_ctx_get_schedule(const qed2d_ctx* ctx, int precision, int* schedule);

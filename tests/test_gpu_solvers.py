@@ -260,7 +260,8 @@ def test_reduction_schedules_give_identical_bits(L, prec):
     """The two grid-reduction schedules of the persistent solvers (last block
     publishes / every block sums) perform the same additions in the same order:
     solutions and iteration counts are bitwise identical, so the tuner's choice
-    never changes a result.  The first solve tunes the schedule (0 or 1)."""
+    never changes a result; the same holds for the mixed solver's second form
+    (4 and 5).  The first solve tunes the schedule."""
     import qed2d
     prm = qed2d.LattParm((L, L), 4.0)
     U, src = to_dev(hot_links(L, L, 5)), to_dev(cgauss(L, L, 6, 2))
@@ -269,15 +270,16 @@ def test_reduction_schedules_give_identical_bits(L, prec):
         qed2d.set_schedule(prm, -1, prec)
         x = qed2d.cfield(L, L)
         qed2d.CG(x, U, src, 0.2, 20000, 1e-24, qed2d.gamm5Dw_sqr_msq, prm, None)
-        assert qed2d.get_schedule(prm, prec) in (0, 1, 2)
-        out = []
-        for sched in (0, 1):
-            qed2d.set_schedule(prm, sched, prec)
-            x = qed2d.cfield(L, L)
-            it = qed2d.CG(x, U, src, 0.2, 20000, 1e-24, qed2d.gamm5Dw_sqr_msq, prm, None)
-            out.append((it, to_host(x)))
-        assert out[0][0] == out[1][0]
-        assert np.array_equal(out[0][1], out[1][1])
+        assert qed2d.get_schedule(prm, prec) in ((0, 1, 2) if prec == "f64" else (0, 1, 2, 4, 5, 6))
+        for pair in ((0, 1), (4, 5)) if prec == "mixed" else ((0, 1),):
+            out = []
+            for sched in pair:
+                qed2d.set_schedule(prm, sched, prec)
+                x = qed2d.cfield(L, L)
+                it = qed2d.CG(x, U, src, 0.2, 20000, 1e-24, qed2d.gamm5Dw_sqr_msq, prm, None)
+                out.append((it, to_host(x)))
+            assert out[0][0] == out[1][0], pair
+            assert np.array_equal(out[0][1], out[1][1]), pair
     finally:
         qed2d.set_schedule(prm, -1, prec)
         qed2d.set_precision("f64")
@@ -401,3 +403,44 @@ def test_rhmc_trajectory_fp32_inner_multishift_vs_oracle():
     assert st == 0 and info.accepted == acco
     bound("RHMC FP32-inner multishift dH abs vs oracle", abs(info.dH - (hf - hi)), 1e-9)
     bound("RHMC FP32-inner multishift links vs oracle", rel(to_host(Ud), Uo), 1e-11)
+
+
+@pytest.mark.parametrize("L1,L2,mu", [(64, 48, 0.0), (100, 37, 0.0), (128, 128, 0.4), (512, 512, 0.0)])
+def test_mixed_cg_rl_form_vs_plain_form_and_oracle(q, L1, L2, mu):
+    """The mixed CG's second form (schedules 4, 5, 6: the first stencil applied
+    to r, t = g5Dw r + beta t_old, and the FP32 links staged in shared memory)
+    under each reduction schedule that fits, against the first form (0, 1, 2)
+    and the oracle: the same FP64 stop rule, so solutions agree to the mixed
+    solver's accuracy (5e-12 against the oracle), iteration counts within 2 of
+    the first form, plain and shifted (method 2) systems."""
+    q.set_precision("mixed")
+    prm = q.LattParm((L1, L2), 4.0)
+    o = Oracle(L1, L2, 4.0)
+    U, b = setup(L1, L2, seed=31)
+    am0 = 0.25
+    st, xo, _, _ = o.cg(U, b, am0, 20000, 1e-24, mu=mu)
+    assert st == 0
+    Ud, bd = to_dev(U), to_dev(b)
+    res = {}
+    try:
+        for sched in (0, 1, 2, 4, 5, 6):
+            q.set_schedule(prm, sched, "mixed")
+            x = q.cfield(L1, L2)
+            try:
+                if mu:
+                    it = q.CG(x, Ud, bd, am0, mu, 20000, 1e-24, q.gamm5Dw_sqr_musq, prm, None)
+                else:
+                    it = q.CG(x, Ud, bd, am0, 20000, 1e-24, q.gamm5Dw_sqr_msq, prm, None)
+            except q.Qed2dError as e:   # a cluster or the staged links do not fit at this size
+                assert e.status == q._lib.UNSUPPORTED and sched in (2, 4, 5, 6), (sched, e)
+                continue
+            res[sched] = (it, to_host(x))
+            bound("mixed CG (both forms) vs oracle", rel(res[sched][1], xo), 5e-12)  # sched
+    finally:
+        q.set_schedule(prm, -1, "mixed")
+        q.set_precision("f64")
+    assert 0 in res and 1 in res
+    rl = [s for s in (4, 5, 6) if s in res]
+    assert rl or L1 * L2 > 1 << 18   # the staged links fit up to 512^2 at least
+    for s in rl:
+        bound("mixed CG second form vs first form iterations", abs(res[s][0] - res[s - 4][0]), 2)  # s
