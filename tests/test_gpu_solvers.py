@@ -7,7 +7,7 @@ helpers.bound; the solution error of a CG stopped at |r|^2 < eps |b|^2 is at mos
 the condition number times the residual, but two solvers that follow the same
 Krylov recurrences agree far closer than that):
   * FP64 and reference-structured paths, eps = 1e-24 (relative residual 1e-12):
-    max|x_gpu - x_oracle| / max|x_oracle| < 1e-13 (the north star asks 1e-12),
+    max|x_gpu - x_oracle| / max|x_oracle| < 1e-13 (the FP64-path requirement is 1e-12),
     iteration counts within 1;
   * mixed FP32/FP64 path: 5e-12 -- the final solve meets the same FP64 residual
     along a different (FP32) Krylov path."""
@@ -47,7 +47,7 @@ def test_cg_method1(q, prec, L1, L2, unitary):
     assert st == 0
     x = q.cfield(L1, L2)
     it = q.CG(x, to_dev(U), to_dev(b), am0, 20000, 1e-24, q.gamm5Dw_sqr_msq, prm, None)
-    # FP64 paths: the north star asks 1e-12; measured <= 2e-15.  Mixed: the same
+    # FP64 paths: 1e-12 required; measured <= 2e-15.  Mixed: the same
     # FP64 stop rule through a different Krylov path; measured <= 6e-13
     bound(f"CG method 1 {prec} vs oracle", rel(to_host(x), xo), 1e-13 if prec != "mixed" else 5e-12)
     # residual of the GPU solution, evaluated by the oracle
