@@ -75,3 +75,34 @@ def test_gauge_checkpoint_roundtrip(tmp_path):
     # Julia column-major order: first lines are U[1,1,1], U[2,1,1], ...
     assert float(lines[1].split("\t")[0]) == U[0, 0, 1].real
     assert np.array_equal(load_gauge_text(str(f), 4, 3), U)
+
+
+def prototypes():
+    """{name: number of parameters} of every prototype in include/qed2d.h."""
+    txt = re.sub(r"/\*.*?\*/", " ", open(HEADER).read(), flags=re.S)
+    out = {}
+    for m in re.finditer(r"\b(qed2d_[A-Za-z0-9_]+)\s*\(([^;{]*?)\)\s*;", txt):
+        args = m.group(2).strip()
+        out[m.group(1)] = 0 if args in ("", "void") else args.count(",") + 1
+    return out
+
+
+def test_python_signatures_match_header_arity(built):
+    """Every ctypes signature of the Python mirror passes as many arguments as the
+    header's prototype declares (a dropped or extra argument would shift every
+    later one)."""
+    from qed2d import _lib
+    protos = prototypes()
+    assert set(protos) == set(declared())
+    wrong = {s: (len(_lib.SIGNATURES[s][1]), n) for s, n in protos.items() if len(_lib.SIGNATURES[s][1]) != n}
+    assert not wrong, wrong
+
+
+def test_graph_entry_points_reject_null_handles(built):
+    """The CUDA-graph controls reject a NULL context or batch without touching a GPU."""
+    from qed2d import _lib
+    L = _lib.lib()
+    assert L.qed2d_ctx_set_graphs(None, 1) == _lib.BAD_ARG
+    assert L.qed2d_ctx_graph_stats(None, None, None, None, None) == _lib.BAD_ARG
+    assert L.qed2d_batch_set_graphs(None, 0) == _lib.BAD_ARG
+    assert L.qed2d_batch_graph_stats(None, None, None, None, None) == _lib.BAD_ARG
