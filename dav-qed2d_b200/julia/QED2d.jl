@@ -83,6 +83,9 @@ function ctx(prm::LattParm)
 end
 set_precision!(prm::LattParm, p::Integer) = check(ccall((:qed2d_ctx_set_precision, lib), Cint,
                                                         (Ptr{Cvoid}, Cint), ctx(prm), p), "set_precision")
+# CUDA-graph replay of HMC!'s MD integration on this lattice's context (on by default)
+set_graphs!(prm::LattParm, on::Bool) = check(ccall((:qed2d_ctx_set_graphs, lib), Cint,
+                                                   (Ptr{Cvoid}, Cint), ctx(prm), on ? 1 : 0), "set_graphs")
 
 const CF = CuArray{ComplexF64}
 const RF = CuArray{Float64}
